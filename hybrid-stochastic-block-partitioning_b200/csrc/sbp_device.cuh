@@ -1,0 +1,396 @@
+// Device-side building blocks of the B200 stochastic block partitioning engine:
+// counter-based random numbers, warp primitives, the per-warp neighbour-block table, and the
+// warp-cooperative vertex-move evaluation (proposal, Hastings correction, delta-MDL, accept).
+//
+// Semantics follow the reference (vtsynergy/Hybrid-Stochastic-Block-Partitioning):
+//   proposal          src/common.cpp:131-192  (canonical row-then-column multinomial order)
+//   hastings          src/entropy.cpp:495-557 (new degree of r/s ignores the in-side self edge)
+//   delta-MDL         src/entropy.cpp:296-401 (a present Delta cell with net change 0 and a
+//                     non-zero count at (r,s) or (s,r) is counted twice, as the reference's
+//                     "unchanged cell" loops do)
+//   accept            src/finetune.cpp:19-29
+// Log terms are FP64. delta-MDL uses the closed form
+//   dS = sum_changed [g(M)-g(M')] - sum_{x in r,s} [g(d_out x)-g(d_out' x)] - [same for d_in] + Q
+// with g(x) = x log x, which equals the reference's per-cell sum over rows/cols r,s.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sbpb {
+
+constexpr int kWarp = 32;
+constexpr unsigned kFull = 0xffffffffu;
+
+// Error bits written to the device status word (never trap).
+enum : int {
+  kErrTableFull = 1,      // neighbour-block table overflow
+  kErrScan = 2,           // multinomial walk ran off the row (inconsistent counts)
+  kErrReplay = 4,         // replay record index out of range
+  kErrBounds = 8,         // block or vertex id out of range
+};
+
+// ------------------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon et al., SC'11). Counter (a, b, call, tag), key = seed.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+struct RngParams {
+  uint64_t seed;
+  const uint4* replay;      // optional host-supplied stream (device copy)
+  long long replay_records;
+  uint32_t call;
+};
+
+// Record for (a, b, tag); replay records are indexed by `slot`.
+__device__ __forceinline__ uint4 draw_record(const RngParams& p, uint32_t a, uint32_t b, uint32_t tag,
+                                             long long slot, int* status) {
+  if (p.replay) {
+    if (slot < 0 || slot >= p.replay_records) {
+      atomicOr(status, kErrReplay);
+      return make_uint4(0, 0, 0, 0xffffffffu);   // u_acc ~ 1: never accepts
+    }
+    return p.replay[slot];
+  }
+  return philox4x32_10(make_uint4(a, b, p.call, tag), (uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+}
+
+__device__ __forceinline__ long long scale32(uint32_t x, long long n) {
+  return (long long)(((unsigned long long)x * (unsigned long long)n) >> 32);
+}
+__device__ __forceinline__ double u53(uint32_t hi, uint32_t lo) {
+  const unsigned long long m = ((unsigned long long)hi << 21) | (unsigned long long)(lo >> 11);
+  return (double)m * (1.0 / 9007199254740992.0);
+}
+// common::propose_random_block with a scaled 32-bit draw.
+__device__ __forceinline__ int random_block(int r, int B, uint32_t x) {
+  int p = (int)scale32(x, (long long)B - 1);
+  return p >= r ? p + 1 : p;
+}
+
+// ------------------------------------------------------------------------------------------
+// FP64 helpers: g(x) = x log x and accurate differences g(a) - g(b).
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ double xlogx(double x) { return x > 0.0 ? x * log(x) : 0.0; }
+__device__ __forceinline__ double dxlogx(double a, double b) {
+  if (a == b) return 0.0;
+  if (a <= 0.0 || b <= 0.0) return xlogx(a) - xlogx(b);
+  return (a - b) * log(a) + b * log1p((a - b) / b);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+__device__ __forceinline__ int warp_sum_int(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+__device__ __forceinline__ long long warp_incl_scan(long long v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    long long n = __shfl_up_sync(kFull, v, o);
+    if (lane >= o) v += n;
+  }
+  return v;
+}
+
+// ------------------------------------------------------------------------------------------
+// Device views of the graph and the blockmodel.
+// ------------------------------------------------------------------------------------------
+struct GraphView {
+  int V;
+  long long E;
+  const int* out_ptr;     // [V+1]
+  const int* out_idx;     // out-neighbours incl. self loop, first-occurrence order
+  const int* in_ptr;      // [V+1]
+  const int* in_idx;      // in-neighbours, self loop removed
+  const unsigned char* self;
+};
+
+struct BlockView {
+  int B;
+  int ld;                 // row stride of M and MT (multiple of 32 ints)
+  int* b;                 // [V] assignment
+  int* M;                 // [B*ld] row-major counts M[row*ld+col]
+  int* MT;                // [B*ld] transpose: MT[col*ld+row] = M[row*ld+col]
+  int* d_out;             // [B]
+  int* d_in;              // [B]
+  int* d;                 // [B] block degrees as the reference maintains them
+};
+
+// Walk values row[0..n) ascending and return the first index whose running sum exceeds
+// `target` (skipping index `skip`). Warp-cooperative; returns -1 if the row is exhausted.
+// Plain (coherent) loads: the Metropolis-Hastings kernel updates M while it runs.
+__device__ __forceinline__ int warp_select_dense(const int* row, int n, long long target, int skip,
+                                                 int lane) {
+  for (int base = 0; base < n; base += kWarp) {
+    const int c = base + lane;
+    long long v = (c < n && c != skip) ? (long long)row[c] : 0;
+    const long long incl = warp_incl_scan(v, lane);
+    const long long tot = __shfl_sync(kFull, incl, 31);
+    if (target < tot) {
+      const unsigned hit = __ballot_sync(kFull, incl > target);
+      return base + __ffs(hit) - 1;
+    }
+    target -= tot;
+  }
+  return -1;
+}
+
+// Same walk over a compressed list (idx[i], val[i]), i in [0, n).
+__device__ __forceinline__ int warp_select_sparse(const int* __restrict__ idx, const int* __restrict__ val, int n,
+                                                  long long target, int skip, int lane) {
+  for (int base = 0; base < n; base += kWarp) {
+    const int i = base + lane;
+    int c = -1;
+    long long v = 0;
+    if (i < n) {
+      c = idx[i];
+      v = (c != skip) ? (long long)val[i] : 0;
+    }
+    const long long incl = warp_incl_scan(v, lane);
+    const long long tot = __shfl_sync(kFull, incl, 31);
+    if (target < tot) {
+      const unsigned hit = __ballot_sync(kFull, incl > target);
+      return __shfl_sync(kFull, c, __ffs(hit) - 1);
+    }
+    target -= tot;
+  }
+  return -1;
+}
+
+// ------------------------------------------------------------------------------------------
+// Per-warp neighbour-block table in shared memory: open addressing on block id, with a
+// compact list of used slots so reset and enumeration cost O(distinct blocks).
+// ------------------------------------------------------------------------------------------
+struct WarpTable {
+  int* keys;   // [cap], -1 = empty
+  int* cout;   // [cap] out-neighbour counts (self loop excluded)
+  int* cin;    // [cap] in-neighbour counts (self loop excluded)
+  int* list;   // [cap] used slots
+  int* nlist;  // [1]
+  int mask;    // cap - 1 (cap power of two)
+};
+
+__device__ __forceinline__ int table_slot(const WarpTable& t, int key, int* status) {
+  unsigned h = ((unsigned)key * 2654435761u) & (unsigned)t.mask;
+  for (int probe = 0; probe <= t.mask; ++probe) {
+    const int k = t.keys[h];
+    if (k == key) return (int)h;
+    if (k == -1) {
+      const int prev = atomicCAS(&t.keys[h], -1, key);
+      if (prev == -1) {
+        t.list[atomicAdd(t.nlist, 1)] = (int)h;
+        return (int)h;
+      }
+      if (prev == key) return (int)h;
+    }
+    h = (h + 1) & (unsigned)t.mask;
+  }
+  atomicOr(status, kErrTableFull);
+  return -1;
+}
+
+__device__ __forceinline__ int table_find(const WarpTable& t, int key) {
+  unsigned h = ((unsigned)key * 2654435761u) & (unsigned)t.mask;
+  for (int probe = 0; probe <= t.mask; ++probe) {
+    const int k = t.keys[h];
+    if (k == key) return (int)h;
+    if (k == -1) return -1;
+    h = (h + 1) & (unsigned)t.mask;
+  }
+  return -1;
+}
+
+// Warp-aggregated insertion: lanes holding the same key add their multiplicity once.
+__device__ __forceinline__ void table_add(const WarpTable& t, int key, bool valid, bool incoming, int* status) {
+  const int k = valid ? key : -2;
+  const unsigned peers = __match_any_sync(kFull, k);
+  const int lane = threadIdx.x & 31;
+  if (valid && (__ffs(peers) - 1) == lane) {
+    const int slot = table_slot(t, key, status);
+    if (slot >= 0) atomicAdd(incoming ? &t.cin[slot] : &t.cout[slot], __popc(peers));
+  }
+}
+
+__device__ __forceinline__ void table_reset(const WarpTable& t, int lane) {
+  __syncwarp();
+  const int n = *t.nlist;
+  for (int i = lane; i < n; i += kWarp) {
+    const int h = t.list[i];
+    t.keys[h] = -1;
+    t.cout[h] = 0;
+    t.cin[h] = 0;
+  }
+  __syncwarp();
+  if (lane == 0) *t.nlist = 0;
+  __syncwarp();
+}
+
+// Build the table for vertex v from the current assignment (self loop excluded; block r is
+// inserted when v has a self loop so the Hastings sum sees it).
+__device__ __forceinline__ void build_table(const GraphView& g, const BlockView& bm, int v, int r, const WarpTable& t,
+                                            int lane, int* status) {
+  const int o0 = g.out_ptr[v], o1 = g.out_ptr[v + 1];
+  for (int e0 = o0; e0 < o1; e0 += kWarp) {
+    const int e = e0 + lane;
+    int key = -1;
+    bool valid = false;
+    if (e < o1) {
+      const int u = __ldg(g.out_idx + e);
+      if (u != v) { key = bm.b[u]; valid = true; }
+    }
+    table_add(t, key, valid, false, status);
+  }
+  const int i0 = g.in_ptr[v], i1 = g.in_ptr[v + 1];
+  for (int e0 = i0; e0 < i1; e0 += kWarp) {
+    const int e = e0 + lane;
+    int key = -1;
+    bool valid = false;
+    if (e < i1) { key = bm.b[__ldg(g.in_idx + e)]; valid = true; }
+    table_add(t, key, valid, true, status);
+  }
+  if (lane == 0 && g.self[v]) table_slot(t, r, status);
+  __syncwarp();
+}
+
+struct EvalResult {
+  int s;          // proposed block
+  int accepted;   // 1 if accepted (s != r)
+  double dS;      // delta MDL (0 when s == r)
+  double H;       // Hastings correction
+};
+
+struct MoveCounts {   // self-loop-free neighbour counts by block for the four corner blocks
+  int co_r, co_s, ci_r, ci_s;
+};
+
+__device__ __forceinline__ MoveCounts corner_counts(const WarpTable& t, int r, int s) {
+  MoveCounts mc;
+  const int hr = table_find(t, r), hs = table_find(t, s);
+  mc.co_r = hr >= 0 ? t.cout[hr] : 0;
+  mc.ci_r = hr >= 0 ? t.cin[hr] : 0;
+  mc.co_s = hs >= 0 ? t.cout[hs] : 0;
+  mc.ci_s = hs >= 0 ? t.cin[hs] : 0;
+  return mc;
+}
+
+// Proposal for vertex v (src/common.cpp:131-182 with canonical order).
+__device__ __forceinline__ int propose_block(const GraphView& g, const BlockView& bm, int v, int r, int k_out,
+                                             int k_in, uint4 x, int lane, int* status) {
+  const int k = k_out + k_in;
+  if (k == 0) return random_block(r, bm.B, x.y);
+  const int idx = (int)scale32(x.x, k);
+  const int nbr = idx < k_out ? __ldg(g.out_idx + g.out_ptr[v] + idx) : __ldg(g.in_idx + g.in_ptr[v] + (idx - k_out));
+  const int t = bm.b[nbr];
+  const int dot = bm.d_out[t];
+  const long long total = (long long)dot + (long long)bm.d_in[t];
+  long long target = scale32(x.y, total);
+  int s;
+  if (target < dot) s = warp_select_dense(bm.M + (size_t)t * bm.ld, bm.B, target, -1, lane);
+  else s = warp_select_dense(bm.MT + (size_t)t * bm.ld, bm.B, target - dot, -1, lane);
+  if (s < 0) {
+    if (lane == 0) atomicOr(status, kErrScan);
+    s = r;
+  }
+  return s;
+}
+
+// Full evaluation of vertex v against the current state, table left filled on return
+// (caller resets it). Every lane returns the same result.
+__device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const BlockView& bm, int v, uint4 x,
+                                                      const WarpTable& t, int lane, int* status, int* r_out,
+                                                      int* k_out_out, int* k_in_out) {
+  EvalResult res;
+  const int r = bm.b[v];
+  const int k_out = g.out_ptr[v + 1] - g.out_ptr[v];
+  const int self = g.self[v];
+  const int k_in = g.in_ptr[v + 1] - g.in_ptr[v];
+  *r_out = r;
+  *k_out_out = k_out;
+  *k_in_out = k_in;
+  const int s = propose_block(g, bm, v, r, k_out, k_in, x, lane, status);
+  res.s = s;
+  res.accepted = 0;
+  res.dS = 0.0;
+  res.H = 1.0;
+  if (s == r) return res;
+
+  build_table(g, bm, v, r, t, lane, status);
+  const MoveCounts mc = corner_counts(t, r, s);
+  const int B = bm.B, ld = bm.ld;
+  const int d_rr = -mc.co_r - mc.ci_r - self;
+  const int d_rs = -mc.co_s + mc.ci_r;
+  const int d_sr = mc.co_r - mc.ci_s;
+  const int d_ss = mc.co_s + mc.ci_s + self;
+  const int M_rr = bm.M[(size_t)r * ld + r], M_rs = bm.M[(size_t)r * ld + s];
+  const int M_sr = bm.M[(size_t)s * ld + r], M_ss = bm.M[(size_t)s * ld + s];
+  const int dout_r = bm.d_out[r], dout_s = bm.d_out[s], din_r = bm.d_in[r], din_s = bm.d_in[s];
+
+  double fwd = 0.0, bwd = 0.0, dS = 0.0;
+  const int n = *t.nlist;
+  const int* Mr = bm.M + (size_t)r * ld;
+  const int* Ms = bm.M + (size_t)s * ld;
+  const int* MTr = bm.MT + (size_t)r * ld;
+  const int* MTs = bm.MT + (size_t)s * ld;
+  for (int i = lane; i < n; i += kWarp) {
+    const int h = t.list[i];
+    const int u = t.keys[h];
+    const int co = t.cout[h], ci = t.cin[h];
+    const int M_su = Ms[u], M_us = MTs[u];
+    const int du = bm.d[u];
+    const double c = (double)(co + ci + (u == r ? self : 0));
+    fwd += c * (M_su + M_us + 1.0) / ((double)du + (double)B);
+    double bw;
+    int nd;
+    if (u == r) {
+      bw = (double)(M_rr + d_rr) + (double)(M_rr + d_rr) + 1.0;
+      nd = (dout_r - k_out) + (din_r - k_in) - (M_rr + d_rr);
+    } else if (u == s) {
+      bw = (double)(M_rs + d_rs) + (double)(M_sr + d_sr) + 1.0;
+      nd = (dout_s + k_out) + (din_s + k_in) - (M_ss + d_ss);
+    } else {
+      const int M_ru = Mr[u], M_ur = MTr[u];
+      bw = (double)(M_ru - co) + (double)(M_ur - ci) + 1.0;
+      nd = du;
+      if (co) dS += dxlogx(M_ru, M_ru - co) + dxlogx(M_su, M_su + co);
+      if (ci) dS += dxlogx(M_ur, M_ur - ci) + dxlogx(M_us, M_us + ci);
+    }
+    bwd += c * bw / ((double)nd + (double)B);
+  }
+  fwd = warp_sum(fwd);
+  bwd = warp_sum(bwd);
+  dS = warp_sum(dS);
+
+  // corner cells, degree terms and the double-count of net-zero Delta cells
+  const int kin_self = k_in + self;
+  dS += dxlogx(M_rr, M_rr + d_rr) + dxlogx(M_rs, M_rs + d_rs) + dxlogx(M_sr, M_sr + d_sr) + dxlogx(M_ss, M_ss + d_ss);
+  dS -= dxlogx(dout_r, dout_r - k_out) + dxlogx(dout_s, dout_s + k_out);
+  dS -= dxlogx(din_r, din_r - kin_self) + dxlogx(din_s, din_s + kin_self);
+  if ((mc.co_s > 0 || mc.ci_r > 0) && d_rs == 0 && M_rs > 0)
+    dS += (double)M_rs * (log1p((double)kin_self / (double)din_s) + log1p(-(double)k_out / (double)dout_r));
+  if ((mc.co_r > 0 || mc.ci_s > 0) && d_sr == 0 && M_sr > 0)
+    dS += (double)M_sr * (log1p(-(double)kin_self / (double)din_r) + log1p((double)k_out / (double)dout_s));
+
+  const double H = (k_out + k_in == 0) ? 1.0 : bwd / fwd;
+  double ap = exp(-3.0 * dS) * H;
+  ap = ap >= 1.0 ? 1.0 : ap;
+  res.dS = dS;
+  res.H = H;
+  res.accepted = (u53(x.z, x.w) <= ap) ? 1 : 0;
+  return res;
+}
+
+}  // namespace sbpb

@@ -1,0 +1,1302 @@
+// Host side of the B200 stochastic block partitioning engine: device-resident graph and
+// blockmodel handles, the finetune / merge / partition drivers and the C ABI declared in
+// include/sbp_b200.h.  Control flow mirrors the reference driver (src/sbp.cpp:61-112,
+// src/blockmodel/blockmodel_triplet.cpp:3-100, src/finetune.cpp:31-162,342-444,
+// src/block_merge.cpp:123-311); all per-vertex and per-block work runs in the kernels of
+// sbp_kernels.cu.  No CPU fallback: every compute entry point needs a CUDA device.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/sbp_b200.h"
+#include "sbp_kernels.cuh"
+
+namespace sbpb {
+
+// ------------------------------------------------------------------------------------------
+// Errors
+// ------------------------------------------------------------------------------------------
+struct Error : std::runtime_error {
+  SbpStatus code;
+  Error(SbpStatus c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+static thread_local std::string g_last_error;
+
+#define SBP_CUDA(x)                                                                                     \
+  do {                                                                                                  \
+    cudaError_t e_ = (x);                                                                               \
+    if (e_ != cudaSuccess) {                                                                            \
+      if (e_ == cudaErrorMemoryAllocation) throw Error(SBP_ERR_OUT_OF_MEMORY, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+      throw Error(SBP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));                       \
+    }                                                                                                   \
+  } while (0)
+
+static long long g_launches = 0;   // kernels launched by this library (all entry points)
+static long long g_h2d = 0, g_d2h = 0;   // bytes copied host->device / device->host
+
+#define SBP_CHECK_LAUNCH() \
+  do {                     \
+    ++g_launches;          \
+    SBP_CUDA(cudaGetLastError()); \
+  } while (0)
+
+static cudaError_t count_copy(cudaError_t e, size_t bytes, cudaMemcpyKind kind) {
+  if (kind == cudaMemcpyHostToDevice) g_h2d += (long long)bytes;
+  if (kind == cudaMemcpyDeviceToHost) g_d2h += (long long)bytes;
+  return e;
+}
+#define SBP_COPY(dst, src, bytes, kind) count_copy(cudaMemcpy(dst, src, bytes, kind), bytes, kind)
+#define SBP_COPY_ASYNC(dst, src, bytes, kind, stream) \
+  count_copy(cudaMemcpyAsync(dst, src, bytes, kind, stream), bytes, kind)
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void reserve(size_t count) {   // grow-only, contents not preserved
+    if (count <= n && p) return;
+    release();
+    SBP_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    n = std::max<size_t>(count, 1);
+  }
+};
+
+// ------------------------------------------------------------------------------------------
+// Process-wide context: one stream, the device status word, counters and readback buffers.
+// ------------------------------------------------------------------------------------------
+struct Context {
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  int* status = nullptr;                 // device error bits
+  unsigned long long* counters = nullptr;  // device counters [8]
+  double* partial = nullptr;             // MDL partial sums
+  double* scalar = nullptr;              // MDL result
+  double* mh_out = nullptr;              // MH sweep outputs [4]
+  int npartial = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  static Context& get() {
+    static Context* ctx = nullptr;
+    if (!ctx) {
+      int n = 0;
+      if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        throw Error(SBP_ERR_CUDA, "no CUDA device available (the engine has no CPU fallback)");
+      }
+      auto* c = new Context();
+      SBP_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+      int dev = 0;
+      SBP_CUDA(cudaGetDevice(&dev));
+      SBP_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
+      c->npartial = 4 * c->num_sms;
+      SBP_CUDA(cudaMalloc(&c->status, sizeof(int)));
+      SBP_CUDA(cudaMalloc(&c->counters, 8 * sizeof(unsigned long long)));
+      SBP_CUDA(cudaMalloc(&c->partial, c->npartial * sizeof(double)));
+      SBP_CUDA(cudaMalloc(&c->scalar, sizeof(double)));
+      SBP_CUDA(cudaMalloc(&c->mh_out, 4 * sizeof(double)));
+      SBP_CUDA(cudaMemset(c->status, 0, sizeof(int)));
+      SBP_CUDA(cudaEventCreate(&c->ev0));
+      SBP_CUDA(cudaEventCreate(&c->ev1));
+      ctx = c;
+    }
+    return *ctx;
+  }
+  void sync() { SBP_CUDA(cudaStreamSynchronize(stream)); }
+  // Read and clear the device status word; throw on any error bit.
+  void check_status() {
+    int st = 0;
+    SBP_CUDA(SBP_COPY_ASYNC(&st, status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    sync();
+    if (st) {
+      SBP_CUDA(cudaMemsetAsync(status, 0, sizeof(int), stream));
+      if (st & kErrReplay) throw Error(SBP_ERR_REPLAY, "replay stream shorter than the run needs");
+      char msg[160];
+      snprintf(msg, sizeof msg, "device status 0x%x (table overflow=1, multinomial walk=2, bounds=8)", st);
+      throw Error(SBP_ERR_DEVICE, msg);
+    }
+  }
+};
+
+// Optional timing of the vertex-evaluation kernel: CUDA events around every light-vertex
+// evaluation launch on the launching stream, resolved when the profile is read.
+struct EvalProfiler {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+  double ms = 0.0, bytes = 0.0;
+  long long launches = 0, visits = 0;
+  cudaEvent_t get() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    SBP_CUDA(cudaEventCreate(&e));
+    return e;
+  }
+  void resolve() {
+    for (auto& pr : pending) {
+      SBP_CUDA(cudaEventSynchronize(pr.second));
+      float t = 0.f;
+      SBP_CUDA(cudaEventElapsedTime(&t, pr.first, pr.second));
+      ms += t;
+      pool.push_back(pr.first);
+      pool.push_back(pr.second);
+    }
+    pending.clear();
+  }
+};
+static EvalProfiler g_prof;
+
+static int grid_for(long long work_items, int per_block, int max_blocks) {
+  long long g = (work_items + per_block - 1) / per_block;
+  if (g < 1) g = 1;
+  if (g > max_blocks) g = max_blocks;
+  return (int)g;
+}
+
+static int pow2_at_least(int x) {
+  int c = 1;
+  while (c < x) c <<= 1;
+  return c;
+}
+
+constexpr int kLightCap = 256;        // per-warp table slots for light vertices
+constexpr int kLightMaxK = kLightCap / 2;
+constexpr int kLightWarps = 8;
+constexpr int kMaxCap = 8192;         // largest per-warp table
+constexpr size_t kSmemBudget = 200 * 1024;
+constexpr int kSmemRebuildMaxB = 100;
+
+}  // namespace sbpb
+
+using namespace sbpb;
+
+// ------------------------------------------------------------------------------------------
+// Graph
+// ------------------------------------------------------------------------------------------
+struct BatchPlan {
+  DevBuf<int> order;                       // per batch: light vertices then heavy vertices
+  std::vector<int> light_begin, light_n, heavy_begin, heavy_n;
+  std::vector<double> light_bytes;         // algorithmic bytes of each light evaluation launch
+  int max_batch = 0;
+};
+
+struct SbpGraph {
+  int V = 0;
+  long long E = 0;
+  DevBuf<int> out_ptr, out_idx, in_ptr, in_idx, identity, high_dev;
+  DevBuf<unsigned char> self;
+  std::vector<int> h_k;        // k_out + k_in per vertex (self loop counted once, on the out side)
+  std::vector<int> high, low;  // hybrid split
+  int max_k = 0;
+  int heavy_cap = 512;         // table slots for heavy vertices
+  std::unordered_map<long long, std::unique_ptr<BatchPlan>> plans;
+
+  GraphView view() const {
+    GraphView g;
+    g.V = V;
+    g.E = E;
+    g.out_ptr = out_ptr.p;
+    g.out_idx = out_idx.p;
+    g.in_ptr = in_ptr.p;
+    g.in_idx = in_idx.p;
+    g.self = self.p;
+    return g;
+  }
+
+  int max_k_of(const std::vector<int>& verts) const {
+    int m = 0;
+    for (int v : verts) m = std::max(m, h_k[v]);
+    return m;
+  }
+
+  // Batches of asynchronous Gibbs over `list` (src/finetune.cpp:43-47, 352-366): batch_size =
+  // ceil(n / batches), loop bound n / batch_size (a trailing partial batch is skipped).
+  BatchPlan& plan(int algo, int batches) {
+    const long long key = (long long)algo * 1000003LL + batches;
+    auto it = plans.find(key);
+    if (it != plans.end()) return *it->second;
+    std::vector<int> list;
+    if (algo == SBP_ASYNC_GIBBS) {
+      list.resize(V);
+      std::iota(list.begin(), list.end(), 0);
+    } else {
+      list = low;
+    }
+    auto p = std::make_unique<BatchPlan>();
+    const int n = (int)list.size();
+    const int batch_size = (int)std::ceil(n / (double)batches);
+    std::vector<int> order;
+    order.reserve(n);
+    if (batch_size > 0) {
+      for (int bt = 0; bt < n / batch_size; ++bt) {
+        const int start = bt * batch_size, end = std::min(n, (bt + 1) * batch_size);
+        p->light_begin.push_back((int)order.size());
+        for (int i = start; i < end; ++i)
+          if (h_k[list[i]] <= kLightMaxK) order.push_back(list[i]);
+        p->light_n.push_back((int)order.size() - p->light_begin.back());
+        double lb = 0.0;   // 12 B (CSR offsets + b[v]) + 8 B per neighbour (id + block gather)
+        for (int i = p->light_begin.back(); i < (int)order.size(); ++i) lb += 12.0 + 8.0 * h_k[order[i]];
+        p->light_bytes.push_back(lb);
+        p->heavy_begin.push_back((int)order.size());
+        for (int i = start; i < end; ++i)
+          if (h_k[list[i]] > kLightMaxK) order.push_back(list[i]);
+        p->heavy_n.push_back((int)order.size() - p->heavy_begin.back());
+        p->max_batch = std::max(p->max_batch, end - start);
+      }
+    }
+    p->order.reserve(order.size());
+    if (!order.empty())
+      SBP_CUDA(SBP_COPY(p->order.p, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
+    auto& ref = *p;
+    plans[key] = std::move(p);
+    return ref;
+  }
+};
+
+// ------------------------------------------------------------------------------------------
+// Blockmodel
+// ------------------------------------------------------------------------------------------
+struct SbpBlockmodel {
+  int V = 0, B = 0, ld = 0;
+  DevBuf<int> b, M, MT, d_out, d_in, d;
+  DevBuf<int> prop, last, qr, qs, moved, n_moved;
+  float overall_entropy = 3.40282347e+38f;
+  int num_blocks_to_merge = 0;
+
+  BlockView view() {
+    BlockView v;
+    v.B = B;
+    v.ld = ld;
+    v.b = b.p;
+    v.M = M.p;
+    v.MT = MT.p;
+    v.d_out = d_out.p;
+    v.d_in = d_in.p;
+    v.d = d.p;
+    return v;
+  }
+
+  void init_vertex_scratch(int nv) {
+    Context& c = Context::get();
+    V = nv;
+    b.reserve(V);
+    prop.reserve(V);
+    qr.reserve(V);
+    qs.reserve(V);
+    moved.reserve(V);
+    n_moved.reserve(1);
+    SBP_CUDA(cudaMemsetAsync(prop.p, 0xff, sizeof(int) * V, c.stream));
+    SBP_CUDA(cudaMemsetAsync(n_moved.p, 0, sizeof(int), c.stream));
+  }
+
+  void set_blocks(int nb) {
+    Context& c = Context::get();
+    B = nb;
+    ld = ((B + 31) / 32) * 32;
+    const size_t cells = (size_t)B * (size_t)ld;
+    M.reserve(cells);
+    MT.reserve(cells);
+    d_out.reserve(B);
+    d_in.reserve(B);
+    d.reserve(B);
+    last.reserve(B);
+    SBP_CUDA(cudaMemsetAsync(last.p, 0xff, sizeof(int) * B, c.stream));
+  }
+};
+
+namespace sbpb {
+
+// Blockmodel::initialize_edge_counts (src/blockmodel/blockmodel.cpp:187-255).
+static void rebuild(SbpBlockmodel& bm, const SbpGraph& g) {
+  Context& c = Context::get();
+  const size_t cells = (size_t)bm.B * (size_t)bm.ld;
+  SBP_CUDA(cudaMemsetAsync(bm.M.p, 0, cells * sizeof(int), c.stream));
+  SBP_CUDA(cudaMemsetAsync(bm.MT.p, 0, cells * sizeof(int), c.stream));
+  SBP_CUDA(cudaMemsetAsync(bm.d_out.p, 0, bm.B * sizeof(int), c.stream));
+  SBP_CUDA(cudaMemsetAsync(bm.d_in.p, 0, bm.B * sizeof(int), c.stream));
+  if (g.V > 0) {
+    if (bm.B <= kSmemRebuildMaxB) {   // B*B ints fit the default 48 KB of shared memory
+      k_rebuild_smem<<<grid_for(g.V, 256, c.num_sms), 256, (size_t)bm.B * bm.B * sizeof(int), c.stream>>>(
+          g.view(), bm.view());
+    } else {
+      k_rebuild_global<<<grid_for(g.V, 256, 8 * c.num_sms), 256, 0, c.stream>>>(g.view(), bm.view());
+    }
+    SBP_CHECK_LAUNCH();
+  }
+  k_rebuild_degrees<<<grid_for(bm.B, 256, 1 << 20), 256, 0, c.stream>>>(bm.view());
+  SBP_CHECK_LAUNCH();
+}
+
+// entropy::mdl (src/entropy.cpp:584-589).
+static double mdl(SbpBlockmodel& bm, const SbpGraph& g) {
+  Context& c = Context::get();
+  const int grid = c.npartial;
+  if ((long long)bm.B * bm.B <= 4LL * g.E) k_mdl_cells<<<grid, 256, 0, c.stream>>>(bm.view(), c.partial);
+  else k_mdl_edges<<<grid, 256, 0, c.stream>>>(g.view(), bm.view(), c.partial);
+  SBP_CHECK_LAUNCH();
+  k_mdl_final<<<1, 32, 0, c.stream>>>(c.partial, grid, g.V, g.E, bm.B, c.scalar);
+  SBP_CHECK_LAUNCH();
+  double out = 0.0;
+  SBP_CUDA(SBP_COPY_ASYNC(&out, c.scalar, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  return out;
+}
+
+// finetune::early_stop (src/finetune.cpp:144-162).
+static bool early_stop(int iteration, bool bracket, double initial_entropy, const std::vector<double>& deltas) {
+  const size_t last = deltas.size() - 1;
+  if (deltas[last] == 0.0) return true;
+  if (iteration < 3) return false;
+  double average = deltas[last] + deltas[last - 1] + deltas[last - 2];
+  average /= -3.0;
+  const double threshold = bracket ? 1e-4 * initial_entropy : 5e-4 * initial_entropy;
+  return average < threshold;
+}
+
+struct MhResult {
+  long long visits = 0, moved = 0, accepted = 0;
+  double sum_dS = 0.0;
+};
+
+static int mh_cap(int max_k) {
+  int cap = pow2_at_least(std::max(2 * max_k, kLightCap));
+  if (cap > kMaxCap) throw Error(SBP_ERR_UNSUPPORTED, "vertex degree too large for the Metropolis-Hastings kernel");
+  return cap;
+}
+
+static void set_smem_limit(const void* fn, size_t bytes) {
+  SBP_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+// One sequential Metropolis-Hastings pass over verts (device list of n vertices).
+static MhResult mh_pass(SbpBlockmodel& bm, const SbpGraph& g, const int* verts, int n, int max_k, RngParams rng,
+                        int sweep) {
+  Context& c = Context::get();
+  MhResult res;
+  if (n == 0) return res;
+  const int cap = mh_cap(max_k);
+  const size_t per_warp = (size_t)table_ints(cap) * sizeof(int);
+  int W = (int)std::min<size_t>(16, kSmemBudget / per_warp);
+  if (W < 1) throw Error(SBP_ERR_UNSUPPORTED, "vertex degree too large for the Metropolis-Hastings kernel");
+  const size_t smem = per_warp * W;
+  set_smem_limit((const void*)k_mh, smem);
+  k_mh<<<1, W * 32, smem, c.stream>>>(g.view(), bm.view(), verts, n, rng, sweep, cap, c.mh_out, c.status);
+  SBP_CHECK_LAUNCH();
+  double out[4];
+  SBP_CUDA(SBP_COPY_ASYNC(out, c.mh_out, sizeof(out), cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  res.visits = (long long)out[0];
+  res.moved = (long long)out[1];
+  res.accepted = (long long)out[2];
+  res.sum_dS = out[3];
+  return res;
+}
+
+// One asynchronous-Gibbs batch: evaluate (light + heavy vertices), then apply.
+static void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, int bt, RngParams rng,
+                        int sweep) {
+  Context& c = Context::get();
+  const int nl = plan.light_n[bt], nh = plan.heavy_n[bt];
+  if (nl > 0) {
+    const size_t smem = (size_t)table_ints(kLightCap) * sizeof(int) * kLightWarps;
+    const int grid = grid_for(nl, kLightWarps, 64 * c.num_sms);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (g_prof.on) {
+      e0 = g_prof.get();
+      e1 = g_prof.get();
+      SBP_CUDA(cudaEventRecord(e0, c.stream));
+    }
+    k_gibbs_eval<<<grid, kLightWarps * 32, smem, c.stream>>>(g.view(), bm.view(), plan.order.p + plan.light_begin[bt],
+                                                            nl, rng, sweep, bm.prop.p, bm.moved.p, bm.n_moved.p,
+                                                            c.counters, kLightCap, c.status);
+    SBP_CHECK_LAUNCH();
+    if (g_prof.on) {
+      SBP_CUDA(cudaEventRecord(e1, c.stream));
+      g_prof.pending.push_back({e0, e1});
+      g_prof.launches++;
+      g_prof.visits += nl;
+      g_prof.bytes += plan.light_bytes[bt];
+    }
+  }
+  if (nh > 0) {
+    const size_t smem = (size_t)table_ints(g.heavy_cap) * sizeof(int);
+    set_smem_limit((const void*)k_gibbs_eval, std::max(smem, (size_t)table_ints(kLightCap) * sizeof(int) * kLightWarps));
+    k_gibbs_eval<<<grid_for(nh, 1, 64 * c.num_sms), 32, smem, c.stream>>>(
+        g.view(), bm.view(), plan.order.p + plan.heavy_begin[bt], nh, rng, sweep, bm.prop.p, bm.moved.p,
+        bm.n_moved.p, c.counters, g.heavy_cap, c.status);
+    SBP_CHECK_LAUNCH();
+  }
+  const int batch = nl + nh;
+  const int gw = grid_for((long long)batch * 32, 256, 64 * c.num_sms);
+  k_apply_edges<<<gw, 256, 0, c.stream>>>(g.view(), bm.view(), bm.moved.p, bm.n_moved.p, bm.prop.p, bm.qr.p, bm.qs.p,
+                                          bm.last.p);
+  SBP_CHECK_LAUNCH();
+  const int gt = grid_for(batch, 256, 64 * c.num_sms);
+  k_apply_degrees<<<gt, 256, 0, c.stream>>>(bm.view(), bm.moved.p, bm.n_moved.p, bm.prop.p, bm.qr.p, bm.qs.p,
+                                            bm.last.p);
+  SBP_CHECK_LAUNCH();
+  k_apply_finish<<<gt, 256, 0, c.stream>>>(bm.view(), bm.moved.p, bm.n_moved.p, bm.prop.p, bm.last.p);
+  SBP_CHECK_LAUNCH();
+  SBP_CUDA(cudaMemsetAsync(bm.n_moved.p, 0, sizeof(int), c.stream));
+}
+
+struct ReplayDev {
+  DevBuf<uint4> buf;
+  long long records = 0;
+  void upload(const SbpReplay* r) {
+    if (!r || !r->words || r->records <= 0) return;
+    buf.reserve((size_t)r->records);
+    SBP_CUDA(SBP_COPY(buf.p, r->words, (size_t)r->records * sizeof(uint4), cudaMemcpyHostToDevice));
+    records = r->records;
+  }
+};
+
+// finetune::{metropolis_hastings, asynchronous_gibbs, hybrid_mcmc}.
+static void finetune(SbpBlockmodel& bm, SbpGraph& g, int algo, const SbpFinetuneOptions& opt, const SbpReplay* replay,
+                     SbpStats& st) {
+  Context& c = Context::get();
+  std::memset(&st, 0, sizeof st);
+  st.num_blocks = bm.B;
+  if (algo < 0 || algo > 2) throw Error(SBP_ERR_INVALID_ARGUMENT, "unknown finetune algorithm");
+  if (opt.batches <= 0 && algo != SBP_METROPOLIS_HASTINGS) throw Error(SBP_ERR_INVALID_ARGUMENT, "batches must be >= 1");
+  if (bm.B == 1) {   // src/finetune.cpp:33-35: nothing to do, entropy left as it was
+    st.mdl = bm.overall_entropy;
+    return;
+  }
+  SBP_CUDA(cudaEventRecord(c.ev0, c.stream));
+  ReplayDev rp;
+  rp.upload(replay);
+  RngParams rng;
+  rng.seed = opt.seed;
+  rng.replay = rp.records ? rp.buf.p : nullptr;
+  rng.replay_records = rp.records;
+  rng.call = opt.call;
+  const int max_sweeps = (opt.max_sweeps <= 0 || opt.max_sweeps > kMaxIterations) ? kMaxIterations : opt.max_sweeps;
+  const bool bracket = opt.bracket_established != 0;
+  SBP_CUDA(cudaMemsetAsync(c.counters, 0, 8 * sizeof(unsigned long long), c.stream));
+  bm.overall_entropy = (float)mdl(bm, g);
+  const double initial_entropy = bm.overall_entropy;
+  std::vector<double> deltas;
+  long long mh_visits = 0, mh_moved = 0, mh_acc = 0;
+  const BatchPlan* plan = nullptr;
+  if (algo != SBP_METROPOLIS_HASTINGS) plan = &g.plan(algo, opt.batches);
+  for (int it = 0; it < max_sweeps; ++it) {
+    if (algo == SBP_METROPOLIS_HASTINGS) {
+      const MhResult r = mh_pass(bm, g, g.identity.p, g.V, g.max_k, rng, it);
+      mh_visits += r.visits;
+      mh_moved += r.moved;
+      mh_acc += r.accepted;
+      deltas.push_back(r.sum_dS);
+      st.sweeps++;
+      c.check_status();
+      if (early_stop(it, bracket, (double)bm.overall_entropy, deltas)) break;
+    } else {
+      if (algo == SBP_HYBRID_MCMC && !g.high.empty()) {
+        const MhResult r = mh_pass(bm, g, g.high_dev.p, (int)g.high.size(), g.max_k_of(g.high), rng, it);
+        mh_visits += r.visits;
+        mh_moved += r.moved;
+        mh_acc += r.accepted;
+      }
+      for (size_t bt = 0; bt < plan->light_n.size(); ++bt) gibbs_batch(bm, g, *plan, (int)bt, rng, it);
+      const double entropy = mdl(bm, g);
+      deltas.push_back(entropy - initial_entropy);   // last_iteration_entropy is never updated
+      st.sweeps++;
+      c.check_status();
+      if (early_stop(it, bracket, initial_entropy, deltas)) break;
+    }
+  }
+  bm.overall_entropy = (float)mdl(bm, g);
+  unsigned long long cnt[8];
+  SBP_CUDA(SBP_COPY_ASYNC(cnt, c.counters, sizeof cnt, cudaMemcpyDeviceToHost, c.stream));
+  SBP_CUDA(cudaEventRecord(c.ev1, c.stream));
+  c.sync();
+  c.check_status();
+  float ms = 0.f;
+  SBP_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+  st.visits = (long long)cnt[0] + mh_visits;
+  st.proposals_moved = (long long)cnt[1] + mh_moved;
+  st.accepted = (long long)cnt[2] + mh_acc;
+  st.mdl = bm.overall_entropy;
+  st.mcmc_seconds = ms * 1e-3;
+  st.num_blocks = bm.B;
+}
+
+// ------------------------------------------------------------------------------------------
+// Block merge
+// ------------------------------------------------------------------------------------------
+struct MergeScratch {
+  DevBuf<int> rcnt, rptr, ridx, rval, ccnt, cptr, cidx, cval, best_s, sizes, map;
+  DevBuf<double> best_dS;
+};
+
+// block_merge::carry_out_best_merges_advanced (src/block_merge.cpp:123-217) on a host copy
+// of the sparse matrix (serial by construction); heap order (dS, block).
+static void carry_out_advanced(int B, int to_merge, const std::vector<int>& rptr, const std::vector<int>& ridx,
+                               const std::vector<int>& rval, std::vector<int> d_out, std::vector<int> d_in,
+                               const std::vector<double>& dS, const std::vector<int>& best, std::vector<int>& block_map) {
+  std::vector<std::unordered_map<int, int>> rows(B), cols(B);
+  for (int r = 0; r < B; ++r)
+    for (int j = rptr[r]; j < rptr[r + 1]; ++j) {
+      rows[r][ridx[j]] = rval[j];
+      cols[ridx[j]][r] = rval[j];
+    }
+  auto get = [&](int r, int c) {
+    auto it = rows[r].find(c);
+    return it == rows[r].end() ? 0 : it->second;
+  };
+  auto g = [](double x) { return x > 0 ? x * std::log(x) : 0.0; };
+  // closed-form merge delta (matches entropy::block_merge_delta_mdl)
+  auto delta = [&](int r, int s) {
+    double v = 0.0;
+    for (auto& kv : rows[r]) {
+      v += g(kv.second);
+      if (kv.first != r && kv.first != s) {
+        const double m = get(s, kv.first);
+        v += g(m) - g(m + kv.second);
+      }
+    }
+    for (auto& kv : cols[r]) {
+      if (kv.first == r) continue;
+      v += g(kv.second);
+      if (kv.first != s) {
+        const double m = get(kv.first, s);
+        v += g(m) - g(m + kv.second);
+      }
+    }
+    const double mss = get(s, s);
+    v += g(mss) - g(mss + get(r, r) + get(r, s) + get(s, r));
+    v -= g(d_out[r]) + g(d_out[s]) - g((double)d_out[r] + d_out[s]);
+    v -= g(d_in[r]) + g(d_in[s]) - g((double)d_in[r] + d_in[s]);
+    return v;
+  };
+  struct Item {
+    int from, to;
+    double dS;
+  };
+  auto cmp = [](const Item& a, const Item& b) {   // min-heap on (dS, from)
+    if (a.dS != b.dS) return a.dS > b.dS;
+    return a.from > b.from;
+  };
+  std::vector<Item> heap;
+  for (int i = 0; i < B; ++i) heap.push_back({i, best[i], dS[i]});
+  std::make_heap(heap.begin(), heap.end(), cmp);
+  block_map.resize(B);
+  std::iota(block_map.begin(), block_map.end(), 0);
+  int merged = 0;
+  while (merged < to_merge && !heap.empty()) {
+    std::pop_heap(heap.begin(), heap.end(), cmp);
+    Item m = heap.back();
+    heap.pop_back();
+    if (m.to < 0) continue;
+    const int from = m.from, to = block_map[m.to];
+    if (from == to) continue;
+    const double actual = delta(from, to);
+    if (!heap.empty() && actual > heap.front().dS) {
+      m.dS = actual;
+      heap.push_back(m);
+      std::push_heap(heap.begin(), heap.end(), cmp);
+      continue;
+    }
+    for (int i = 0; i < B; ++i)
+      if (block_map[i] == from) block_map[i] = to;
+    // move row/col `from` into `to`
+    std::vector<std::pair<int, int>> rf(rows[from].begin(), rows[from].end());
+    std::vector<std::pair<int, int>> cf(cols[from].begin(), cols[from].end());
+    auto add = [&](int r, int c, int v) {
+      if (!v) return;
+      int& x = rows[r][c];
+      x += v;
+      cols[c][r] = x;
+      if (x == 0) {
+        rows[r].erase(c);
+        cols[c].erase(r);
+      }
+    };
+    for (auto& kv : rf) {
+      add(from, kv.first, -kv.second);
+      add(to, (kv.first == from || kv.first == to) ? to : kv.first, kv.second);
+    }
+    for (auto& kv : cf) {
+      if (kv.first == from) continue;
+      add(kv.first, from, -kv.second);
+      add(kv.first == to ? to : kv.first, to, kv.second);
+    }
+    d_out[to] += d_out[from];
+    d_out[from] = 0;
+    d_in[to] += d_in[from];
+    d_in[from] = 0;
+    merged++;
+  }
+}
+
+static void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& opt, const SbpReplay* replay,
+                         int* best_out, double* dS_out, SbpStats& st) {
+  Context& c = Context::get();
+  const int B = bm.B;
+  if (B < 2) throw Error(SBP_ERR_INVALID_ARGUMENT, "block merge needs at least two blocks");
+  SBP_CUDA(cudaEventRecord(c.ev0, c.stream));
+  MergeScratch ms;
+  ReplayDev rp;
+  rp.upload(replay);
+  // compressed rows of M and of MT (outgoing_edges / incoming_edges views)
+  ms.rcnt.reserve(B);
+  ms.ccnt.reserve(B);
+  ms.rptr.reserve(B + 1);
+  ms.cptr.reserve(B + 1);
+  const int gw = grid_for((long long)B * 32, 256, 64 * c.num_sms);
+  k_row_nnz<<<gw, 256, 0, c.stream>>>(bm.M.p, B, bm.ld, ms.rcnt.p);
+  k_row_nnz<<<gw, 256, 0, c.stream>>>(bm.MT.p, B, bm.ld, ms.ccnt.p);
+  k_excl_scan<<<1, 1024, 0, c.stream>>>(ms.rcnt.p, ms.rptr.p, B);
+  k_excl_scan<<<1, 1024, 0, c.stream>>>(ms.ccnt.p, ms.cptr.p, B);
+  SBP_CHECK_LAUNCH();
+  int nnz[2];
+  SBP_CUDA(SBP_COPY_ASYNC(&nnz[0], ms.rptr.p + B, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(&nnz[1], ms.cptr.p + B, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  ms.ridx.reserve(nnz[0]);
+  ms.rval.reserve(nnz[0]);
+  ms.cidx.reserve(nnz[1]);
+  ms.cval.reserve(nnz[1]);
+  k_row_fill<<<gw, 256, 0, c.stream>>>(bm.M.p, B, bm.ld, ms.rptr.p, ms.ridx.p, ms.rval.p);
+  k_row_fill<<<gw, 256, 0, c.stream>>>(bm.MT.p, B, bm.ld, ms.cptr.p, ms.cidx.p, ms.cval.p);
+  SBP_CHECK_LAUNCH();
+  RngParams rng;
+  rng.seed = opt.seed;
+  rng.replay = rp.records ? rp.buf.p : nullptr;
+  rng.replay_records = rp.records;
+  rng.call = opt.call;
+  ms.best_s.reserve(B);
+  ms.best_dS.reserve(B);
+  SBP_CUDA(cudaMemsetAsync(c.counters, 0, 8 * sizeof(unsigned long long), c.stream));
+  Csr rows{ms.rptr.p, ms.ridx.p, ms.rval.p}, cols{ms.cptr.p, ms.cidx.p, ms.cval.p};
+  k_merge_propose<<<gw, 256, 0, c.stream>>>(bm.view(), rows, cols, rng, ms.best_s.p, ms.best_dS.p, c.counters,
+                                            c.status);
+  SBP_CHECK_LAUNCH();
+  ms.sizes.reserve(B);
+  SBP_CUDA(cudaMemsetAsync(ms.sizes.p, 0, B * sizeof(int), c.stream));
+  k_block_sizes<<<grid_for(bm.V, 256, 8 * c.num_sms), 256, 0, c.stream>>>(bm.b.p, bm.V, ms.sizes.p);
+  SBP_CHECK_LAUNCH();
+  std::vector<int> best(B), sizes(B);
+  std::vector<double> dS(B);
+  unsigned long long cnt[8];
+  SBP_CUDA(SBP_COPY_ASYNC(best.data(), ms.best_s.p, B * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(dS.data(), ms.best_dS.p, B * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(sizes.data(), ms.sizes.p, B * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(cnt, c.counters, sizeof cnt, cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  c.check_status();
+  st.merge_proposals += (long long)cnt[0];
+  st.merge_avoided += (long long)cnt[1];
+  if (best_out) std::memcpy(best_out, best.data(), B * sizeof(int));
+  if (dS_out) std::memcpy(dS_out, dS.data(), B * sizeof(double));
+
+  std::vector<int> block_map(B);
+  const int to_merge = bm.num_blocks_to_merge;
+  if (opt.approximate) {
+    // Blockmodel::carry_out_best_merges (src/blockmodel/blockmodel.cpp:50-78); sort ties by index
+    std::vector<int> order(B);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b2) { return dS[a] < dS[b2]; });
+    std::iota(block_map.begin(), block_map.end(), 0);
+    int merged = 0, counter = 0;
+    while (merged < to_merge) {
+      if (counter >= B) throw Error(SBP_ERR_DEVICE, "not enough mergeable blocks for num_blocks_to_merge");
+      const int from = order[counter++];
+      if (best[from] < 0) continue;
+      const int to = block_map[best[from]];
+      if (to != from) {
+        for (int i = 0; i < B; ++i)
+          if (block_map[i] == from) block_map[i] = to;
+        merged++;
+      }
+    }
+  } else {
+    std::vector<int> rptr(B + 1), ridx(nnz[0]), rval(nnz[0]), dout(B), din(B);
+    SBP_CUDA(SBP_COPY_ASYNC(rptr.data(), ms.rptr.p, (B + 1) * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    SBP_CUDA(SBP_COPY_ASYNC(ridx.data(), ms.ridx.p, nnz[0] * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    SBP_CUDA(SBP_COPY_ASYNC(rval.data(), ms.rval.p, nnz[0] * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    SBP_CUDA(SBP_COPY_ASYNC(dout.data(), bm.d_out.p, B * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    SBP_CUDA(SBP_COPY_ASYNC(din.data(), bm.d_in.p, B * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    carry_out_advanced(B, to_merge, rptr, ridx, rval, dout, din, dS, best, block_map);
+  }
+  // Blockmodel::build_mapping over the labels the vertices carry, then relabel
+  std::vector<char> present(B, 0);
+  for (int x = 0; x < B; ++x)
+    if (sizes[x] > 0) present[block_map[x]] = 1;
+  std::vector<int> rank(B, -1), map(B, 0);
+  int counter = 0;
+  for (int x = 0; x < B; ++x)
+    if (present[x]) rank[x] = counter++;
+  for (int x = 0; x < B; ++x) map[x] = sizes[x] > 0 ? rank[block_map[x]] : 0;
+  ms.map.reserve(B);
+  SBP_CUDA(SBP_COPY_ASYNC(ms.map.p, map.data(), B * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  k_relabel<<<grid_for(bm.V, 256, 8 * c.num_sms), 256, 0, c.stream>>>(bm.b.p, bm.V, ms.map.p);
+  SBP_CHECK_LAUNCH();
+  c.sync();   // host vectors above must outlive the async copy
+  bm.set_blocks(B - to_merge);
+  rebuild(bm, g);
+  SBP_CUDA(cudaEventRecord(c.ev1, c.stream));
+  c.sync();
+  float ms_time = 0.f;
+  SBP_CUDA(cudaEventElapsedTime(&ms_time, c.ev0, c.ev1));
+  st.merge_seconds += ms_time * 1e-3;
+  st.num_blocks = bm.B;
+}
+
+// ------------------------------------------------------------------------------------------
+// Golden-section triplet over B (src/blockmodel/blockmodel_triplet.cpp:3-100) holding
+// host copies of the assignment; a restored blockmodel is rebuilt on the device.
+// ------------------------------------------------------------------------------------------
+struct Snapshot {
+  bool empty = true;
+  std::vector<int> b;
+  int B = 0;
+  float entropy = 0.f;
+};
+
+struct Triplet {
+  Snapshot s[3];
+  bool optimal = false;
+  void update(const Snapshot& x) {
+    int index;
+    if (s[1].empty) index = 1;
+    else if (x.entropy <= s[1].entropy) {
+      const int old_index = (s[1].B > x.B) ? 0 : 2;
+      s[old_index] = s[1];
+      index = 1;
+    } else index = (s[1].B > x.B) ? 2 : 0;
+    s[index] = x;
+  }
+  // returns the snapshot to continue from and its num_blocks_to_merge
+  Snapshot next(const Snapshot& old, int* to_merge) {
+    update(old);
+    if (s[2].empty) {
+      Snapshot r = s[1];
+      *to_merge = (int)(r.B * 0.5);
+      if (*to_merge == 0) optimal = true;
+      return r;
+    }
+    if ((!s[0].empty && s[0].B - s[2].B == 2) || (s[0].empty && s[1].B - s[2].B == 1)) optimal = true;
+    if (optimal) {
+      *to_merge = 0;
+      return s[1];
+    }
+    int index;
+    if (s[0].empty && s[1].B > s[2].B) index = 1;
+    else if ((s[0].B - s[1].B) >= (s[1].B - s[2].B)) index = 0;
+    else index = 1;
+    int next_b = s[index + 1].B;
+    next_b += (int)((s[index].B - s[index + 1].B) * 0.618);
+    *to_merge = s[index].B - next_b;
+    return s[index];
+  }
+};
+
+static Snapshot snapshot(SbpBlockmodel& bm) {
+  Context& c = Context::get();
+  Snapshot x;
+  x.empty = false;
+  x.B = bm.B;
+  x.entropy = bm.overall_entropy;
+  x.b.resize(bm.V);
+  SBP_CUDA(SBP_COPY_ASYNC(x.b.data(), bm.b.p, bm.V * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  return x;
+}
+
+static void restore(SbpBlockmodel& bm, SbpGraph& g, const Snapshot& x) {
+  Context& c = Context::get();
+  SBP_CUDA(SBP_COPY_ASYNC(bm.b.p, x.b.data(), bm.V * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  bm.set_blocks(x.B);
+  bm.overall_entropy = x.entropy;
+  rebuild(bm, g);
+  c.sync();
+}
+
+// sbp::stochastic_block_partition (src/sbp.cpp:61-98).
+static void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st) {
+  Context& c = Context::get();
+  std::memset(&st, 0, sizeof st);
+  cudaEvent_t t0, t1;
+  SBP_CUDA(cudaEventCreate(&t0));
+  SBP_CUDA(cudaEventCreate(&t1));
+  SBP_CUDA(cudaEventRecord(t0, c.stream));
+  SbpBlockmodel bm;
+  bm.init_vertex_scratch(g.V);
+  std::vector<int> ident(g.V);
+  std::iota(ident.begin(), ident.end(), 0);
+  SBP_CUDA(SBP_COPY_ASYNC(bm.b.p, ident.data(), g.V * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  bm.set_blocks(g.V);
+  bm.num_blocks_to_merge = (int)(g.V * 0.5f);
+  rebuild(bm, g);
+  c.sync();
+  Triplet t;
+  float iteration = 0;
+  uint32_t call = 0;
+  while (!t.optimal) {
+    SbpMergeOptions mo;
+    mo.approximate = opt.approximate;
+    mo.call = call;
+    mo.seed = opt.seed;
+    merge_blocks(bm, g, mo, nullptr, nullptr, nullptr, st);
+    int algo = opt.algorithm;
+    if (algo == SBP_ASYNC_GIBBS && !(iteration < (float)opt.asynciterations)) algo = SBP_METROPOLIS_HASTINGS;
+    SbpFinetuneOptions fo;
+    fo.batches = opt.batches;
+    fo.bracket_established = !t.s[2].empty;
+    fo.max_sweeps = 0;
+    fo.call = call;
+    fo.seed = opt.seed;
+    SbpStats fs;
+    finetune(bm, g, algo, fo, nullptr, fs);
+    st.visits += fs.visits;
+    st.proposals_moved += fs.proposals_moved;
+    st.accepted += fs.accepted;
+    st.sweeps += fs.sweeps;
+    st.mcmc_seconds += fs.mcmc_seconds;
+    ++iteration;
+    ++call;
+    st.outer_iterations++;
+    int to_merge = 0;
+    const Snapshot nxt = t.next(snapshot(bm), &to_merge);
+    if (t.optimal) {
+      std::memcpy(out, nxt.b.data(), g.V * sizeof(int));
+      st.mdl = nxt.entropy;
+      st.num_blocks = nxt.B;
+      break;
+    }
+    restore(bm, g, nxt);
+    bm.num_blocks_to_merge = to_merge;
+  }
+  SBP_CUDA(cudaEventRecord(t1, c.stream));
+  c.sync();
+  float ms = 0.f;
+  SBP_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+  st.total_seconds = ms * 1e-3;
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+}
+
+}  // namespace sbpb
+
+// ------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------
+#define SBP_API_BEGIN try {
+#define SBP_API_END                                        \
+  return SBP_OK;                                           \
+  }                                                        \
+  catch (const Error& e) {                                 \
+    g_last_error = e.what();                               \
+    return e.code;                                         \
+  }                                                        \
+  catch (const std::bad_alloc&) {                          \
+    g_last_error = "host allocation failed";               \
+    return SBP_ERR_OUT_OF_MEMORY;                          \
+  }                                                        \
+  catch (const std::exception& e) {                        \
+    g_last_error = e.what();                               \
+    return SBP_ERR_CUDA;                                   \
+  }
+
+#define SBP_REQUIRE(cond, msg) \
+  if (!(cond)) throw Error(SBP_ERR_INVALID_ARGUMENT, msg)
+
+extern "C" {
+
+const char* sbp_last_error(void) { return g_last_error.c_str(); }
+
+int32_t sbp_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+SbpStatus sbp_get_stream(void** out) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(out, "out is NULL");
+  *out = (void*)Context::get().stream;
+  SBP_API_END
+}
+
+SbpStatus sbp_profile_enable(int32_t on) {
+  SBP_API_BEGIN
+  Context::get();
+  g_prof.on = on != 0;
+  SBP_API_END
+}
+
+SbpStatus sbp_profile_read(SbpProfile* out, int32_t reset) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(out, "out is NULL");
+  g_prof.resolve();
+  out->launches = g_launches;
+  out->eval_launches = g_prof.launches;
+  out->eval_visits = g_prof.visits;
+  out->eval_ms = g_prof.ms;
+  out->eval_bytes = g_prof.bytes;
+  out->h2d_bytes = g_h2d;
+  out->d2h_bytes = g_d2h;
+  if (reset) {
+    g_prof.launches = g_prof.visits = 0;
+    g_prof.ms = g_prof.bytes = 0.0;
+  }
+  SBP_API_END
+}
+
+SbpStatus sbp_graph_create(int32_t V, int64_t n, const int32_t* src, const int32_t* dst, SbpGraph** out) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(out, "out is NULL");
+  *out = nullptr;
+  SBP_REQUIRE(V > 0, "num_vertices must be positive");
+  SBP_REQUIRE(n >= 0 && (n == 0 || (src && dst)), "edge arrays are NULL");
+  Context& c = Context::get();
+  for (int64_t i = 0; i < n; ++i)
+    SBP_REQUIRE(src[i] >= 0 && src[i] < V && dst[i] >= 0 && dst[i] < V, "edge endpoint out of range");
+  // utils::insert_nodup: keep the first occurrence of each (src, dst)
+  uint64_t cap = 16;
+  while (cap < (uint64_t)(2 * n + 16)) cap <<= 1;
+  std::vector<uint64_t> table(cap, ~0ull);
+  std::vector<int> ks, kd;
+  ks.reserve(n);
+  kd.reserve(n);
+  int shift = 64;
+  for (uint64_t x = cap; x > 1; x >>= 1) --shift;
+  for (int64_t i = 0; i < n; ++i) {
+    const uint64_t key = (uint64_t)(uint32_t)src[i] * (uint64_t)V + (uint64_t)(uint32_t)dst[i];
+    uint64_t h = (key * 0x9E3779B97F4A7C15ull) >> shift;
+    bool dup = false;
+    while (table[h] != ~0ull) {
+      if (table[h] == key) {
+        dup = true;
+        break;
+      }
+      h = (h + 1) & (cap - 1);
+    }
+    if (dup) continue;
+    table[h] = key;
+    ks.push_back(src[i]);
+    kd.push_back(dst[i]);
+  }
+  std::vector<uint64_t>().swap(table);
+  auto g = std::make_unique<SbpGraph>();
+  g->V = V;
+  g->E = (long long)ks.size();
+  const size_t m = ks.size();
+  std::vector<int> op(V + 1, 0), ip(V + 1, 0), oi(m), ii(m);
+  std::vector<unsigned char> self(V, 0);
+  for (size_t i = 0; i < m; ++i) {
+    op[ks[i] + 1]++;
+    if (ks[i] == kd[i]) self[ks[i]] = 1;
+    else ip[kd[i] + 1]++;
+  }
+  for (int v = 0; v < V; ++v) {
+    op[v + 1] += op[v];
+    ip[v + 1] += ip[v];
+  }
+  {
+    std::vector<int> fo(op.begin(), op.end() - 1), fi(ip.begin(), ip.end() - 1);
+    for (size_t i = 0; i < m; ++i) {
+      oi[fo[ks[i]]++] = kd[i];
+      if (ks[i] != kd[i]) ii[fi[kd[i]]++] = ks[i];
+    }
+  }
+  g->h_k.resize(V);
+  for (int v = 0; v < V; ++v) {
+    g->h_k[v] = (op[v + 1] - op[v]) + (ip[v + 1] - ip[v]);
+    g->max_k = std::max(g->max_k, g->h_k[v]);
+  }
+  g->heavy_cap = std::max(512, pow2_at_least(2 * g->max_k));
+  if (g->heavy_cap > kMaxCap) {
+    if (V <= kMaxCap) g->heavy_cap = kMaxCap;   // distinct neighbour blocks <= B <= V
+    else throw Error(SBP_ERR_UNSUPPORTED, "vertex degree above 4096 is not supported");
+  }
+  // Graph::sort_vertices: degree = out + in - self, descending; ties by vertex id
+  std::vector<int> ord(V);
+  std::iota(ord.begin(), ord.end(), 0);
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return g->h_k[a] > g->h_k[b]; });
+  for (int i = 0; i < V; ++i) {
+    if ((double)i < 0.15 * (double)V) g->high.push_back(ord[i]);
+    else g->low.push_back(ord[i]);
+  }
+  g->out_ptr.reserve(V + 1);
+  g->in_ptr.reserve(V + 1);
+  g->out_idx.reserve(m);
+  g->in_idx.reserve(m);
+  g->self.reserve(V);
+  g->identity.reserve(V);
+  g->high_dev.reserve(g->high.size());
+  SBP_CUDA(SBP_COPY(g->out_ptr.p, op.data(), (V + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  SBP_CUDA(SBP_COPY(g->in_ptr.p, ip.data(), (V + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  if (m) {
+    SBP_CUDA(SBP_COPY(g->out_idx.p, oi.data(), m * sizeof(int), cudaMemcpyHostToDevice));
+    if (ip[V]) SBP_CUDA(SBP_COPY(g->in_idx.p, ii.data(), ip[V] * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  SBP_CUDA(SBP_COPY(g->self.p, self.data(), V, cudaMemcpyHostToDevice));
+  std::vector<int> ident(V);
+  std::iota(ident.begin(), ident.end(), 0);
+  SBP_CUDA(SBP_COPY(g->identity.p, ident.data(), V * sizeof(int), cudaMemcpyHostToDevice));
+  if (!g->high.empty())
+    SBP_CUDA(SBP_COPY(g->high_dev.p, g->high.data(), g->high.size() * sizeof(int), cudaMemcpyHostToDevice));
+  (void)c;
+  *out = g.release();
+  SBP_API_END
+}
+
+SbpStatus sbp_graph_destroy(SbpGraph* g) {
+  SBP_API_BEGIN
+  delete g;
+  SBP_API_END
+}
+
+SbpStatus sbp_graph_num_edges(const SbpGraph* g, int64_t* out) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(g && out, "NULL argument");
+  *out = g->E;
+  SBP_API_END
+}
+
+SbpStatus sbp_graph_get_split(const SbpGraph* g, int32_t* num_high, int32_t* high, int32_t* low) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(g && num_high, "NULL argument");
+  *num_high = (int32_t)g->high.size();
+  if (high) std::memcpy(high, g->high.data(), g->high.size() * sizeof(int));
+  if (low) std::memcpy(low, g->low.data(), g->low.size() * sizeof(int));
+  SBP_API_END
+}
+
+SbpStatus sbp_graph_set_split(SbpGraph* g, int32_t nh, const int32_t* high, int32_t nl, const int32_t* low) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(g, "NULL graph");
+  SBP_REQUIRE(nh >= 0 && nl >= 0 && nh + nl == g->V, "split must cover every vertex once");
+  std::vector<char> seen(g->V, 0);
+  for (int i = 0; i < nh; ++i) {
+    SBP_REQUIRE(high[i] >= 0 && high[i] < g->V && !seen[high[i]], "bad vertex in split");
+    seen[high[i]] = 1;
+  }
+  for (int i = 0; i < nl; ++i) {
+    SBP_REQUIRE(low[i] >= 0 && low[i] < g->V && !seen[low[i]], "bad vertex in split");
+    seen[low[i]] = 1;
+  }
+  g->high.assign(high, high + nh);
+  g->low.assign(low, low + nl);
+  g->plans.clear();
+  g->high_dev.reserve(std::max(nh, 1));
+  if (nh) SBP_CUDA(SBP_COPY(g->high_dev.p, high, nh * sizeof(int), cudaMemcpyHostToDevice));
+  SBP_API_END
+}
+
+SbpStatus sbp_blockmodel_create(const SbpGraph* g, int32_t B, const int32_t* assignment, SbpBlockmodel** out) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(g && assignment && out, "NULL argument");
+  *out = nullptr;
+  SBP_REQUIRE(B >= 1 && B <= g->V, "num_blocks must be in [1, V]");
+  for (int v = 0; v < g->V; ++v) SBP_REQUIRE(assignment[v] >= 0 && assignment[v] < B, "block id out of range");
+  Context& c = Context::get();
+  auto bm = std::make_unique<SbpBlockmodel>();
+  bm->init_vertex_scratch(g->V);
+  SBP_CUDA(SBP_COPY_ASYNC(bm->b.p, assignment, g->V * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  bm->set_blocks(B);
+  bm->num_blocks_to_merge = (int)(B * 0.5f);
+  rebuild(*bm, *g);
+  c.sync();
+  *out = bm.release();
+  SBP_API_END
+}
+
+SbpStatus sbp_blockmodel_copy(const SbpBlockmodel* src, SbpBlockmodel** out) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(src && out, "NULL argument");
+  Context& c = Context::get();
+  auto bm = std::make_unique<SbpBlockmodel>();
+  bm->init_vertex_scratch(src->V);
+  bm->set_blocks(src->B);
+  const size_t cells = (size_t)src->B * src->ld;
+  SBP_CUDA(SBP_COPY_ASYNC(bm->b.p, src->b.p, src->V * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(bm->M.p, src->M.p, cells * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(bm->MT.p, src->MT.p, cells * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(bm->d_out.p, src->d_out.p, src->B * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(bm->d_in.p, src->d_in.p, src->B * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(bm->d.p, src->d.p, src->B * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+  bm->overall_entropy = src->overall_entropy;
+  bm->num_blocks_to_merge = 0;
+  c.sync();
+  *out = bm.release();
+  SBP_API_END
+}
+
+SbpStatus sbp_blockmodel_destroy(SbpBlockmodel* bm) {
+  SBP_API_BEGIN
+  delete bm;
+  SBP_API_END
+}
+
+SbpStatus sbp_blockmodel_num_blocks(const SbpBlockmodel* bm, int32_t* out) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(bm && out, "NULL argument");
+  *out = bm->B;
+  SBP_API_END
+}
+
+SbpStatus sbp_blockmodel_set_num_blocks_to_merge(SbpBlockmodel* bm, int32_t n) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(bm && n >= 0 && n < bm->B, "num_blocks_to_merge must be in [0, B)");
+  bm->num_blocks_to_merge = n;
+  SBP_API_END
+}
+
+SbpStatus sbp_blockmodel_overall_entropy(const SbpBlockmodel* bm, float* out) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(bm && out, "NULL argument");
+  *out = bm->overall_entropy;
+  SBP_API_END
+}
+
+SbpStatus sbp_get_assignment(const SbpBlockmodel* bm, int32_t* out) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(bm && out, "NULL argument");
+  Context& c = Context::get();
+  SBP_CUDA(SBP_COPY_ASYNC(out, bm->b.p, bm->V * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  SBP_API_END
+}
+
+SbpStatus sbp_get_block_matrix(const SbpBlockmodel* bm, int32_t* out) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(bm && out, "NULL argument");
+  Context& c = Context::get();
+  SBP_CUDA(cudaMemcpy2DAsync(out, bm->B * sizeof(int), bm->M.p, bm->ld * sizeof(int), bm->B * sizeof(int), bm->B,
+                             cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  SBP_API_END
+}
+
+SbpStatus sbp_get_degrees(const SbpBlockmodel* bm, int32_t* d_out, int32_t* d_in, int32_t* d) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(bm, "NULL argument");
+  Context& c = Context::get();
+  if (d_out) SBP_CUDA(SBP_COPY_ASYNC(d_out, bm->d_out.p, bm->B * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  if (d_in) SBP_CUDA(SBP_COPY_ASYNC(d_in, bm->d_in.p, bm->B * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  if (d) SBP_CUDA(SBP_COPY_ASYNC(d, bm->d.p, bm->B * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  SBP_API_END
+}
+
+SbpStatus sbp_mdl(const SbpBlockmodel* bm, const SbpGraph* g, double* out) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(bm && g && out && bm->V == g->V, "bad argument");
+  *out = mdl(const_cast<SbpBlockmodel&>(*bm), *g);
+  SBP_API_END
+}
+
+SbpStatus sbp_evaluate_vertices(const SbpBlockmodel* cbm, const SbpGraph* g, int32_t n, const int32_t* vertices,
+                                const uint32_t* records, int32_t* proposal, double* delta_mdl, double* hastings,
+                                int32_t* accepted) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(cbm && g && cbm->V == g->V && n >= 0, "bad argument");
+  if (n == 0) return SBP_OK;
+  SBP_REQUIRE(vertices && records && proposal && delta_mdl && hastings && accepted, "NULL buffer");
+  for (int i = 0; i < n; ++i) SBP_REQUIRE(vertices[i] >= 0 && vertices[i] < g->V, "vertex out of range");
+  SbpBlockmodel& bm = const_cast<SbpBlockmodel&>(*cbm);
+  Context& c = Context::get();
+  std::vector<int> vv(vertices, vertices + n);
+  const int cap = mh_cap(g->max_k_of(vv));
+  const size_t per_warp = (size_t)table_ints(cap) * sizeof(int);
+  const int W = (int)std::max<size_t>(1, std::min<size_t>(8, kSmemBudget / per_warp));
+  DevBuf<int> dv, ds, da;
+  DevBuf<double> dd, dh;
+  DevBuf<uint4> dr;
+  dv.reserve(n);
+  ds.reserve(n);
+  da.reserve(n);
+  dd.reserve(n);
+  dh.reserve(n);
+  dr.reserve(n);
+  SBP_CUDA(SBP_COPY_ASYNC(dv.p, vertices, n * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(dr.p, records, n * sizeof(uint4), cudaMemcpyHostToDevice, c.stream));
+  set_smem_limit((const void*)k_eval_list, per_warp * W);
+  k_eval_list<<<grid_for(n, W, 64 * c.num_sms), W * 32, per_warp * W, c.stream>>>(
+      g->view(), bm.view(), dv.p, n, dr.p, cap, ds.p, dd.p, dh.p, da.p, c.status);
+  SBP_CHECK_LAUNCH();
+  SBP_CUDA(SBP_COPY_ASYNC(proposal, ds.p, n * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(delta_mdl, dd.p, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(hastings, dh.p, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(accepted, da.p, n * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  c.check_status();
+  SBP_API_END
+}
+
+SbpStatus sbp_move_vertex(SbpBlockmodel* bm, const SbpGraph* g, int32_t vertex, int32_t block) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(bm && g && bm->V == g->V, "bad argument");
+  SBP_REQUIRE(vertex >= 0 && vertex < g->V, "vertex out of range");
+  SBP_REQUIRE(block >= 0 && block < bm->B, "block out of range");
+  Context& c = Context::get();
+  const int cap = mh_cap(g->h_k[vertex]);
+  const size_t smem = (size_t)table_ints(cap) * sizeof(int);
+  set_smem_limit((const void*)k_move_vertex, smem);
+  k_move_vertex<<<1, 32, smem, c.stream>>>(g->view(), bm->view(), vertex, block, cap, c.status);
+  SBP_CHECK_LAUNCH();
+  c.sync();
+  c.check_status();
+  SBP_API_END
+}
+
+SbpStatus sbp_finetune(SbpBlockmodel* bm, const SbpGraph* g, int32_t algorithm, const SbpFinetuneOptions* opt,
+                       const SbpReplay* replay, SbpStats* stats) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(bm && g && opt && bm->V == g->V, "bad argument");
+  SbpStats st;
+  finetune(*bm, const_cast<SbpGraph&>(*g), algorithm, *opt, replay, st);
+  if (stats) *stats = st;
+  SBP_API_END
+}
+
+SbpStatus sbp_merge_blocks(SbpBlockmodel* bm, const SbpGraph* g, const SbpMergeOptions* opt, const SbpReplay* replay,
+                           int32_t* best_merge, double* delta_mdl, SbpStats* stats) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(bm && g && opt && bm->V == g->V, "bad argument");
+  SbpStats st;
+  std::memset(&st, 0, sizeof st);
+  merge_blocks(*bm, const_cast<SbpGraph&>(*g), *opt, replay, best_merge, delta_mdl, st);
+  if (stats) *stats = st;
+  SBP_API_END
+}
+
+SbpStatus sbp_partition(const SbpGraph* g, const SbpOptions* opt, int32_t* out_assignment, SbpStats* stats) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(g && opt && out_assignment, "NULL argument");
+  SBP_REQUIRE(opt->algorithm >= 0 && opt->algorithm <= 2, "unknown algorithm");
+  SBP_REQUIRE(opt->batches >= 1, "batches must be >= 1");
+  SbpStats st;
+  partition(const_cast<SbpGraph&>(*g), *opt, out_assignment, st);
+  if (stats) *stats = st;
+  SBP_API_END
+}
+
+}  // extern "C"

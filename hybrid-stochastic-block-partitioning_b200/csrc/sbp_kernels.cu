@@ -1,0 +1,646 @@
+// CUDA kernels of the B200 stochastic block partitioning engine.
+//
+// Kernel map (reference function each one stands in for):
+//   k_rebuild_*        Blockmodel::initialize_edge_counts     src/blockmodel/blockmodel.cpp:187-255
+//   k_mdl_*            entropy::mdl / log_posterior_probability src/entropy.cpp:584-589, blockmodel.cpp:267-285
+//   k_gibbs_eval       asynchronous_gibbs evaluation half     src/finetune.cpp:49-57, 531-545
+//   k_apply_*          asynchronous_gibbs apply half          src/finetune.cpp:58-71 + Blockmodel::move_vertex
+//   k_mh               metropolis_hastings sweep              src/finetune.cpp:412-444, 446-501
+//   k_row_nnz/fill     ISparseMatrix row/column views for the merge phase
+//   k_merge_propose    merge_blocks proposal scoring          src/block_merge.cpp:278-301, 335-368
+//   k_relabel          carry-out relabel                      src/blockmodel/blockmodel.cpp:71-76
+#include "sbp_kernels.cuh"
+
+namespace sbpb {
+
+// ------------------------------------------------------------------------------------------
+// Rebuild: M, MT, d_out, d_in from the assignment; d = d_out + d_in - M[x,x].
+// ------------------------------------------------------------------------------------------
+__global__ void k_rebuild_global(GraphView g, BlockView bm) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < g.V; v += stride) {
+    const int bv = bm.b[v];
+    const int o0 = g.out_ptr[v], o1 = g.out_ptr[v + 1];
+    for (int e = o0; e < o1; ++e) {
+      const int bu = bm.b[__ldg(g.out_idx + e)];
+      atomicAdd(bm.M + (size_t)bv * bm.ld + bu, 1);
+      atomicAdd(bm.MT + (size_t)bu * bm.ld + bv, 1);
+    }
+    atomicAdd(bm.d_out + bv, o1 - o0);
+    atomicAdd(bm.d_in + bv, (g.in_ptr[v + 1] - g.in_ptr[v]) + g.self[v]);
+  }
+}
+
+// Small-B variant: a CTA-private B x B histogram in shared memory, flushed once.
+__global__ void k_rebuild_smem(GraphView g, BlockView bm) {
+  extern __shared__ int hist[];   // B*B
+  const int BB = bm.B * bm.B;
+  for (int i = threadIdx.x; i < BB; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  const int stride = gridDim.x * blockDim.x;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < g.V; v += stride) {
+    const int bv = bm.b[v];
+    const int o0 = g.out_ptr[v], o1 = g.out_ptr[v + 1];
+    for (int e = o0; e < o1; ++e) atomicAdd(hist + bv * bm.B + bm.b[__ldg(g.out_idx + e)], 1);
+    atomicAdd(bm.d_out + bv, o1 - o0);
+    atomicAdd(bm.d_in + bv, (g.in_ptr[v + 1] - g.in_ptr[v]) + g.self[v]);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < BB; i += blockDim.x) {
+    const int c = hist[i];
+    if (c) {
+      const int row = i / bm.B, col = i - row * bm.B;
+      atomicAdd(bm.M + (size_t)row * bm.ld + col, c);
+      atomicAdd(bm.MT + (size_t)col * bm.ld + row, c);
+    }
+  }
+}
+
+__global__ void k_rebuild_degrees(BlockView bm) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x < bm.B) bm.d[x] = bm.d_out[x] + bm.d_in[x] - bm.M[(size_t)x * bm.ld + x];
+}
+
+// ------------------------------------------------------------------------------------------
+// MDL: L = sum_cells g(M) - sum g(d_out) - sum g(d_in);
+// mdl = E h(B^2/E) + V log B - L.  Deterministic two-pass reduction.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+  __syncthreads();
+  return t;
+}
+
+__global__ void k_mdl_cells(BlockView bm, double* partial) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  const long long BB = (long long)bm.B * bm.B;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < BB; i += stride) {
+    const int row = (int)(i / bm.B), col = (int)(i - (long long)row * bm.B);
+    const int m = bm.M[(size_t)row * bm.ld + col];
+    if (m > 0) acc += xlogx((double)m);
+  }
+  for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < bm.B; x += stride)
+    acc -= xlogx((double)bm.d_out[x]) + xlogx((double)bm.d_in[x]);
+  const double t = block_sum(acc, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = t;
+}
+
+// Edge form: sum_cells M log M = sum over edges of log M[b_src, b_dst].
+__global__ void k_mdl_edges(GraphView g, BlockView bm, double* partial) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < g.V; v += stride) {
+    const int bv = bm.b[v];
+    const int* row = bm.M + (size_t)bv * bm.ld;
+    for (int e = g.out_ptr[v]; e < g.out_ptr[v + 1]; ++e) acc += log((double)row[bm.b[__ldg(g.out_idx + e)]]);
+  }
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < bm.B; x += stride)
+    acc -= xlogx((double)bm.d_out[x]) + xlogx((double)bm.d_in[x]);
+  const double t = block_sum(acc, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = t;
+}
+
+__global__ void k_mdl_final(const double* partial, int n, int V, long long E, int B, double* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double L = 0.0;
+  for (int i = 0; i < n; ++i) L += partial[i];
+  const double x = pow((double)B, 2) / (double)E;
+  const double h = ((1 + x) * log(1 + x)) - (x * log(x));
+  *out = ((double)E * h) + ((double)V * log((double)B)) - L;
+}
+
+// ------------------------------------------------------------------------------------------
+// Per-warp table carving from dynamic shared memory.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ WarpTable carve_table(int* base, int cap, int warp) {
+  int* p = base + (size_t)warp * (4 * cap + 32);
+  WarpTable t;
+  t.keys = p;
+  t.cout = p + cap;
+  t.cin = p + 2 * cap;
+  t.list = p + 3 * cap;
+  t.nlist = p + 4 * cap;
+  t.mask = cap - 1;
+  return t;
+}
+
+__device__ __forceinline__ void init_table(const WarpTable& t, int lane) {
+  const int cap = t.mask + 1;
+  for (int i = lane; i < cap; i += kWarp) {
+    t.keys[i] = -1;
+    t.cout[i] = 0;
+    t.cin[i] = 0;
+  }
+  if (lane == 0) *t.nlist = 0;
+  __syncwarp();
+}
+
+// ------------------------------------------------------------------------------------------
+// Asynchronous Gibbs: evaluate a list of vertices against the frozen state.  Accepted moves
+// go to prop[v] and the moved list; counters: [0] visits [1] proposals_moved [2] accepted.
+// ------------------------------------------------------------------------------------------
+__global__ void k_gibbs_eval(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng,
+                             int sweep, int* prop, int* moved_list, int* n_moved, unsigned long long* counters,
+                             int cap, int* status) {
+  extern __shared__ int smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wpb = blockDim.x >> 5;
+  WarpTable t = carve_table(smem, cap, warp);
+  init_table(t, lane);
+  unsigned long long c_visit = 0, c_moved = 0, c_acc = 0;
+  for (int i = blockIdx.x * wpb + warp; i < n; i += gridDim.x * wpb) {
+    const int v = verts[i];
+    const uint4 x = draw_record(rng, (uint32_t)v, (uint32_t)sweep, 0u, (long long)sweep * g.V + v, status);
+    int r, k_out, k_in;
+    const EvalResult res = evaluate_vertex(g, bm, v, x, t, lane, status, &r, &k_out, &k_in);
+    c_visit++;
+    if (res.s != r) c_moved++;
+    if (res.accepted) {
+      c_acc++;
+      if (lane == 0) {
+        prop[v] = res.s;
+        moved_list[atomicAdd(n_moved, 1)] = v;
+      }
+    }
+    table_reset(t, lane);
+  }
+  if (lane == 0 && c_visit) {
+    atomicAdd(counters + 0, c_visit);
+    atomicAdd(counters + 1, c_moved);
+    atomicAdd(counters + 2, c_acc);
+  }
+}
+
+// Apply accepted moves of one batch.  Every edge incident to a moved vertex moves once from
+// its old cell to its new cell; the result equals the reference's one-by-one application.
+// qr/qs keep the reference's diagonal delta of each move as seen at its turn in vertex order,
+// which Blockmodel::move_vertex folds into d[r], d[s] (blockmodel.cpp:348-359).
+__global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, const int* n_moved, const int* prop,
+                              int* qr, int* qs, int* last) {
+  const int lane = threadIdx.x & 31;
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int n = *n_moved;
+  for (int i = wid; i < n; i += nw) {
+    const int v = moved_list[i];
+    const int r = bm.b[v], s = prop[v];
+    const int self = g.self[v];
+    int cr = 0, cs = 0;
+    const int o0 = g.out_ptr[v], o1 = g.out_ptr[v + 1];
+    for (int e = o0 + lane; e < o1; e += kWarp) {
+      const int u = __ldg(g.out_idx + e);
+      if (u == v) continue;
+      const int bo = bm.b[u], pu = prop[u];
+      const int bn = pu >= 0 ? pu : bo;
+      atomicAdd(bm.M + (size_t)r * bm.ld + bo, -1);
+      atomicAdd(bm.MT + (size_t)bo * bm.ld + r, -1);
+      atomicAdd(bm.M + (size_t)s * bm.ld + bn, 1);
+      atomicAdd(bm.MT + (size_t)bn * bm.ld + s, 1);
+      const int ba = (pu >= 0 && u < v) ? pu : bo;
+      cr += (ba == r);
+      cs += (ba == s);
+    }
+    const int i0 = g.in_ptr[v], i1 = g.in_ptr[v + 1];
+    for (int e = i0 + lane; e < i1; e += kWarp) {
+      const int u = __ldg(g.in_idx + e);
+      const int bo = bm.b[u], pu = prop[u];
+      if (pu < 0) {
+        atomicAdd(bm.M + (size_t)bo * bm.ld + r, -1);
+        atomicAdd(bm.MT + (size_t)r * bm.ld + bo, -1);
+        atomicAdd(bm.M + (size_t)bo * bm.ld + s, 1);
+        atomicAdd(bm.MT + (size_t)s * bm.ld + bo, 1);
+      }
+      const int ba = (pu >= 0 && u < v) ? pu : bo;
+      cr += (ba == r);
+      cs += (ba == s);
+    }
+    cr = warp_sum_int(cr);
+    cs = warp_sum_int(cs);
+    if (lane == 0) {
+      if (self) {
+        atomicAdd(bm.M + (size_t)r * bm.ld + r, -1);
+        atomicAdd(bm.MT + (size_t)r * bm.ld + r, -1);
+        atomicAdd(bm.M + (size_t)s * bm.ld + s, 1);
+        atomicAdd(bm.MT + (size_t)s * bm.ld + s, 1);
+      }
+      const int k_out = o1 - o0, k_in_self = (i1 - i0) + self;
+      atomicAdd(bm.d_out + r, -k_out);
+      atomicAdd(bm.d_out + s, k_out);
+      atomicAdd(bm.d_in + r, -k_in_self);
+      atomicAdd(bm.d_in + s, k_in_self);
+      qr[v] = -(cr + self);
+      qs[v] = cs + self;
+      atomicMax(last + r, v);
+      atomicMax(last + s, v);
+    }
+  }
+}
+
+__global__ void k_apply_degrees(BlockView bm, const int* moved_list, const int* n_moved, const int* prop,
+                                const int* qr, const int* qs, const int* last) {
+  const int n = *n_moved;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int v = moved_list[i];
+    const int r = bm.b[v], s = prop[v];
+    if (last[r] == v) bm.d[r] = bm.d_out[r] + bm.d_in[r] - bm.M[(size_t)r * bm.ld + r] - qr[v];
+    if (last[s] == v) bm.d[s] = bm.d_out[s] + bm.d_in[s] - bm.M[(size_t)s * bm.ld + s] - qs[v];
+  }
+}
+
+__global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n_moved, int* prop, int* last) {
+  const int n = *n_moved;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int v = moved_list[i];
+    last[bm.b[v]] = -1;
+    last[prop[v]] = -1;
+    bm.b[v] = prop[v];
+    prop[v] = -1;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Metropolis-Hastings over a vertex list, exact sequential semantics, one CTA.
+// Round: the W warps evaluate the next W vertices against the current state; the first
+// accepted one (in list order) is applied by the warp that evaluated it, everything before it
+// was rejected against the true state, everything after it is re-evaluated next round.  The
+// random record of a visit depends only on (vertex, sweep), so re-evaluation is idempotent.
+// out: [0] visits [1] proposals_moved [2] accepted (as doubles), [3] sum of accepted dS.
+// ------------------------------------------------------------------------------------------
+__global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
+                     int cap, double* out, int* status) {
+  extern __shared__ int smem[];
+  __shared__ int s_acc[32], s_moved[32];
+  __shared__ double s_dS[32];
+  __shared__ int s_first;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int W = blockDim.x >> 5;
+  WarpTable t = carve_table(smem, cap, warp);
+  init_table(t, lane);
+  long long visits = 0, moved = 0, accepted = 0;
+  double sum_dS = 0.0;
+  int pos = 0;
+  __syncthreads();
+  while (pos < n) {
+    const int i = pos + warp;
+    int r = -1, k_out = 0, k_in = 0, v = -1;
+    EvalResult res;
+    res.accepted = 0;
+    res.s = -1;
+    res.dS = 0.0;
+    if (i < n) {
+      v = verts[i];
+      const uint4 x = draw_record(rng, (uint32_t)v, (uint32_t)sweep, 0u, (long long)sweep * g.V + v, status);
+      res = evaluate_vertex(g, bm, v, x, t, lane, status, &r, &k_out, &k_in);
+    }
+    if (lane == 0) {
+      s_acc[warp] = (i < n) ? res.accepted : 0;
+      s_moved[warp] = (i < n && res.s != r) ? 1 : 0;
+      s_dS[warp] = res.dS;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int first = -1;
+      for (int w = 0; w < W; ++w)
+        if (s_acc[w]) { first = w; break; }
+      s_first = first;
+    }
+    __syncthreads();
+    const int first = s_first;
+    if (first == warp) {
+      // apply the move of v from r to s with the counts still in this warp's table; lanes own
+      // distinct non-corner cells, lane 0 owns the four corner cells (r,r) (r,s) (s,r) (s,s)
+      const int s = res.s;
+      const int self = g.self[v];
+      const MoveCounts mc = corner_counts(t, r, s);
+      const int nl = *t.nlist;
+      const int ld = bm.ld;
+      for (int j = lane; j < nl; j += kWarp) {
+        const int h = t.list[j];
+        const int u = t.keys[h], co = t.cout[h], ci = t.cin[h];
+        if (u == r || u == s) continue;
+        if (co) {
+          bm.M[(size_t)r * ld + u] -= co;
+          bm.MT[(size_t)u * ld + r] -= co;
+          bm.M[(size_t)s * ld + u] += co;
+          bm.MT[(size_t)u * ld + s] += co;
+        }
+        if (ci) {
+          bm.M[(size_t)u * ld + r] -= ci;
+          bm.MT[(size_t)r * ld + u] -= ci;
+          bm.M[(size_t)u * ld + s] += ci;
+          bm.MT[(size_t)s * ld + u] += ci;
+        }
+      }
+      if (lane == 0) {
+        const int d_rr = -mc.co_r - mc.ci_r - self;
+        const int d_rs = -mc.co_s + mc.ci_r;
+        const int d_sr = mc.co_r - mc.ci_s;
+        const int d_ss = mc.co_s + mc.ci_s + self;
+        bm.M[(size_t)r * ld + r] += d_rr;
+        bm.MT[(size_t)r * ld + r] += d_rr;
+        bm.M[(size_t)r * ld + s] += d_rs;
+        bm.MT[(size_t)s * ld + r] += d_rs;
+        bm.M[(size_t)s * ld + r] += d_sr;
+        bm.MT[(size_t)r * ld + s] += d_sr;
+        bm.M[(size_t)s * ld + s] += d_ss;
+        bm.MT[(size_t)s * ld + s] += d_ss;
+        bm.b[v] = s;
+        bm.d_out[r] -= k_out;
+        bm.d_out[s] += k_out;
+        bm.d_in[r] -= k_in + self;
+        bm.d_in[s] += k_in + self;
+        // Blockmodel::move_vertex reads the already-updated diagonal and adds the delta again
+        bm.d[r] = bm.d_out[r] + bm.d_in[r] - (bm.M[(size_t)r * ld + r] + d_rr);
+        bm.d[s] = bm.d_out[s] + bm.d_in[s] - (bm.M[(size_t)s * ld + s] + d_ss);
+      }
+    }
+    if (threadIdx.x == 0) {
+      const int upto = first >= 0 ? first + 1 : min(W, n - pos);
+      for (int w = 0; w < upto; ++w) moved += s_moved[w];
+      visits += upto;
+      if (first >= 0) {
+        accepted++;
+        sum_dS += s_dS[first];
+      }
+    }
+    pos += first >= 0 ? first + 1 : W;
+    table_reset(t, lane);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = (double)visits;
+    out[1] = (double)moved;
+    out[2] = (double)accepted;
+    out[3] = sum_dS;
+  }
+}
+
+// Blockmodel::move_vertex(vertex, delta, proposal) (src/blockmodel/blockmodel.cpp:344-360) for
+// one vertex: a single warp builds the neighbour-block table and applies the move, including
+// the reference's d[r], d[s] update from the already-updated diagonal.
+__global__ void k_move_vertex(GraphView g, BlockView bm, int v, int s, int cap, int* status) {
+  extern __shared__ int smem[];
+  const int lane = threadIdx.x & 31;
+  WarpTable t = carve_table(smem, cap, 0);
+  init_table(t, lane);
+  const int r = bm.b[v];
+  if (r == s) return;
+  build_table(g, bm, v, r, t, lane, status);
+  const int self = g.self[v];
+  const int k_out = g.out_ptr[v + 1] - g.out_ptr[v];
+  const int k_in = g.in_ptr[v + 1] - g.in_ptr[v];
+  const MoveCounts mc = corner_counts(t, r, s);
+  const int nl = *t.nlist, ld = bm.ld;
+  for (int j = lane; j < nl; j += kWarp) {
+    const int h = t.list[j];
+    const int u = t.keys[h], co = t.cout[h], ci = t.cin[h];
+    if (u == r || u == s) continue;
+    bm.M[(size_t)r * ld + u] -= co;
+    bm.MT[(size_t)u * ld + r] -= co;
+    bm.M[(size_t)s * ld + u] += co;
+    bm.MT[(size_t)u * ld + s] += co;
+    bm.M[(size_t)u * ld + r] -= ci;
+    bm.MT[(size_t)r * ld + u] -= ci;
+    bm.M[(size_t)u * ld + s] += ci;
+    bm.MT[(size_t)s * ld + u] += ci;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    const int d_rr = -mc.co_r - mc.ci_r - self, d_rs = -mc.co_s + mc.ci_r;
+    const int d_sr = mc.co_r - mc.ci_s, d_ss = mc.co_s + mc.ci_s + self;
+    bm.M[(size_t)r * ld + r] += d_rr;
+    bm.MT[(size_t)r * ld + r] += d_rr;
+    bm.M[(size_t)r * ld + s] += d_rs;
+    bm.MT[(size_t)s * ld + r] += d_rs;
+    bm.M[(size_t)s * ld + r] += d_sr;
+    bm.MT[(size_t)r * ld + s] += d_sr;
+    bm.M[(size_t)s * ld + s] += d_ss;
+    bm.MT[(size_t)s * ld + s] += d_ss;
+    bm.b[v] = s;
+    bm.d_out[r] -= k_out;
+    bm.d_out[s] += k_out;
+    bm.d_in[r] -= k_in + self;
+    bm.d_in[s] += k_in + self;
+    bm.d[r] = bm.d_out[r] + bm.d_in[r] - (bm.M[(size_t)r * ld + r] + d_rr);
+    bm.d[s] = bm.d_out[s] + bm.d_in[s] - (bm.M[(size_t)s * ld + s] + d_ss);
+  }
+}
+
+// Evaluate (without moving) a list of vertices with caller-supplied records.
+__global__ void k_eval_list(GraphView g, BlockView bm, const int* verts, int n, const uint4* records, int cap,
+                            int* out_s, double* out_dS, double* out_H, int* out_acc, int* status) {
+  extern __shared__ int smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wpb = blockDim.x >> 5;
+  WarpTable t = carve_table(smem, cap, warp);
+  init_table(t, lane);
+  for (int i = blockIdx.x * wpb + warp; i < n; i += gridDim.x * wpb) {
+    const int v = verts[i];
+    int r, k_out, k_in;
+    const EvalResult res = evaluate_vertex(g, bm, v, records[i], t, lane, status, &r, &k_out, &k_in);
+    if (lane == 0) {
+      out_s[i] = res.s;
+      out_dS[i] = res.dS;
+      out_H[i] = res.H;
+      out_acc[i] = res.accepted;
+    }
+    table_reset(t, lane);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Merge phase: compressed rows of M (out_blocks) and of MT (in_blocks), ascending.
+// ------------------------------------------------------------------------------------------
+__global__ void k_row_nnz(const int* A, int B, int ld, int* cnt) {
+  const int lane = threadIdx.x & 31;
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int row = wid; row < B; row += nw) {
+    int c = 0;
+    const int* p = A + (size_t)row * ld;
+    for (int col = lane; col < B; col += kWarp) c += (p[col] != 0);
+    c = warp_sum_int(c);
+    if (lane == 0) cnt[row] = c;
+  }
+}
+
+// Exclusive scan of n ints (single CTA of 1024 threads).
+__global__ void k_excl_scan(const int* in, int* out, int n) {
+  __shared__ int warp_tot[32];
+  __shared__ int carry;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const int v = i < n ? in[i] : 0;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      int t = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, t, o);
+        if (lane >= o) t += y;
+      }
+      warp_tot[lane] = t;
+    }
+    __syncthreads();
+    const int before = carry + (w > 0 ? warp_tot[w - 1] : 0);
+    if (i < n) out[i] = before + incl - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = before + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[n] = carry;
+}
+
+__global__ void k_row_fill(const int* A, int B, int ld, const int* ptr, int* idx, int* val) {
+  const int lane = threadIdx.x & 31;
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int row = wid; row < B; row += nw) {
+    int pos = ptr[row];
+    const int* p = A + (size_t)row * ld;
+    for (int base = 0; base < B; base += kWarp) {
+      const int col = base + lane;
+      const int x = col < B ? p[col] : 0;
+      const unsigned m = __ballot_sync(kFull, x != 0);
+      if (x != 0) {
+        const int o = pos + __popc(m & ((1u << lane) - 1));
+        idx[o] = col;
+        val[o] = x;
+      }
+      pos += __popc(m);
+    }
+  }
+}
+
+// Merge proposal for block r (common::propose_new_block with block_merge = true, canonical
+// order) and the merge delta-MDL in closed form:
+//   dS = sum_c g(M[r,c]) + sum_{c!=r} g(M[c,r]) + sum_{c not in r,s} [g(M[s,c]) - g(M[s,c]+M[r,c])]
+//      + sum_{c not in r,s} [g(M[c,s]) - g(M[c,s]+M[c,r])] + g(M[s,s]) - g(M[s,s]+M[r,r]+M[r,s]+M[s,r])
+//      - [g(do_r)+g(do_s)-g(do_r+do_s)] - [g(di_r)+g(di_s)-g(di_r+di_s)]
+// which equals entropy::block_merge_delta_mdl (src/entropy.cpp:127-180).
+__device__ double merge_delta(const BlockView& bm, const Csr& rows, const Csr& cols, int r, int s, int lane) {
+  const int ld = bm.ld;
+  double dS = 0.0;
+  const int* Ms = bm.M + (size_t)s * ld;
+  const int* MTs = bm.MT + (size_t)s * ld;
+  for (int j = rows.ptr[r] + lane; j < rows.ptr[r + 1]; j += kWarp) {
+    const int c = rows.idx[j], m = rows.val[j];
+    dS += xlogx((double)m);
+    if (c != r && c != s) {
+      const int msc = Ms[c];
+      dS += dxlogx((double)msc, (double)(msc + m));
+    }
+  }
+  for (int j = cols.ptr[r] + lane; j < cols.ptr[r + 1]; j += kWarp) {
+    const int c = cols.idx[j], m = cols.val[j];
+    if (c == r) continue;
+    dS += xlogx((double)m);
+    if (c != s) {
+      const int mcs = MTs[c];
+      dS += dxlogx((double)mcs, (double)(mcs + m));
+    }
+  }
+  dS = warp_sum(dS);
+  const int M_rr = bm.M[(size_t)r * ld + r], M_rs = bm.M[(size_t)r * ld + s];
+  const int M_sr = bm.M[(size_t)s * ld + r], M_ss = bm.M[(size_t)s * ld + s];
+  dS += dxlogx((double)M_ss, (double)(M_ss + M_rr + M_rs + M_sr));
+  const double dor = bm.d_out[r], dos = bm.d_out[s], dir = bm.d_in[r], dis = bm.d_in[s];
+  dS -= xlogx(dor) + xlogx(dos) - xlogx(dor + dos);
+  dS -= xlogx(dir) + xlogx(dis) - xlogx(dir + dis);
+  return dS;
+}
+
+__global__ void k_merge_propose(BlockView bm, Csr rows, Csr cols, RngParams rng, int* best_s, double* best_dS,
+                                unsigned long long* counters, int* status) {
+  const int lane = threadIdx.x & 31;
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int B = bm.B;
+  for (int r = wid; r < B; r += nw) {
+    int seen[kProposalsPerBlock];
+    int nseen = 0;
+    int best = -1;
+    double bdS = 1.79769313486231570815e+308;
+    int avoided = 0;
+    const long long k_out = bm.d_out[r], k = k_out + bm.d_in[r];
+    for (int i = 0; i < kProposalsPerBlock; ++i) {
+      const uint4 x = draw_record(rng, (uint32_t)r, (uint32_t)i, 1u, (long long)r * kProposalsPerBlock + i, status);
+      int s;
+      if (k == 0) {
+        s = random_block(r, B, x.y);
+      } else {
+        const long long target = scale32(x.x, k);
+        int t;
+        if (target < k_out) t = warp_select_sparse(rows.idx + rows.ptr[r], rows.val + rows.ptr[r],
+                                                   rows.ptr[r + 1] - rows.ptr[r], target, -1, lane);
+        else t = warp_select_sparse(cols.idx + cols.ptr[r], cols.val + cols.ptr[r], cols.ptr[r + 1] - cols.ptr[r],
+                                    target - k_out, -1, lane);
+        if (t < 0) {
+          if (lane == 0) atomicOr(status, kErrScan);
+          t = r;
+        }
+        const long long m_tr = bm.M[(size_t)t * bm.ld + r], m_rt = bm.M[(size_t)r * bm.ld + t];
+        const long long rowpart = (long long)bm.d_out[t] - m_tr;
+        const long long total = rowpart + (long long)bm.d_in[t] - m_rt;
+        if (total == 0) {
+          s = random_block(r, B, x.y);
+        } else {
+          const long long tg = scale32(x.y, total);
+          if (tg < rowpart) s = warp_select_sparse(rows.idx + rows.ptr[t], rows.val + rows.ptr[t],
+                                                   rows.ptr[t + 1] - rows.ptr[t], tg, r, lane);
+          else s = warp_select_sparse(cols.idx + cols.ptr[t], cols.val + cols.ptr[t], cols.ptr[t + 1] - cols.ptr[t],
+                                      tg - rowpart, r, lane);
+          if (s < 0) {
+            if (lane == 0) atomicOr(status, kErrScan);
+            s = random_block(r, B, x.y);
+          }
+        }
+      }
+      bool dup = false;
+      for (int j = 0; j < nseen; ++j) dup |= (seen[j] == s);
+      if (dup) {
+        avoided++;
+        continue;
+      }
+      seen[nseen++] = s;
+      const double dS = merge_delta(bm, rows, cols, r, s, lane);
+      if (dS < bdS) {
+        bdS = dS;
+        best = s;
+      }
+    }
+    if (lane == 0) {
+      best_s[r] = best;
+      best_dS[r] = bdS;
+      atomicAdd(counters + 0, (unsigned long long)kProposalsPerBlock);
+      atomicAdd(counters + 1, (unsigned long long)avoided);
+    }
+  }
+}
+
+__global__ void k_block_sizes(const int* b, int V, int* size) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) atomicAdd(size + b[v], 1);
+}
+
+__global__ void k_relabel(int* b, int V, const int* map) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) b[v] = map[b[v]];
+}
+
+}  // namespace sbpb

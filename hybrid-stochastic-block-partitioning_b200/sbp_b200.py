@@ -1,0 +1,341 @@
+"""Python binding of libsbp_b200.so (the C ABI in include/sbp_b200.h).
+
+Mirrors the reference's C++ API (vtsynergy/Hybrid-Stochastic-Block-Partitioning):
+  Graph                      include/graph.hpp:15-113
+  Blockmodel                 include/blockmodel/blockmodel.hpp:45-184
+  entropy.mdl                src/entropy.cpp:584-589
+  block_merge.merge_blocks   src/block_merge.cpp:278-311
+  finetune.metropolis_hastings / asynchronous_gibbs / hybrid_mcmc   src/finetune.cpp
+  sbp.stochastic_block_partition                                    src/sbp.cpp:61-98
+All compute runs on the GPU; without the built library or a CUDA device every call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsbp_b200.so")
+
+METROPOLIS_HASTINGS, ASYNC_GIBBS, HYBRID_MCMC = 0, 1, 2
+ALGORITHMS = {"metropolis_hastings": METROPOLIS_HASTINGS, "async_gibbs": ASYNC_GIBBS, "hybrid_mcmc": HYBRID_MCMC}
+
+STATUS = {0: "SBP_OK", 1: "SBP_ERR_INVALID_ARGUMENT", 2: "SBP_ERR_CUDA", 3: "SBP_ERR_UNSUPPORTED",
+          4: "SBP_ERR_REPLAY", 5: "SBP_ERR_DEVICE", 6: "SBP_ERR_OUT_OF_MEMORY"}
+
+EXPORTED = [
+    "sbp_last_error", "sbp_device_count", "sbp_get_stream", "sbp_profile_enable", "sbp_profile_read",
+    "sbp_graph_create", "sbp_graph_destroy", "sbp_graph_num_edges",
+    "sbp_graph_get_split", "sbp_graph_set_split", "sbp_blockmodel_create", "sbp_blockmodel_copy",
+    "sbp_blockmodel_destroy", "sbp_blockmodel_num_blocks", "sbp_blockmodel_set_num_blocks_to_merge",
+    "sbp_blockmodel_overall_entropy", "sbp_get_assignment", "sbp_get_block_matrix", "sbp_get_degrees", "sbp_mdl",
+    "sbp_evaluate_vertices", "sbp_move_vertex", "sbp_finetune", "sbp_merge_blocks", "sbp_partition",
+]
+
+
+class SbpError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Replay(ctypes.Structure):
+    _fields_ = [("words", ctypes.POINTER(ctypes.c_uint32)), ("records", ctypes.c_int64)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("visits", ctypes.c_int64), ("proposals_moved", ctypes.c_int64), ("accepted", ctypes.c_int64),
+                ("sweeps", ctypes.c_int32), ("outer_iterations", ctypes.c_int32), ("num_blocks", ctypes.c_int32),
+                ("_pad", ctypes.c_int32), ("mdl", ctypes.c_double), ("mcmc_seconds", ctypes.c_double),
+                ("merge_seconds", ctypes.c_double), ("merge_proposals", ctypes.c_int64),
+                ("merge_avoided", ctypes.c_int64), ("total_seconds", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("_")}
+
+
+class Profile(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_int64), ("eval_launches", ctypes.c_int64), ("eval_visits", ctypes.c_int64),
+                ("eval_ms", ctypes.c_double), ("eval_bytes", ctypes.c_double), ("h2d_bytes", ctypes.c_int64),
+                ("d2h_bytes", ctypes.c_int64)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("algorithm", ctypes.c_int32), ("batches", ctypes.c_int32), ("approximate", ctypes.c_int32),
+                ("asynciterations", ctypes.c_int32), ("seed", ctypes.c_uint64)]
+
+
+class FinetuneOptions(ctypes.Structure):
+    _fields_ = [("batches", ctypes.c_int32), ("bracket_established", ctypes.c_int32),
+                ("max_sweeps", ctypes.c_int32), ("call", ctypes.c_uint32), ("seed", ctypes.c_uint64)]
+
+
+class MergeOptions(ctypes.Structure):
+    _fields_ = [("approximate", ctypes.c_int32), ("call", ctypes.c_uint32), ("seed", ctypes.c_uint64)]
+
+
+_lib = None
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+def load(path=LIB_PATH):
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise SbpError(2, f"{path} is missing: run __graft_entry__.build() (no CPU fallback exists)")
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    pp = ctypes.POINTER(ctypes.c_void_p)
+    L.sbp_last_error.restype = ctypes.c_char_p
+    L.sbp_device_count.restype = ctypes.c_int32
+    for name in EXPORTED[2:]:
+        getattr(L, name).restype = ctypes.c_int
+    L.sbp_get_stream.argtypes = [pp]
+    L.sbp_profile_enable.argtypes = [ctypes.c_int32]
+    L.sbp_profile_read.argtypes = [ctypes.POINTER(Profile), ctypes.c_int32]
+    L.sbp_graph_create.argtypes = [ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, pp]
+    L.sbp_graph_destroy.argtypes = [vp]
+    L.sbp_graph_num_edges.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    L.sbp_graph_get_split.argtypes = [vp, _i32p, _i32p, _i32p]
+    L.sbp_graph_set_split.argtypes = [vp, ctypes.c_int32, _i32p, ctypes.c_int32, _i32p]
+    L.sbp_blockmodel_create.argtypes = [vp, ctypes.c_int32, _i32p, pp]
+    L.sbp_blockmodel_copy.argtypes = [vp, pp]
+    L.sbp_blockmodel_destroy.argtypes = [vp]
+    L.sbp_blockmodel_num_blocks.argtypes = [vp, _i32p]
+    L.sbp_blockmodel_set_num_blocks_to_merge.argtypes = [vp, ctypes.c_int32]
+    L.sbp_blockmodel_overall_entropy.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    L.sbp_get_assignment.argtypes = [vp, _i32p]
+    L.sbp_get_block_matrix.argtypes = [vp, _i32p]
+    L.sbp_get_degrees.argtypes = [vp, _i32p, _i32p, _i32p]
+    L.sbp_mdl.argtypes = [vp, vp, _f64p]
+    L.sbp_evaluate_vertices.argtypes = [vp, vp, ctypes.c_int32, _i32p, _u32p, _i32p, _f64p, _f64p, _i32p]
+    L.sbp_move_vertex.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32]
+    L.sbp_finetune.argtypes = [vp, vp, ctypes.c_int32, ctypes.POINTER(FinetuneOptions), ctypes.POINTER(Replay),
+                               ctypes.POINTER(Stats)]
+    L.sbp_merge_blocks.argtypes = [vp, vp, ctypes.POINTER(MergeOptions), ctypes.POINTER(Replay), _i32p, _f64p,
+                                   ctypes.POINTER(Stats)]
+    L.sbp_partition.argtypes = [vp, ctypes.POINTER(Options), _i32p, ctypes.POINTER(Stats)]
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise SbpError(rc, _lib.sbp_last_error().decode())
+
+
+def _p(a, t=_i32p):
+    return a.ctypes.data_as(t)
+
+
+def _replay(records):
+    if records is None:
+        return None, None
+    arr = np.ascontiguousarray(records, dtype=np.uint32).reshape(-1)
+    rp = Replay(arr.ctypes.data_as(_u32p), len(arr) // 4)
+    return arr, ctypes.byref(rp)
+
+
+def device_count():
+    return load().sbp_device_count()
+
+
+def stream_handle():
+    """cudaStream_t of the library (use with torch.cuda.ExternalStream for events)."""
+    h = ctypes.c_void_p()
+    _check(load().sbp_get_stream(ctypes.byref(h)))
+    return h.value
+
+
+def profile_enable(on=True):
+    _check(load().sbp_profile_enable(int(bool(on))))
+
+
+def profile_read(reset=False):
+    p = Profile()
+    _check(load().sbp_profile_read(ctypes.byref(p), int(bool(reset))))
+    return {k: getattr(p, k) for k, _ in p._fields_}
+
+
+class Graph:
+    """Device-resident directed graph (Graph::load_text semantics: first occurrence of each edge kept)."""
+
+    def __init__(self, num_vertices, src, dst):
+        L = load()
+        s = np.ascontiguousarray(src, dtype=np.int32)
+        d = np.ascontiguousarray(dst, dtype=np.int32)
+        if s.shape != d.shape:
+            raise SbpError(1, "src and dst differ in length")
+        h = ctypes.c_void_p()
+        _check(L.sbp_graph_create(int(num_vertices), len(s), _p(s), _p(d), ctypes.byref(h)))
+        self.h = h
+        self.V = int(num_vertices)
+        e = ctypes.c_int64()
+        _check(L.sbp_graph_num_edges(h, ctypes.byref(e)))
+        self.E = e.value
+
+    def num_vertices(self):
+        return self.V
+
+    def num_edges(self):
+        return self.E
+
+    def split(self):
+        nh = ctypes.c_int32()
+        hi = np.zeros(self.V, np.int32)
+        lo = np.zeros(self.V, np.int32)
+        _check(_lib.sbp_graph_get_split(self.h, ctypes.byref(nh), _p(hi), _p(lo)))
+        return hi[:nh.value].copy(), lo[:self.V - nh.value].copy()
+
+    def set_split(self, high, low):
+        hi = np.ascontiguousarray(high, np.int32)
+        lo = np.ascontiguousarray(low, np.int32)
+        _check(_lib.sbp_graph_set_split(self.h, len(hi), _p(hi), len(lo), _p(lo)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.sbp_graph_destroy(self.h)
+            self.h = None
+
+
+class Blockmodel:
+    """Device-resident blockmodel: assignment, B x B counts, degrees (Blockmodel)."""
+
+    def __init__(self, graph, num_blocks=None, assignment=None, _handle=None):
+        self.graph = graph
+        if _handle is not None:
+            self.h = _handle
+            return
+        a = np.ascontiguousarray(assignment, dtype=np.int32)
+        h = ctypes.c_void_p()
+        _check(load().sbp_blockmodel_create(graph.h, int(num_blocks), _p(a), ctypes.byref(h)))
+        self.h = h
+
+    def copy(self):
+        h = ctypes.c_void_p()
+        _check(_lib.sbp_blockmodel_copy(self.h, ctypes.byref(h)))
+        return Blockmodel(self.graph, _handle=h)
+
+    def getNum_blocks(self):
+        b = ctypes.c_int32()
+        _check(_lib.sbp_blockmodel_num_blocks(self.h, ctypes.byref(b)))
+        return b.value
+
+    B = property(getNum_blocks)
+
+    def setNum_blocks_to_merge(self, n):
+        _check(_lib.sbp_blockmodel_set_num_blocks_to_merge(self.h, int(n)))
+
+    def getOverall_entropy(self):
+        f = ctypes.c_float()
+        _check(_lib.sbp_blockmodel_overall_entropy(self.h, ctypes.byref(f)))
+        return f.value
+
+    def block_assignment(self):
+        out = np.zeros(self.graph.V, np.int32)
+        _check(_lib.sbp_get_assignment(self.h, _p(out)))
+        return out
+
+    def blockmatrix(self):
+        B = self.B
+        out = np.zeros(B * B, np.int32)
+        _check(_lib.sbp_get_block_matrix(self.h, _p(out)))
+        return out.reshape(B, B)
+
+    def degrees_all(self):
+        B = self.B
+        do, di, d = (np.zeros(B, np.int32) for _ in range(3))
+        _check(_lib.sbp_get_degrees(self.h, _p(do), _p(di), _p(d)))
+        return do, di, d
+
+    def degrees_out(self):
+        return self.degrees_all()[0]
+
+    def degrees_in(self):
+        return self.degrees_all()[1]
+
+    def degrees(self):
+        return self.degrees_all()[2]
+
+    def move_vertex(self, vertex, block):
+        _check(_lib.sbp_move_vertex(self.h, self.graph.h, int(vertex), int(block)))
+
+    def evaluate_vertices(self, vertices, records):
+        v = np.ascontiguousarray(vertices, np.int32)
+        r = np.ascontiguousarray(records, np.uint32).reshape(-1)
+        n = len(v)
+        s = np.zeros(n, np.int32)
+        dS = np.zeros(n, np.float64)
+        H = np.zeros(n, np.float64)
+        acc = np.zeros(n, np.int32)
+        _check(_lib.sbp_evaluate_vertices(self.h, self.graph.h, n, _p(v), _p(r, _u32p), _p(s), _p(dS, _f64p),
+                                          _p(H, _f64p), _p(acc)))
+        return s, dS, H, acc.astype(bool)
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.sbp_blockmodel_destroy(self.h)
+            self.h = None
+
+
+class entropy:
+    @staticmethod
+    def mdl(blockmodel, graph=None):
+        out = ctypes.c_double()
+        _check(_lib.sbp_mdl(blockmodel.h, (graph or blockmodel.graph).h, ctypes.byref(out)))
+        return out.value
+
+
+class finetune:
+    @staticmethod
+    def run(blockmodel, algorithm, batches=10, bracket=False, seed=0, call=0, replay=None, max_sweeps=0):
+        opt = FinetuneOptions(int(batches), int(bool(bracket)), int(max_sweeps), int(call), int(seed))
+        keep, rp = _replay(replay)
+        st = Stats()
+        _check(_lib.sbp_finetune(blockmodel.h, blockmodel.graph.h, int(algorithm), ctypes.byref(opt), rp,
+                                 ctypes.byref(st)))
+        del keep
+        return st.as_dict()
+
+    @staticmethod
+    def metropolis_hastings(blockmodel, **kw):
+        return finetune.run(blockmodel, METROPOLIS_HASTINGS, **kw)
+
+    @staticmethod
+    def asynchronous_gibbs(blockmodel, **kw):
+        return finetune.run(blockmodel, ASYNC_GIBBS, **kw)
+
+    @staticmethod
+    def hybrid_mcmc(blockmodel, **kw):
+        return finetune.run(blockmodel, HYBRID_MCMC, **kw)
+
+
+class block_merge:
+    @staticmethod
+    def merge_blocks(blockmodel, approximate=True, seed=0, call=0, replay=None):
+        B = blockmodel.B
+        best = np.zeros(B, np.int32)
+        dS = np.zeros(B, np.float64)
+        opt = MergeOptions(int(bool(approximate)), int(call), int(seed))
+        keep, rp = _replay(replay)
+        st = Stats()
+        _check(_lib.sbp_merge_blocks(blockmodel.h, blockmodel.graph.h, ctypes.byref(opt), rp, _p(best),
+                                     _p(dS, _f64p), ctypes.byref(st)))
+        del keep
+        return dict(best=best, dS=dS, **st.as_dict())
+
+
+class sbp:
+    @staticmethod
+    def stochastic_block_partition(graph, algorithm="async_gibbs", batches=10, approximate=True,
+                                   asynciterations=2**31 - 1, seed=0):
+        algo = ALGORITHMS[algorithm] if isinstance(algorithm, str) else int(algorithm)
+        opt = Options(algo, int(batches), int(bool(approximate)), int(asynciterations), int(seed))
+        out = np.zeros(graph.V, np.int32)
+        st = Stats()
+        _check(_lib.sbp_partition(graph.h, ctypes.byref(opt), _p(out), ctypes.byref(st)))
+        return out, st.as_dict()

@@ -1,0 +1,185 @@
+/*
+ * sbp_b200.h -- C ABI of the B200 stochastic block partitioning engine (libsbp_b200.so).
+ *
+ * Plain pointers and sizes only; no exceptions cross this boundary.  Every function returns
+ * an SbpStatus; sbp_last_error() gives a message for the last failure on the calling thread.
+ * Device memory is owned by the handles; the caller owns every host buffer.  Calls on the
+ * same handle are not thread-safe.  There is no CPU fallback: without a usable CUDA device
+ * every compute call fails with SBP_ERR_CUDA.
+ *
+ * Each entry point names the reference interface it replaces
+ * (vtsynergy/Hybrid-Stochastic-Block-Partitioning, file:line).
+ */
+#ifndef SBP_B200_H
+#define SBP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SBP_OK = 0,
+    SBP_ERR_INVALID_ARGUMENT = 1,  /* bad pointer, size, vertex or block id */
+    SBP_ERR_CUDA = 2,              /* CUDA runtime failure or no device */
+    SBP_ERR_UNSUPPORTED = 3,       /* input outside what the kernels support (e.g. degree) */
+    SBP_ERR_REPLAY = 4,            /* replay stream shorter than the run needs */
+    SBP_ERR_DEVICE = 5,            /* a kernel reported an inconsistency (status word) */
+    SBP_ERR_OUT_OF_MEMORY = 6
+} SbpStatus;
+
+/* Finetune algorithms (include/args.hpp:45-48, `-a`). */
+typedef enum {
+    SBP_METROPOLIS_HASTINGS = 0,
+    SBP_ASYNC_GIBBS = 1,
+    SBP_HYBRID_MCMC = 2
+} SbpAlgorithm;
+
+typedef struct SbpGraph SbpGraph;
+typedef struct SbpBlockmodel SbpBlockmodel;
+
+/* Host-supplied random stream: `records` 4-word records (x_neighbour, x_multinomial,
+ * u_hi, u_lo).  A finetune call reads record sweep*V + v for the visit of vertex v in that
+ * sweep; a merge call reads record block*10 + proposal. */
+typedef struct {
+    const uint32_t *words;   /* 4 * records words */
+    int64_t records;
+} SbpReplay;
+
+/* Counters of one finetune, merge or partition call. */
+typedef struct {
+    int64_t visits;            /* vertex evaluations (proposals drawn) */
+    int64_t proposals_moved;   /* proposals with s != r */
+    int64_t accepted;          /* accepted vertex moves */
+    int32_t sweeps;            /* MCMC iterations */
+    int32_t outer_iterations;  /* partition only: merge+finetune rounds */
+    int32_t num_blocks;        /* blocks after the call */
+    int32_t _pad;
+    double mdl;                /* overall entropy after the call (the reference stores it as float) */
+    double mcmc_seconds;       /* device time spent in finetune */
+    double merge_seconds;      /* device time spent in block merge */
+    int64_t merge_proposals;   /* block-merge proposals drawn */
+    int64_t merge_avoided;     /* proposals skipped as duplicates */
+    double total_seconds;      /* partition only: device-clock time of the whole call */
+} SbpStats;
+
+/* Launch and timing counters of this library (process-wide). */
+typedef struct {
+    int64_t launches;          /* kernels launched by the library since load */
+    int64_t eval_launches;     /* profiled vertex-evaluation launches */
+    int64_t eval_visits;       /* vertices they evaluated */
+    double eval_ms;            /* summed CUDA-event duration of those launches */
+    double eval_bytes;         /* algorithmic bytes: sum over vertices of 12 + 8 (k_out + k_in) */
+    int64_t h2d_bytes;         /* bytes the library copied host -> device since load */
+    int64_t d2h_bytes;         /* bytes the library copied device -> host since load */
+} SbpProfile;
+
+/* Options of sbp_partition (src/sbp.cpp:61-98; include/args.hpp flags). */
+typedef struct {
+    int32_t algorithm;         /* SbpAlgorithm */
+    int32_t batches;           /* --batches (default 10) */
+    int32_t approximate;       /* --approximate: simple merge carry-out */
+    int32_t asynciterations;   /* --asynciterations (async Gibbs rounds before MH) */
+    uint64_t seed;             /* Philox key */
+} SbpOptions;
+
+/* Finetune call options. */
+typedef struct {
+    int32_t batches;               /* --batches */
+    int32_t bracket_established;   /* BlockmodelTriplet::get(2) non-empty: early-stop threshold 1e-4 */
+    int32_t max_sweeps;            /* <= 0: MAX_NUM_ITERATIONS (100) */
+    uint32_t call;                 /* Philox counter word 2 */
+    uint64_t seed;
+} SbpFinetuneOptions;
+
+/* Merge call options. */
+typedef struct {
+    int32_t approximate;       /* 1: Blockmodel::carry_out_best_merges, 0: advanced */
+    uint32_t call;
+    uint64_t seed;
+} SbpMergeOptions;
+
+/* Last error message of the calling thread (static storage). */
+const char *sbp_last_error(void);
+
+/* Number of usable CUDA devices (0 if none). */
+int32_t sbp_device_count(void);
+
+/* The CUDA stream every call of this library runs on (cudaStream_t), for interop and timing.
+ * No reference counterpart (the reference is CPU-only). */
+SbpStatus sbp_get_stream(void **out);
+/* Enable CUDA-event timing of the vertex-evaluation kernel launches (off by default), and read
+ * the counters.  No reference counterpart. */
+SbpStatus sbp_profile_enable(int32_t on);
+SbpStatus sbp_profile_read(SbpProfile *out, int32_t reset);
+
+/* Graph(out_neighbors, in_neighbors, ...) built from an edge list: duplicates are dropped
+ * keeping the first occurrence (utils::insert_nodup, src/utils.cpp:52-60), self loops kept,
+ * vertices split high/low by degree for the hybrid schedule (Graph::sort_vertices,
+ * src/graph.cpp:215-228; ties by vertex id).  Replaces Graph::load_text (src/graph.cpp:123-140). */
+SbpStatus sbp_graph_create(int32_t num_vertices, int64_t num_edges, const int32_t *src, const int32_t *dst,
+                           SbpGraph **out);
+SbpStatus sbp_graph_destroy(SbpGraph *graph);
+/* Graph::num_edges (include/graph.hpp:106): unique directed edges. */
+SbpStatus sbp_graph_num_edges(const SbpGraph *graph, int64_t *out);
+/* Graph::high_degree_vertices / low_degree_vertices (include/graph.hpp:100-102). */
+SbpStatus sbp_graph_get_split(const SbpGraph *graph, int32_t *num_high, int32_t *high, int32_t *low);
+SbpStatus sbp_graph_set_split(SbpGraph *graph, int32_t num_high, const int32_t *high, int32_t num_low,
+                              const int32_t *low);
+
+/* Blockmodel(num_blocks, graph, 0.5, assignment) (include/blockmodel/blockmodel.hpp:70-76):
+ * counts rebuilt on the device (Blockmodel::initialize_edge_counts, blockmodel.cpp:187-255). */
+SbpStatus sbp_blockmodel_create(const SbpGraph *graph, int32_t num_blocks, const int32_t *assignment,
+                                SbpBlockmodel **out);
+/* Blockmodel::copy (src/blockmodel/blockmodel.cpp:95-105). */
+SbpStatus sbp_blockmodel_copy(const SbpBlockmodel *src, SbpBlockmodel **out);
+SbpStatus sbp_blockmodel_destroy(SbpBlockmodel *bm);
+SbpStatus sbp_blockmodel_num_blocks(const SbpBlockmodel *bm, int32_t *out);
+/* Blockmodel::setNum_blocks_to_merge (include/blockmodel/blockmodel.hpp:167). */
+SbpStatus sbp_blockmodel_set_num_blocks_to_merge(SbpBlockmodel *bm, int32_t n);
+/* Blockmodel::getOverall_entropy (float, include/blockmodel/blockmodel.hpp:164). */
+SbpStatus sbp_blockmodel_overall_entropy(const SbpBlockmodel *bm, float *out);
+/* Blockmodel::block_assignment (include/blockmodel/blockmodel.hpp:126). out: V ints. */
+SbpStatus sbp_get_assignment(const SbpBlockmodel *bm, int32_t *out);
+/* Dense dump of the block matrix (ISparseMatrix::get). out: B*B ints, row-major. */
+SbpStatus sbp_get_block_matrix(const SbpBlockmodel *bm, int32_t *out);
+/* Blockmodel::degrees_out / degrees_in / degrees. Each out: B ints. */
+SbpStatus sbp_get_degrees(const SbpBlockmodel *bm, int32_t *d_out, int32_t *d_in, int32_t *d);
+
+/* entropy::mdl (src/entropy.cpp:584-589), FP64 logs. */
+SbpStatus sbp_mdl(const SbpBlockmodel *bm, const SbpGraph *graph, double *out);
+
+/* Evaluate vertices against the current (frozen) state without moving them: proposal,
+ * Hastings correction, delta-MDL and the accept test for each vertex with the given records
+ * (finetune::propose_gibbs_move_v2, src/finetune.cpp:531-545).  records: 4*n words.
+ * Outputs (n each): proposed block, delta-MDL, Hastings, accepted flag. */
+SbpStatus sbp_evaluate_vertices(const SbpBlockmodel *bm, const SbpGraph *graph, int32_t n, const int32_t *vertices,
+                                const uint32_t *records, int32_t *proposal, double *delta_mdl, double *hastings,
+                                int32_t *accepted);
+
+/* Blockmodel::move_vertex(vertex, delta, proposal) (src/blockmodel/blockmodel.cpp:344-360):
+ * move one vertex to `block`, updating counts and degrees as the reference does (d[r], d[s]
+ * are set from the already-updated diagonal plus the diagonal delta). */
+SbpStatus sbp_move_vertex(SbpBlockmodel *bm, const SbpGraph *graph, int32_t vertex, int32_t block);
+
+/* finetune::metropolis_hastings / asynchronous_gibbs / hybrid_mcmc
+ * (src/finetune.cpp:412-444, 31-89, 342-410).  `replay` may be NULL (Philox stream). */
+SbpStatus sbp_finetune(SbpBlockmodel *bm, const SbpGraph *graph, int32_t algorithm, const SbpFinetuneOptions *opt,
+                       const SbpReplay *replay, SbpStats *stats);
+
+/* block_merge::merge_blocks (src/block_merge.cpp:278-311).  `replay` may be NULL.
+ * best_merge / delta_mdl (B entries each, may be NULL) receive the per-block best proposal
+ * and its delta-MDL before the merges are carried out. */
+SbpStatus sbp_merge_blocks(SbpBlockmodel *bm, const SbpGraph *graph, const SbpMergeOptions *opt,
+                           const SbpReplay *replay, int32_t *best_merge, double *delta_mdl, SbpStats *stats);
+
+/* sbp::stochastic_block_partition (src/sbp.cpp:61-98): golden-section search over B with
+ * merge + finetune rounds.  out_assignment: V ints. */
+SbpStatus sbp_partition(const SbpGraph *graph, const SbpOptions *opt, int32_t *out_assignment, SbpStats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SBP_B200_H */

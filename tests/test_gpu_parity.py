@@ -1,0 +1,222 @@
+"""GPU parity tests: the CUDA engine (through the C ABI) against the CPU oracle.
+
+Integer state (assignment, block matrix, d_out, d_in, d, counters) must be bit-exact; delta-MDL
+and MDL (FP64 log terms) within 1e-9 relative; the Hastings correction within 1e-12 relative.
+Random numbers are identical on both sides (Philox4x32-10 or a replayed stream).
+"""
+import numpy as np
+import pytest
+
+from conftest import random_assignment, random_graph, random_records, toy_fixture
+
+pytestmark = pytest.mark.gpu
+RTOL_MDL = 1e-9
+
+
+def pair(S, O, V, s, d, B, a):
+    g, og = S.Graph(V, s, d), O.Graph(V, s, d)
+    return g, og, S.Blockmodel(g, B, a), O.Blockmodel(og, B, a)
+
+
+def assert_same_state(bm, obm):
+    assert bm.B == obm.B
+    assert np.array_equal(bm.block_assignment(), obm.assignment())
+    assert np.array_equal(bm.blockmatrix(), obm.matrix())
+    do, di, d = bm.degrees_all()
+    odo, odi, od = obm.degrees()
+    assert np.array_equal(do, odo)
+    assert np.array_equal(di, odi)
+    assert np.array_equal(d, od)
+
+
+def test_toy_known_answers_on_gpu(S, O):
+    fx = toy_fixture()
+    e = np.array(fx["edges"], np.int32)
+    g = S.Graph(fx["num_vertices"], e[:, 0], e[:, 1])
+    assert g.E == 23
+    bm = S.Blockmodel(g, 3, np.array(fx["assignment"], np.int32))
+    assert S.entropy.mdl(bm) == pytest.approx(fx["mdl"], rel=1e-6)
+    do, di, d = bm.degrees_all()
+    assert list(do) == [8, 7, 8] and list(di) == [9, 7, 7] and list(d) == [10, 9, 9]
+    M0 = bm.blockmatrix()
+    bm.move_vertex(7, 0)
+    diff = bm.blockmatrix() - M0
+    for k, v in fx["delta_move_7_to_0_with_self_in"].items():
+        r, c = map(int, k.split(","))
+        assert diff[r, c] == v
+
+
+def test_complex_move_matches_oracle(S, O):
+    fx = toy_fixture()
+    e = np.array(fx["edges"], np.int32)
+    a = np.array(fx["complex_assignment"], np.int32)
+    g, og, bm, obm = pair(S, O, 11, e[:, 0], e[:, 1], 6, a)
+    bm.move_vertex(6, 0)
+    obm.move_vertex(6, 0)
+    assert_same_state(bm, obm)
+    assert list(bm.degrees()) == [11, 7, 4, 7, 5, 6]
+
+
+@pytest.mark.parametrize("V,K,B,seed", [(60, 3, 5, 1), (500, 6, 40, 2), (2000, 10, 300, 3), (3000, 20, 1200, 4)])
+def test_mdl_matches_oracle(S, O, V, K, B, seed):
+    V, s, d, _ = random_graph(V, K, seed)
+    a = random_assignment(V, B, seed)
+    g, og, bm, obm = pair(S, O, V, s, d, B, a)
+    assert_same_state(bm, obm)
+    assert S.entropy.mdl(bm) == pytest.approx(obm.mdl(), rel=RTOL_MDL)
+
+
+@pytest.mark.parametrize("V,K,B,seed", [(300, 5, 12, 1), (1500, 8, 200, 2), (800, 6, 3, 3)])
+def test_evaluate_vertices_matches_oracle(S, O, V, K, B, seed):
+    V, s, d, _ = random_graph(V, K, seed)
+    a = random_assignment(V, B, seed)
+    g, og, bm, obm = pair(S, O, V, s, d, B, a)
+    verts = np.arange(V, dtype=np.int32)
+    rec = random_records(V, seed + 100)
+    ps, dS, H, acc = bm.evaluate_vertices(verts, rec)
+    n_moved = 0
+    for v in range(V):
+        ev = obm.eval_vertex(v, rec[v])
+        assert ps[v] == ev["s"], v
+        if ev["moved"]:
+            n_moved += 1
+            assert dS[v] == pytest.approx(ev["dS"], rel=RTOL_MDL, abs=1e-9), v
+            assert H[v] == pytest.approx(ev["H"], rel=1e-12), v
+            assert bool(acc[v]) == ev["accepted"], v
+        else:
+            assert not acc[v]
+    assert n_moved > V // 4
+
+
+@pytest.mark.parametrize("algo", ["metropolis_hastings", "asynchronous_gibbs", "hybrid_mcmc"])
+@pytest.mark.parametrize("V,K,B,batches,seed", [(400, 5, 20, 4, 11), (1200, 8, 150, 10, 12), (900, 6, 6, 3, 13)])
+def test_finetune_bit_exact(S, O, algo, V, K, B, batches, seed):
+    V, s, d, _ = random_graph(V, K, seed)
+    a = random_assignment(V, B, seed)
+    g, og, bm, obm = pair(S, O, V, s, d, B, a)
+    code = {"metropolis_hastings": 0, "asynchronous_gibbs": 1, "hybrid_mcmc": 2}[algo]
+    st = getattr(S.finetune, algo)(bm, batches=batches, seed=seed, call=3, max_sweeps=6)
+    ost = obm.finetune(code, batches=batches, seed=seed, call=3, max_sweeps=6)
+    assert_same_state(bm, obm)
+    assert st["sweeps"] == ost["sweeps"]
+    assert st["visits"] == ost["visits"]
+    assert st["accepted"] == ost["accepted"]
+    assert st["proposals_moved"] == ost["proposals_moved"]
+    assert st["mdl"] == pytest.approx(ost["mdl"], rel=1e-7)   # both stored as float
+
+
+@pytest.mark.parametrize("algo", [0, 1, 2])
+def test_finetune_replay_bit_exact(S, O, algo):
+    V, s, d, _ = random_graph(700, 6, 21)
+    a = random_assignment(V, 30, 21)
+    g, og, bm, obm = pair(S, O, V, s, d, 30, a)
+    sweeps = 5
+    rec = random_records(sweeps * V, 77)
+    st = S.finetune.run(bm, algo, batches=5, replay=rec, max_sweeps=sweeps)
+    ost = obm.finetune(algo, batches=5, replay=rec, max_sweeps=sweeps)
+    assert_same_state(bm, obm)
+    assert st["accepted"] == ost["accepted"] and st["visits"] == ost["visits"]
+
+
+def test_replay_too_short_is_an_error(S):
+    V, s, d, _ = random_graph(200, 4, 5)
+    g = S.Graph(V, s, d)
+    bm = S.Blockmodel(g, 10, random_assignment(V, 10, 5))
+    with pytest.raises(S.SbpError) as e:
+        S.finetune.asynchronous_gibbs(bm, batches=2, replay=random_records(V // 2, 1), max_sweeps=2)
+    assert e.value.code == 4
+
+
+@pytest.mark.parametrize("approximate", [True, False])
+@pytest.mark.parametrize("V,K,B,merge,seed", [(500, 5, 60, 30, 31), (1500, 8, 700, 350, 32), (300, 4, 9, 4, 33)])
+def test_merge_blocks_bit_exact(S, O, approximate, V, K, B, merge, seed):
+    V, s, d, _ = random_graph(V, K, seed)
+    a = random_assignment(V, B, seed)
+    g, og, bm, obm = pair(S, O, V, s, d, B, a)
+    bm.setNum_blocks_to_merge(merge)
+    obm.set_num_blocks_to_merge(merge)
+    res = S.block_merge.merge_blocks(bm, approximate=approximate, seed=seed, call=2)
+    ores = obm.merge_blocks(approximate=approximate, seed=seed, call=2)
+    assert np.array_equal(res["best"], ores["best"])
+    np.testing.assert_allclose(res["dS"], ores["dS"], rtol=RTOL_MDL, atol=1e-9)
+    assert res["merge_avoided"] == ores["avoided"]
+    assert_same_state(bm, obm)
+
+
+def test_merge_replay_bit_exact(S, O):
+    V, s, d, _ = random_graph(600, 6, 41)
+    a = random_assignment(V, 80, 41)
+    g, og, bm, obm = pair(S, O, V, s, d, 80, a)
+    rec = random_records(80 * 10, 5)
+    bm.setNum_blocks_to_merge(40)
+    obm.set_num_blocks_to_merge(40)
+    res = S.block_merge.merge_blocks(bm, replay=rec)
+    ores = obm.merge_blocks(replay=rec)
+    assert np.array_equal(res["best"], ores["best"])
+    assert_same_state(bm, obm)
+
+
+@pytest.mark.parametrize("algo", ["metropolis_hastings", "async_gibbs", "hybrid_mcmc"])
+def test_partition_bit_exact(S, O, algo):
+    V, s, d, truth = random_graph(500, 5, 51, kmin=6, kmax=40, w=0.85, alpha=10.0)
+    g, og = S.Graph(V, s, d), O.Graph(V, s, d)
+    out, st = S.sbp.stochastic_block_partition(g, algorithm=algo, batches=5, seed=9)
+    code = {"metropolis_hastings": 0, "async_gibbs": 1, "hybrid_mcmc": 2}[algo]
+    oout, ost = O.sbp(og, algo=code, batches=5, seed=9)
+    assert np.array_equal(out, oout)
+    assert st["num_blocks"] == ost["num_blocks"]
+    assert st["mdl"] == ost["mdl"]
+    assert st["visits"] == ost["visits"] and st["accepted"] == ost["accepted"]
+    assert O.nmi(out, truth) > 0.8
+
+
+def test_edge_cases(S, O):
+    # isolated vertices and a vertex with only a self loop
+    s = np.array([0, 1, 2, 5, 5, 6], np.int32)
+    d = np.array([1, 2, 0, 5, 6, 5], np.int32)
+    V = 8
+    a = np.array([0, 1, 2, 0, 1, 2, 0, 1], np.int32)
+    g, og, bm, obm = pair(S, O, V, s, d, 3, a)
+    assert g.E == 6
+    for algo in (0, 1, 2):
+        st = S.finetune.run(bm, algo, batches=2, seed=3, max_sweeps=3)
+        ost = obm.finetune(algo, batches=2, seed=3, max_sweeps=3)
+        assert_same_state(bm, obm)
+        assert st["accepted"] == ost["accepted"]
+    # B == 1: finetune is a no-op (src/finetune.cpp:33-35)
+    one = S.Blockmodel(g, 1, np.zeros(V, np.int32))
+    st = S.finetune.metropolis_hastings(one, seed=1)
+    assert st["sweeps"] == 0 and np.all(one.block_assignment() == 0)
+    # duplicate edges are dropped, first occurrence kept
+    g2 = S.Graph(3, np.array([0, 0, 1, 0], np.int32), np.array([1, 1, 2, 1], np.int32))
+    assert g2.E == 2
+
+
+def test_invalid_arguments_raise(S):
+    with pytest.raises(S.SbpError) as e:
+        S.Graph(3, np.array([0, 5], np.int32), np.array([1, 2], np.int32))
+    assert e.value.code == 1
+    g = S.Graph(3, np.array([0, 1], np.int32), np.array([1, 2], np.int32))
+    with pytest.raises(S.SbpError):
+        S.Blockmodel(g, 2, np.array([0, 1, 2], np.int32))
+    bm = S.Blockmodel(g, 2, np.array([0, 1, 1], np.int32))
+    with pytest.raises(S.SbpError):
+        bm.move_vertex(0, 7)
+
+
+def test_config2_sweeps_keep_invariants(S, O):
+    """20k-vertex, 32-block graph: after Gibbs and hybrid sweeps the counts equal a rebuild and
+    the MDL equals the MDL of the rebuilt blockmodel (size-independent properties)."""
+    import dcsbm
+    V, s, d, truth = dcsbm.config_graph(2)
+    g = S.Graph(V, s, d)
+    a = random_assignment(V, 64, 2)
+    bm = S.Blockmodel(g, 64, a)
+    for algo in ("asynchronous_gibbs", "hybrid_mcmc", "metropolis_hastings"):
+        getattr(S.finetune, algo)(bm, batches=10, seed=5, max_sweeps=2)
+        rebuilt = S.Blockmodel(g, 64, bm.block_assignment())
+        assert np.array_equal(bm.blockmatrix(), rebuilt.blockmatrix())
+        do, di, _ = bm.degrees_all()
+        rdo, rdi, _ = rebuilt.degrees_all()
+        assert np.array_equal(do, rdo) and np.array_equal(di, rdi)
+        assert S.entropy.mdl(bm) == pytest.approx(S.entropy.mdl(rebuilt), rel=1e-12)
