@@ -278,8 +278,9 @@ struct SbpGraph {
 // ------------------------------------------------------------------------------------------
 struct SbpBlockmodel {
   int V = 0, B = 0, ld = 0;
-  DevBuf<int> b, M, MT, d_out, d_in, d;
+  DevBuf<int> b, M, MT, CS, CST, d_out, d_in, d;
   DevBuf<int> prop, last, qr, qs, moved, n_moved;
+  int nch = 0;
   float overall_entropy = 3.40282347e+38f;
   int num_blocks_to_merge = 0;
 
@@ -287,6 +288,9 @@ struct SbpBlockmodel {
     BlockView v;
     v.B = B;
     v.ld = ld;
+    v.nch = nch;
+    v.CS = CS.p;
+    v.CST = CST.p;
     v.b = b.p;
     v.M = M.p;
     v.MT = MT.p;
@@ -312,10 +316,13 @@ struct SbpBlockmodel {
   void set_blocks(int nb) {
     Context& c = Context::get();
     B = nb;
-    ld = ((B + 31) / 32) * 32;
+    ld = ((B + kChunk - 1) / kChunk) * kChunk;
+    nch = (B + kChunk - 1) / kChunk;
     const size_t cells = (size_t)B * (size_t)ld;
     M.reserve(cells);
     MT.reserve(cells);
+    CS.reserve((size_t)B * nch);
+    CST.reserve((size_t)B * nch);
     d_out.reserve(B);
     d_in.reserve(B);
     d.reserve(B);
@@ -332,6 +339,8 @@ static void rebuild(SbpBlockmodel& bm, const SbpGraph& g) {
   const size_t cells = (size_t)bm.B * (size_t)bm.ld;
   SBP_CUDA(cudaMemsetAsync(bm.M.p, 0, cells * sizeof(int), c.stream));
   SBP_CUDA(cudaMemsetAsync(bm.MT.p, 0, cells * sizeof(int), c.stream));
+  SBP_CUDA(cudaMemsetAsync(bm.CS.p, 0, (size_t)bm.B * bm.nch * sizeof(int), c.stream));
+  SBP_CUDA(cudaMemsetAsync(bm.CST.p, 0, (size_t)bm.B * bm.nch * sizeof(int), c.stream));
   SBP_CUDA(cudaMemsetAsync(bm.d_out.p, 0, bm.B * sizeof(int), c.stream));
   SBP_CUDA(cudaMemsetAsync(bm.d_in.p, 0, bm.B * sizeof(int), c.stream));
   if (g.V > 0) {
@@ -610,7 +619,7 @@ static void carry_out_advanced(int B, int to_merge, const std::vector<int>& rptr
     if (m.to < 0) continue;
     const int from = m.from, to = block_map[m.to];
     if (from == to) continue;
-    const double actual = delta(from, to);
+    const double actual = delta(std::min(from, to), std::max(from, to));
     if (!heap.empty() && actual > heap.front().dS) {
       m.dS = actual;
       heap.push_back(m);
@@ -1139,6 +1148,10 @@ SbpStatus sbp_blockmodel_copy(const SbpBlockmodel* src, SbpBlockmodel** out) {
   SBP_CUDA(SBP_COPY_ASYNC(bm->b.p, src->b.p, src->V * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
   SBP_CUDA(SBP_COPY_ASYNC(bm->M.p, src->M.p, cells * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
   SBP_CUDA(SBP_COPY_ASYNC(bm->MT.p, src->MT.p, cells * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(bm->CS.p, src->CS.p, (size_t)src->B * src->nch * sizeof(int), cudaMemcpyDeviceToDevice,
+                          c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(bm->CST.p, src->CST.p, (size_t)src->B * src->nch * sizeof(int), cudaMemcpyDeviceToDevice,
+                          c.stream));
   SBP_CUDA(SBP_COPY_ASYNC(bm->d_out.p, src->d_out.p, src->B * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
   SBP_CUDA(SBP_COPY_ASYNC(bm->d_in.p, src->d_in.p, src->B * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
   SBP_CUDA(SBP_COPY_ASYNC(bm->d.p, src->d.p, src->B * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));

@@ -25,6 +25,8 @@ __global__ void k_rebuild_global(GraphView g, BlockView bm) {
       const int bu = bm.b[__ldg(g.out_idx + e)];
       atomicAdd(bm.M + (size_t)bv * bm.ld + bu, 1);
       atomicAdd(bm.MT + (size_t)bu * bm.ld + bv, 1);
+      chunk_add(bm.CS, bm.nch, bv, bu, 1);
+      chunk_add(bm.CST, bm.nch, bu, bv, 1);
     }
     atomicAdd(bm.d_out + bv, o1 - o0);
     atomicAdd(bm.d_in + bv, (g.in_ptr[v + 1] - g.in_ptr[v]) + g.self[v]);
@@ -52,6 +54,8 @@ __global__ void k_rebuild_smem(GraphView g, BlockView bm) {
       const int row = i / bm.B, col = i - row * bm.B;
       atomicAdd(bm.M + (size_t)row * bm.ld + col, c);
       atomicAdd(bm.MT + (size_t)col * bm.ld + row, c);
+      chunk_add(bm.CS, bm.nch, row, col, c);
+      chunk_add(bm.CST, bm.nch, col, row, c);
     }
   }
 }
@@ -180,6 +184,23 @@ __global__ void k_gibbs_eval(GraphView g, BlockView bm, const int* __restrict__ 
   }
 }
 
+// M[row,col] += delta with the transpose and both chunk sums kept in step (atomic).
+__device__ __forceinline__ void cell_add(const BlockView& bm, int row, int col, int delta) {
+  atomicAdd(bm.M + (size_t)row * bm.ld + col, delta);
+  atomicAdd(bm.MT + (size_t)col * bm.ld + row, delta);
+  chunk_add(bm.CS, bm.nch, row, col, delta);
+  chunk_add(bm.CST, bm.nch, col, row, delta);
+}
+
+// Same for a cell owned by one thread (plain update of M/MT, atomic chunk sums, which lanes share).
+__device__ __forceinline__ void cell_add_owned(const BlockView& bm, int row, int col, int delta) {
+  if (!delta) return;
+  bm.M[(size_t)row * bm.ld + col] += delta;
+  bm.MT[(size_t)col * bm.ld + row] += delta;
+  chunk_add(bm.CS, bm.nch, row, col, delta);
+  chunk_add(bm.CST, bm.nch, col, row, delta);
+}
+
 // Apply accepted moves of one batch.  Every edge incident to a moved vertex moves once from
 // its old cell to its new cell; the result equals the reference's one-by-one application.
 // qr/qs keep the reference's diagonal delta of each move as seen at its turn in vertex order,
@@ -201,10 +222,8 @@ __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, 
       if (u == v) continue;
       const int bo = bm.b[u], pu = prop[u];
       const int bn = pu >= 0 ? pu : bo;
-      atomicAdd(bm.M + (size_t)r * bm.ld + bo, -1);
-      atomicAdd(bm.MT + (size_t)bo * bm.ld + r, -1);
-      atomicAdd(bm.M + (size_t)s * bm.ld + bn, 1);
-      atomicAdd(bm.MT + (size_t)bn * bm.ld + s, 1);
+      cell_add(bm, r, bo, -1);
+      cell_add(bm, s, bn, 1);
       const int ba = (pu >= 0 && u < v) ? pu : bo;
       cr += (ba == r);
       cs += (ba == s);
@@ -214,10 +233,8 @@ __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, 
       const int u = __ldg(g.in_idx + e);
       const int bo = bm.b[u], pu = prop[u];
       if (pu < 0) {
-        atomicAdd(bm.M + (size_t)bo * bm.ld + r, -1);
-        atomicAdd(bm.MT + (size_t)r * bm.ld + bo, -1);
-        atomicAdd(bm.M + (size_t)bo * bm.ld + s, 1);
-        atomicAdd(bm.MT + (size_t)s * bm.ld + bo, 1);
+        cell_add(bm, bo, r, -1);
+        cell_add(bm, bo, s, 1);
       }
       const int ba = (pu >= 0 && u < v) ? pu : bo;
       cr += (ba == r);
@@ -227,10 +244,8 @@ __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, 
     cs = warp_sum_int(cs);
     if (lane == 0) {
       if (self) {
-        atomicAdd(bm.M + (size_t)r * bm.ld + r, -1);
-        atomicAdd(bm.MT + (size_t)r * bm.ld + r, -1);
-        atomicAdd(bm.M + (size_t)s * bm.ld + s, 1);
-        atomicAdd(bm.MT + (size_t)s * bm.ld + s, 1);
+        cell_add(bm, r, r, -1);
+        cell_add(bm, s, s, 1);
       }
       const int k_out = o1 - o0, k_in_self = (i1 - i0) + self;
       atomicAdd(bm.d_out + r, -k_out);
@@ -327,32 +342,21 @@ __global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, i
         const int h = t.list[j];
         const int u = t.keys[h], co = t.cout[h], ci = t.cin[h];
         if (u == r || u == s) continue;
-        if (co) {
-          bm.M[(size_t)r * ld + u] -= co;
-          bm.MT[(size_t)u * ld + r] -= co;
-          bm.M[(size_t)s * ld + u] += co;
-          bm.MT[(size_t)u * ld + s] += co;
-        }
-        if (ci) {
-          bm.M[(size_t)u * ld + r] -= ci;
-          bm.MT[(size_t)r * ld + u] -= ci;
-          bm.M[(size_t)u * ld + s] += ci;
-          bm.MT[(size_t)s * ld + u] += ci;
-        }
+        cell_add_owned(bm, r, u, -co);
+        cell_add_owned(bm, s, u, co);
+        cell_add_owned(bm, u, r, -ci);
+        cell_add_owned(bm, u, s, ci);
       }
+      __syncwarp();
       if (lane == 0) {
         const int d_rr = -mc.co_r - mc.ci_r - self;
         const int d_rs = -mc.co_s + mc.ci_r;
         const int d_sr = mc.co_r - mc.ci_s;
         const int d_ss = mc.co_s + mc.ci_s + self;
-        bm.M[(size_t)r * ld + r] += d_rr;
-        bm.MT[(size_t)r * ld + r] += d_rr;
-        bm.M[(size_t)r * ld + s] += d_rs;
-        bm.MT[(size_t)s * ld + r] += d_rs;
-        bm.M[(size_t)s * ld + r] += d_sr;
-        bm.MT[(size_t)r * ld + s] += d_sr;
-        bm.M[(size_t)s * ld + s] += d_ss;
-        bm.MT[(size_t)s * ld + s] += d_ss;
+        cell_add_owned(bm, r, r, d_rr);
+        cell_add_owned(bm, r, s, d_rs);
+        cell_add_owned(bm, s, r, d_sr);
+        cell_add_owned(bm, s, s, d_ss);
         bm.b[v] = s;
         bm.d_out[r] -= k_out;
         bm.d_out[s] += k_out;
@@ -404,27 +408,19 @@ __global__ void k_move_vertex(GraphView g, BlockView bm, int v, int s, int cap, 
     const int h = t.list[j];
     const int u = t.keys[h], co = t.cout[h], ci = t.cin[h];
     if (u == r || u == s) continue;
-    bm.M[(size_t)r * ld + u] -= co;
-    bm.MT[(size_t)u * ld + r] -= co;
-    bm.M[(size_t)s * ld + u] += co;
-    bm.MT[(size_t)u * ld + s] += co;
-    bm.M[(size_t)u * ld + r] -= ci;
-    bm.MT[(size_t)r * ld + u] -= ci;
-    bm.M[(size_t)u * ld + s] += ci;
-    bm.MT[(size_t)s * ld + u] += ci;
+    cell_add_owned(bm, r, u, -co);
+    cell_add_owned(bm, s, u, co);
+    cell_add_owned(bm, u, r, -ci);
+    cell_add_owned(bm, u, s, ci);
   }
   __syncwarp();
   if (lane == 0) {
     const int d_rr = -mc.co_r - mc.ci_r - self, d_rs = -mc.co_s + mc.ci_r;
     const int d_sr = mc.co_r - mc.ci_s, d_ss = mc.co_s + mc.ci_s + self;
-    bm.M[(size_t)r * ld + r] += d_rr;
-    bm.MT[(size_t)r * ld + r] += d_rr;
-    bm.M[(size_t)r * ld + s] += d_rs;
-    bm.MT[(size_t)s * ld + r] += d_rs;
-    bm.M[(size_t)s * ld + r] += d_sr;
-    bm.MT[(size_t)r * ld + s] += d_sr;
-    bm.M[(size_t)s * ld + s] += d_ss;
-    bm.MT[(size_t)s * ld + s] += d_ss;
+    cell_add_owned(bm, r, r, d_rr);
+    cell_add_owned(bm, r, s, d_rs);
+    cell_add_owned(bm, s, r, d_sr);
+    cell_add_owned(bm, s, s, d_ss);
     bm.b[v] = s;
     bm.d_out[r] -= k_out;
     bm.d_out[s] += k_out;
@@ -620,7 +616,8 @@ __global__ void k_merge_propose(BlockView bm, Csr rows, Csr cols, RngParams rng,
         continue;
       }
       seen[nseen++] = s;
-      const double dS = merge_delta(bm, rows, cols, r, s, lane);
+      // same value for r->s and s->r; one fixed orientation makes mutual pairs tie exactly
+      const double dS = merge_delta(bm, rows, cols, min(r, s), max(r, s), lane);
       if (dS < bdS) {
         bdS = dS;
         best = s;

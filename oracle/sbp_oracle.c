@@ -30,6 +30,11 @@
  *       and then column t ascending (a canonical order; the reference walks robin_map
  *       buckets), and the dead `std::rand() <= B/(d_t+B)` branch (src/common.cpp:154, true
  *       only when rand() returns 0) is not taken.
+ *   D3  a vertex-move delta-MDL whose magnitude is at most 2^-40 * T * log(max(E,2)) is set to
+ *       exactly 0, T being the integer sum of old + new counts of the changed cells and of the
+ *       old + new out/in degrees of r and s.  A mathematically zero change (a symmetric move)
+ *       then reads as 0.0 whatever the summation order, which keeps the Metropolis-Hastings
+ *       early stop (`delta == 0.0`, src/finetune.cpp:147) identical across implementations.
  *   Sorts that the reference does with std::sort (unstable) break ties by index.
  */
 #include <math.h>
@@ -389,8 +394,9 @@ static void vertex_delta(Delta *dl, const SbpoBM *bm, const SbpoGraph *g, int v,
 typedef struct { int s, k_out, k_in, k; } Proposal;   /* utils::ProposalAndEdgeCounts */
 
 /* entropy::delta_mdl(Blockmodel, Delta, Proposal) (src/entropy.cpp:296-401), FP64, with Q1. */
-static double delta_mdl_move(const SbpoBM *bm, const Delta *dl, const Proposal *p) {
+static double delta_mdl_move(const SbpoBM *bm, const Delta *dl, const Proposal *p, int E) {
     int r = dl->r, s = dl->s, B = bm->B;
+    int64_t T = 0;   /* D3 scale */
     int din_shift = p->k_in + dl->self_w, dout_shift = p->k_out;
 #define DIN_NEW(i) ((double)(bm->d_in[i] + ((i) == r ? -din_shift : ((i) == s ? din_shift : 0))))
 #define DOUT_NEW(i) ((double)(bm->d_out[i] + ((i) == r ? -dout_shift : ((i) == s ? dout_shift : 0))))
@@ -402,7 +408,9 @@ static double delta_mdl_move(const SbpoBM *bm, const Delta *dl, const Proposal *
             double val = (double)MAT(bm, row, col);
             dS += cell_entropy(val, (double)bm->d_in[col], (double)bm->d_out[row]);
             dS -= cell_entropy(val + change, DIN_NEW(col), DOUT_NEW(row));
+            if (change != 0) T += 2 * (int64_t)MAT(bm, row, col) + change;
         }
+    T += 2 * ((int64_t)bm->d_out[r] + bm->d_out[s] + bm->d_in[r] + bm->d_in[s]);
     for (int pass = 0; pass < 2; ++pass) {           /* rows r and s */
         int row = pass == 0 ? r : s;
         for (int col = 0; col < B; ++col) {
@@ -423,6 +431,7 @@ static double delta_mdl_move(const SbpoBM *bm, const Delta *dl, const Proposal *
     }
 #undef DIN_NEW
 #undef DOUT_NEW
+    if (fabs(dS) <= 0x1p-40 * (double)T * log(E > 2 ? (double)E : 2.0)) dS = 0.0;   /* D3 */
     return dS;
 }
 
@@ -555,7 +564,7 @@ static Eval eval_vertex(const SbpoBM *bm, const SbpoGraph *g, int v, const uint3
     Delta dl;
     vertex_delta(&dl, bm, g, v, r, p.s);
     ev.H = hastings_move(bm, g, &dl, v, &p);
-    ev.dS = delta_mdl_move(bm, &dl, &p);
+    ev.dS = delta_mdl_move(bm, &dl, &p, g->E);
     delta_free(&dl);
     double u = sbpo_u53(x[2], x[3]);
     double ap = exp(-3.0 * ev.dS) * ev.H;
@@ -579,7 +588,7 @@ double sbpo_delta_mdl_move(const SbpoBM *bm, const SbpoGraph *g, int v, int s, d
     p.k_in = (g->in_ptr[v + 1] - g->in_ptr[v]) - g->self[v]; p.k = p.k_out + p.k_in;
     Delta dl;
     vertex_delta(&dl, bm, g, v, r, s);
-    double dS = delta_mdl_move(bm, &dl, &p);
+    double dS = delta_mdl_move(bm, &dl, &p, g->E);
     if (hastings) *hastings = hastings_move(bm, g, &dl, v, &p);
     delta_free(&dl);
     return dS;
@@ -635,7 +644,7 @@ static int mh_visit(SbpoBM *bm, const SbpoGraph *g, const SbpoRng *rng, int v, i
     Delta dl;
     vertex_delta(&dl, bm, g, v, r, p.s);
     double H = hastings_move(bm, g, &dl, v, &p);
-    double dS = delta_mdl_move(bm, &dl, &p);
+    double dS = delta_mdl_move(bm, &dl, &p, g->E);
     double u = sbpo_u53(x[2], x[3]);
     double ap = exp(-3.0 * dS) * H;
     ap = (ap >= 1.0) ? 1.0 : ap;
@@ -786,7 +795,12 @@ static double merge_delta_mdl(const SbpoBM *bm, const Delta *dl, int k_out, int 
     return dS;
 }
 
+/* Merge delta-MDL of r and s.  It is the same for r -> s and s -> r (the merged block is the
+ * same); it is evaluated in one fixed orientation (lower id into higher id) so that a mutual
+ * best pair ties exactly and the carry-out order of a tie is decided by index, on every
+ * implementation alike. */
 double sbpo_merge_delta_mdl(const SbpoBM *bm, int r, int s) {
+    if (r > s) { int t = r; r = s; s = t; }
     Delta dl;
     merge_delta(&dl, bm, r, s);
     double dS = merge_delta_mdl(bm, &dl, (int)row_sum(bm, r, -1), (int)col_sum(bm, r, -1));
@@ -894,7 +908,7 @@ static int carry_out_advanced(SbpoBM *bm, const double *dS, const int *best) {
         Delta dl;
         merge_delta(&dl, bm, from, to);
         int prop_self = MAT(bm, to, to) + delta_get(&dl, to, to);
-        double actual = merge_delta_mdl(bm, &dl, k_out, k_in);
+        double actual = sbpo_merge_delta_mdl(bm, from, to);
         if (n > 0 && actual > heap[0].dS) {
             merge.dS = actual;
             h_push(heap, &n, merge);
