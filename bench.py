@@ -211,10 +211,12 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     visits, outs = 0, []
     e0.record(ext)
+    step_s = []
     for k in range(a.steps):
         out, st = run(k)
         visits += st["visits"]
         outs.append((out, st))
+        step_s.append(round(st["total_seconds"], 4))
     e1.record(ext)
     barrier()
     prof1 = S.profile_read()
@@ -276,7 +278,8 @@ def main():
         quality = {"final_blocks": int(last_st.get("num_blocks", 0)), "final_mdl": float(last_st.get("mdl", 0.0)),
                    "nmi_vs_planted": float(O.nmi(last_out, truth)) if last_out is not None else None,
                    "sweeps_per_step": int(last_st.get("sweeps", 0)),
-                   "seconds_per_step_device": ms_max / 1e3 / max(1, a.steps)}
+                   "seconds_per_step_device": ms_max / 1e3 / max(1, a.steps),
+                   "partition_seconds_each_step": step_s}
         base = reference_baseline(V, src, dst, truth, 12.0) if world == 1 else None
         launches = int(prof1["launches"] - prof0["launches"])
         line = {

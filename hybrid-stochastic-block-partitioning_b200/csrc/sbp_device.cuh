@@ -81,10 +81,11 @@ __device__ __forceinline__ int random_block(int r, int B, uint32_t x) {
 // FP64 helpers: g(x) = x log x and accurate differences g(a) - g(b).
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ double xlogx(double x) { return x > 0.0 ? x * log(x) : 0.0; }
+// g(a) - g(b) = (a - b) log a + b (log a - log b) for a, b >= 0 without branches: a zero side
+// is replaced by 1 inside the logs, which leaves exactly the other side's g term; a == b gives 0.
 __device__ __forceinline__ double dxlogx(double a, double b) {
-  if (a == b) return 0.0;
-  if (a <= 0.0 || b <= 0.0) return xlogx(a) - xlogx(b);
-  return (a - b) * log(a) + b * log1p((a - b) / b);
+  const double sa = a > 0.0 ? a : 1.0, sb = b > 0.0 ? b : 1.0;
+  return (a - b) * log(sa) + b * log1p((sa - sb) / sb);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -331,48 +332,83 @@ __device__ __forceinline__ MoveCounts corner_counts(const WarpTable& t, int r, i
   return mc;
 }
 
-// Proposal for vertex v (src/common.cpp:131-182 with canonical order).
-__device__ __forceinline__ int propose_block(const GraphView& g, const BlockView& bm, int v, int r, int k_out,
-                                             int k_in, uint4 x, int lane, int* status) {
-  const int k = k_out + k_in;
-  if (k == 0) return random_block(r, bm.B, x.y);
-  const int idx = (int)scale32(x.x, k);
-  const int nbr = idx < k_out ? __ldg(g.out_idx + g.out_ptr[v] + idx) : __ldg(g.in_idx + g.in_ptr[v] + (idx - k_out));
-  const int t = bm.b[nbr];
-  const int dot = bm.d_out[t];
-  const long long total = (long long)dot + (long long)bm.d_in[t];
-  long long target = scale32(x.y, total);
-  int s;
-  if (target < dot) s = warp_select_chunked(bm.M + (size_t)t * bm.ld, bm.CS + (size_t)t * bm.nch, bm.nch, target, lane);
-  else s = warp_select_chunked(bm.MT + (size_t)t * bm.ld, bm.CST + (size_t)t * bm.nch, bm.nch, target - dot, lane);
-  if (s < 0) {
-    if (lane == 0) atomicOr(status, kErrScan);
-    s = r;
+// Warp-aggregated insertion of one element per lane; lanes holding the same block add their
+// out- and in-multiplicities once.
+__device__ __forceinline__ void table_add_dir(const WarpTable& t, int key, bool valid, bool incoming, int* status) {
+  const int k = valid ? key : -2;
+  const unsigned peers = __match_any_sync(kFull, k);
+  const unsigned in_mask = __ballot_sync(kFull, valid && incoming);
+  const int lane = threadIdx.x & 31;
+  if (valid && (__ffs(peers) - 1) == lane) {
+    const int slot = table_slot(t, key, status);
+    if (slot >= 0) {
+      const int nin = __popc(peers & in_mask), nout = __popc(peers) - nin;
+      if (nout) atomicAdd(&t.cout[slot], nout);
+      if (nin) atomicAdd(&t.cin[slot], nin);
+    }
   }
-  return s;
 }
 
 // Full evaluation of vertex v against the current state, table left filled on return
 // (caller resets it). Every lane returns the same result.
+//  1. one pass over the virtual neighbour list (out list incl. the self loop, then in list
+//     without it) gathers every neighbour's block into the table; the proposal's neighbour
+//     (element floor(x0 * k)) is one of these elements, so its block comes from the same gather;
+//  2. the multinomial walk over M[t,:] + M[:,t] picks s;
+//  3. one load round over the distinct neighbour blocks gives the Hastings sums and the changed
+//     cells; the corner cells, degree terms and the net-zero double count are spread over lanes.
 __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const BlockView& bm, int v, uint4 x,
                                                       const WarpTable& t, int lane, int* status, int* r_out,
                                                       int* k_out_out, int* k_in_out) {
   EvalResult res;
   const int r = bm.b[v];
-  const int k_out = g.out_ptr[v + 1] - g.out_ptr[v];
+  const int o0 = g.out_ptr[v], o1 = g.out_ptr[v + 1];
+  const int i0 = g.in_ptr[v], i1 = g.in_ptr[v + 1];
   const int self = g.self[v];
-  const int k_in = g.in_ptr[v + 1] - g.in_ptr[v];
+  const int k_out = o1 - o0, k_in = i1 - i0, k = k_out + k_in;
   *r_out = r;
   *k_out_out = k_out;
   *k_in_out = k_in;
-  const int s = propose_block(g, bm, v, r, k_out, k_in, x, lane, status);
-  res.s = s;
   res.accepted = 0;
   res.dS = 0.0;
   res.H = 1.0;
-  if (s == r) return res;
+  const int idx = k > 0 ? (int)scale32(x.x, k) : -1;
+  int tblk = -1;
+  for (int base = 0; base < k; base += 2 * kWarp) {   // two elements per lane in flight
+    const int e0 = base + lane, e1 = base + kWarp + lane;
+    int u0 = -1, u1 = -1;
+    if (e0 < k) u0 = e0 < k_out ? __ldg(g.out_idx + o0 + e0) : __ldg(g.in_idx + i0 + (e0 - k_out));
+    if (e1 < k) u1 = e1 < k_out ? __ldg(g.out_idx + o0 + e1) : __ldg(g.in_idx + i0 + (e1 - k_out));
+    const int b0 = u0 >= 0 ? bm.b[u0] : -1;
+    const int b1 = u1 >= 0 ? bm.b[u1] : -1;
+    if (idx >= base && idx < base + kWarp) tblk = __shfl_sync(kFull, b0, idx - base);
+    if (idx >= base + kWarp && idx < base + 2 * kWarp) tblk = __shfl_sync(kFull, b1, idx - base - kWarp);
+    table_add_dir(t, b0, u0 >= 0 && u0 != v, e0 >= k_out, status);
+    table_add_dir(t, b1, u1 >= 0 && u1 != v, e1 >= k_out, status);
+  }
+  if (lane == 0 && self) table_slot(t, r, status);
 
-  build_table(g, bm, v, r, t, lane, status);
+  int s;
+  if (k == 0) {
+    s = random_block(r, bm.B, x.y);
+  } else {
+    const int dot = bm.d_out[tblk];
+    const long long total = (long long)dot + (long long)bm.d_in[tblk];
+    const long long target = scale32(x.y, total);
+    if (target < dot)
+      s = warp_select_chunked(bm.M + (size_t)tblk * bm.ld, bm.CS + (size_t)tblk * bm.nch, bm.nch, target, lane);
+    else
+      s = warp_select_chunked(bm.MT + (size_t)tblk * bm.ld, bm.CST + (size_t)tblk * bm.nch, bm.nch, target - dot,
+                              lane);
+    if (s < 0) {
+      if (lane == 0) atomicOr(status, kErrScan);
+      s = r;
+    }
+  }
+  res.s = s;
+  if (s == r) return res;
+  __syncwarp();
+
   const MoveCounts mc = corner_counts(t, r, s);
   const int B = bm.B, ld = bm.ld;
   const int d_rr = -mc.co_r - mc.ci_r - self;
@@ -382,6 +418,7 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
   const int M_rr = bm.M[(size_t)r * ld + r], M_rs = bm.M[(size_t)r * ld + s];
   const int M_sr = bm.M[(size_t)s * ld + r], M_ss = bm.M[(size_t)s * ld + s];
   const int dout_r = bm.d_out[r], dout_s = bm.d_out[s], din_r = bm.d_in[r], din_s = bm.d_in[s];
+  const int kin_self = k_in + self;
 
   double fwd = 0.0, bwd = 0.0, dS = 0.0;
   long long T = 0;   // integer scale of the changed cells and degrees (zero snap below)
@@ -394,58 +431,50 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
     const int h = t.list[i];
     const int u = t.keys[h];
     const int co = t.cout[h], ci = t.cin[h];
-    const int M_su = Ms[u], M_us = MTs[u];
+    const int M_su = Ms[u], M_us = MTs[u], M_ru = Mr[u], M_ur = MTr[u];
     const int du = bm.d[u];
-    const double c = (double)(co + ci + (u == r ? self : 0));
+    const bool is_r = (u == r), is_s = (u == s), corner = is_r || is_s;
+    const double c = (double)(co + ci + (is_r ? self : 0));
     fwd += c * (M_su + M_us + 1.0) / ((double)du + (double)B);
-    double bw;
-    int nd;
-    if (u == r) {
-      bw = (double)(M_rr + d_rr) + (double)(M_rr + d_rr) + 1.0;
-      nd = (dout_r - k_out) + (din_r - k_in) - (M_rr + d_rr);
-    } else if (u == s) {
-      bw = (double)(M_rs + d_rs) + (double)(M_sr + d_sr) + 1.0;
-      nd = (dout_s + k_out) + (din_s + k_in) - (M_ss + d_ss);
-    } else {
-      const int M_ru = Mr[u], M_ur = MTr[u];
-      bw = (double)(M_ru - co) + (double)(M_ur - ci) + 1.0;
-      nd = du;
-      if (co) {
-        dS += dxlogx(M_ru, M_ru - co) + dxlogx(M_su, M_su + co);
-        T += 2LL * (M_ru + M_su);
-      }
-      if (ci) {
-        dS += dxlogx(M_ur, M_ur - ci) + dxlogx(M_us, M_us + ci);
-        T += 2LL * (M_ur + M_us);
-      }
-    }
+    const double bw = is_r ? (double)(M_rr + d_rr) + (double)(M_rr + d_rr) + 1.0
+                    : is_s ? (double)(M_rs + d_rs) + (double)(M_sr + d_sr) + 1.0
+                           : (double)(M_ru - co) + (double)(M_ur - ci) + 1.0;
+    const int nd = is_r ? (dout_r - k_out) + (din_r - k_in) - (M_rr + d_rr)
+                 : is_s ? (dout_s + k_out) + (din_s + k_in) - (M_ss + d_ss) : du;
     bwd += c * bw / ((double)nd + (double)B);
+    // changed non-corner cells (r,u) (s,u) (u,r) (u,s); corner cells are handled below
+    const int co_c = corner ? 0 : co, ci_c = corner ? 0 : ci;
+    dS += dxlogx(M_ru, M_ru - co_c) + dxlogx(M_su, M_su + co_c) + dxlogx(M_ur, M_ur - ci_c) +
+          dxlogx(M_us, M_us + ci_c);
+    T += (co_c ? 2LL * (M_ru + M_su) : 0LL) + (ci_c ? 2LL * (M_ur + M_us) : 0LL);
+  }
+  {
+    // one corner-cell or degree term per lane (lanes 0-7), the double count of a present
+    // net-zero (r,s) / (s,r) Delta cell on lanes 8 and 9; selects, no divergent branches
+    const int ca = lane == 0 ? M_rr : lane == 1 ? M_rs : lane == 2 ? M_sr : lane == 3 ? M_ss
+                 : lane == 4 ? dout_r : lane == 5 ? dout_s : lane == 6 ? din_r : lane == 7 ? din_s : 0;
+    const int cd = lane == 0 ? d_rr : lane == 1 ? d_rs : lane == 2 ? d_sr : lane == 3 ? d_ss
+                 : lane == 4 ? -k_out : lane == 5 ? k_out : lane == 6 ? -kin_self : lane == 7 ? kin_self : 0;
+    const double sign = lane < 4 ? 1.0 : -1.0;
+    dS += sign * dxlogx((double)ca, (double)(ca + cd));
+    T += lane < 4 ? (cd ? 2LL * ca + cd : 0LL) : 2LL * ca;
+    const bool q_rs = (mc.co_s > 0 || mc.ci_r > 0) && d_rs == 0 && M_rs > 0;
+    const bool q_sr = (mc.co_r > 0 || mc.ci_s > 0) && d_sr == 0 && M_sr > 0;
+    const int qm = lane == 8 ? (q_rs ? M_rs : 0) : lane == 9 ? (q_sr ? M_sr : 0) : 0;
+    const double x1 = qm ? (lane == 8 ? (double)kin_self / (double)din_s : -(double)kin_self / (double)din_r) : 0.0;
+    const double x2 = qm ? (lane == 8 ? -(double)k_out / (double)dout_r : (double)k_out / (double)dout_s) : 0.0;
+    dS += (double)qm * (log1p(x1) + log1p(x2));
   }
   fwd = warp_sum(fwd);
   bwd = warp_sum(bwd);
   dS = warp_sum(dS);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) T += __shfl_xor_sync(kFull, T, o);
-
-  // corner cells, degree terms and the double-count of net-zero Delta cells
-  const int kin_self = k_in + self;
-  dS += dxlogx(M_rr, M_rr + d_rr) + dxlogx(M_rs, M_rs + d_rs) + dxlogx(M_sr, M_sr + d_sr) + dxlogx(M_ss, M_ss + d_ss);
-  dS -= dxlogx(dout_r, dout_r - k_out) + dxlogx(dout_s, dout_s + k_out);
-  dS -= dxlogx(din_r, din_r - kin_self) + dxlogx(din_s, din_s + kin_self);
-  if ((mc.co_s > 0 || mc.ci_r > 0) && d_rs == 0 && M_rs > 0)
-    dS += (double)M_rs * (log1p((double)kin_self / (double)din_s) + log1p(-(double)k_out / (double)dout_r));
-  if ((mc.co_r > 0 || mc.ci_s > 0) && d_sr == 0 && M_sr > 0)
-    dS += (double)M_sr * (log1p(-(double)kin_self / (double)din_r) + log1p((double)k_out / (double)dout_s));
   // A mathematically zero change reads as exactly 0 whatever the summation order: the
   // Metropolis-Hastings early stop tests `delta == 0.0` (src/finetune.cpp:147).
-  if (d_rr) T += 2LL * M_rr + d_rr;
-  if (d_rs) T += 2LL * M_rs + d_rs;
-  if (d_sr) T += 2LL * M_sr + d_sr;
-  if (d_ss) T += 2LL * M_ss + d_ss;
-  T += 2LL * ((long long)dout_r + dout_s + din_r + din_s);
   if (fabs(dS) <= 0x1p-40 * (double)T * log(g.E > 2 ? (double)g.E : 2.0)) dS = 0.0;
 
-  const double H = (k_out + k_in == 0) ? 1.0 : bwd / fwd;
+  const double H = (k == 0) ? 1.0 : bwd / fwd;
   double ap = exp(-3.0 * dS) * H;
   ap = ap >= 1.0 ? 1.0 : ap;
   res.dS = dS;

@@ -180,7 +180,7 @@ static int pow2_at_least(int x) {
 }
 
 constexpr int kLightCap = 256;        // per-warp table slots for light vertices
-constexpr int kLightMaxK = kLightCap / 2;
+constexpr int kLightCapMax = 512;     // largest per-warp table of the 8-warp evaluation CTA
 constexpr int kLightWarps = 8;
 constexpr int kMaxCap = 8192;         // largest per-warp table
 constexpr size_t kSmemBudget = 200 * 1024;
@@ -203,12 +203,13 @@ struct BatchPlan {
 struct SbpGraph {
   int V = 0;
   long long E = 0;
-  DevBuf<int> out_ptr, out_idx, in_ptr, in_idx, identity, high_dev;
+  DevBuf<int> out_ptr, out_idx, out_src, in_ptr, in_idx, identity, high_dev;
   DevBuf<unsigned char> self;
   std::vector<int> h_k;        // k_out + k_in per vertex (self loop counted once, on the out side)
   std::vector<int> high, low;  // hybrid split
   int max_k = 0;
   int heavy_cap = 512;         // table slots for heavy vertices
+  int light_cap = 256;         // table slots per warp for light vertices (k <= light_cap / 2)
   std::unordered_map<long long, std::unique_ptr<BatchPlan>> plans;
 
   GraphView view() const {
@@ -252,14 +253,14 @@ struct SbpGraph {
         const int start = bt * batch_size, end = std::min(n, (bt + 1) * batch_size);
         p->light_begin.push_back((int)order.size());
         for (int i = start; i < end; ++i)
-          if (h_k[list[i]] <= kLightMaxK) order.push_back(list[i]);
+          if (h_k[list[i]] <= light_cap / 2) order.push_back(list[i]);
         p->light_n.push_back((int)order.size() - p->light_begin.back());
         double lb = 0.0;   // 12 B (CSR offsets + b[v]) + 8 B per neighbour (id + block gather)
         for (int i = p->light_begin.back(); i < (int)order.size(); ++i) lb += 12.0 + 8.0 * h_k[order[i]];
         p->light_bytes.push_back(lb);
         p->heavy_begin.push_back((int)order.size());
         for (int i = start; i < end; ++i)
-          if (h_k[list[i]] > kLightMaxK) order.push_back(list[i]);
+          if (h_k[list[i]] > light_cap / 2) order.push_back(list[i]);
         p->heavy_n.push_back((int)order.size() - p->heavy_begin.back());
         p->max_batch = std::max(p->max_batch, end - start);
       }
@@ -279,7 +280,9 @@ struct SbpGraph {
 struct SbpBlockmodel {
   int V = 0, B = 0, ld = 0;
   DevBuf<int> b, M, MT, CS, CST, d_out, d_in, d;
-  DevBuf<int> prop, last, qr, qs, moved, n_moved;
+  DevBuf<int> prop, qr, qs, moved, n_moved;   // n_moved: two slots, alternating per batch
+  DevBuf<unsigned long long> last;           // (batch generation << 32 | last mover) per block
+  unsigned gen = 0;                          // batch generation
   int nch = 0;
   float overall_entropy = 3.40282347e+38f;
   int num_blocks_to_merge = 0;
@@ -308,9 +311,9 @@ struct SbpBlockmodel {
     qr.reserve(V);
     qs.reserve(V);
     moved.reserve(V);
-    n_moved.reserve(1);
+    n_moved.reserve(2);
     SBP_CUDA(cudaMemsetAsync(prop.p, 0xff, sizeof(int) * V, c.stream));
-    SBP_CUDA(cudaMemsetAsync(n_moved.p, 0, sizeof(int), c.stream));
+    SBP_CUDA(cudaMemsetAsync(n_moved.p, 0, 2 * sizeof(int), c.stream));
   }
 
   void set_blocks(int nb) {
@@ -327,7 +330,7 @@ struct SbpBlockmodel {
     d_in.reserve(B);
     d.reserve(B);
     last.reserve(B);
-    SBP_CUDA(cudaMemsetAsync(last.p, 0xff, sizeof(int) * B, c.stream));
+    SBP_CUDA(cudaMemsetAsync(last.p, 0, sizeof(unsigned long long) * B, c.stream));
   }
 };
 
@@ -361,9 +364,9 @@ static double mdl(SbpBlockmodel& bm, const SbpGraph& g) {
   Context& c = Context::get();
   const int grid = c.npartial;
   if ((long long)bm.B * bm.B <= 4LL * g.E) k_mdl_cells<<<grid, 256, 0, c.stream>>>(bm.view(), c.partial);
-  else k_mdl_edges<<<grid, 256, 0, c.stream>>>(g.view(), bm.view(), c.partial);
+  else k_mdl_edges<<<grid, 256, 0, c.stream>>>(g.view(), bm.view(), g.out_src.p, c.partial);
   SBP_CHECK_LAUNCH();
-  k_mdl_final<<<1, 32, 0, c.stream>>>(c.partial, grid, g.V, g.E, bm.B, c.scalar);
+  k_mdl_final<<<1, 256, 0, c.stream>>>(c.partial, grid, g.V, g.E, bm.B, c.scalar);
   SBP_CHECK_LAUNCH();
   double out = 0.0;
   SBP_CUDA(SBP_COPY_ASYNC(&out, c.scalar, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -421,13 +424,17 @@ static MhResult mh_pass(SbpBlockmodel& bm, const SbpGraph& g, const int* verts, 
   return res;
 }
 
-// One asynchronous-Gibbs batch: evaluate (light + heavy vertices), then apply.
+// One asynchronous-Gibbs batch: evaluate every vertex of the batch, then apply the moves.
 static void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, int bt, RngParams rng,
                         int sweep) {
   Context& c = Context::get();
   const int nl = plan.light_n[bt], nh = plan.heavy_n[bt];
+  const int slot = bm.gen & 1;
+  int* n_cur = bm.n_moved.p + slot;
+  int* n_next = bm.n_moved.p + (slot ^ 1);
   if (nl > 0) {
-    const size_t smem = (size_t)table_ints(kLightCap) * sizeof(int) * kLightWarps;
+    const size_t smem = (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps;
+    set_smem_limit((const void*)k_gibbs_eval, smem);
     const int grid = grid_for(nl, kLightWarps, 64 * c.num_sms);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (g_prof.on) {
@@ -436,8 +443,8 @@ static void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& p
       SBP_CUDA(cudaEventRecord(e0, c.stream));
     }
     k_gibbs_eval<<<grid, kLightWarps * 32, smem, c.stream>>>(g.view(), bm.view(), plan.order.p + plan.light_begin[bt],
-                                                            nl, rng, sweep, bm.prop.p, bm.moved.p, bm.n_moved.p,
-                                                            c.counters, kLightCap, c.status);
+                                                            nl, rng, sweep, bm.prop.p, bm.moved.p, n_cur,
+                                                            c.counters, g.light_cap, c.status);
     SBP_CHECK_LAUNCH();
     if (g_prof.on) {
       SBP_CUDA(cudaEventRecord(e1, c.stream));
@@ -449,24 +456,21 @@ static void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& p
   }
   if (nh > 0) {
     const size_t smem = (size_t)table_ints(g.heavy_cap) * sizeof(int);
-    set_smem_limit((const void*)k_gibbs_eval, std::max(smem, (size_t)table_ints(kLightCap) * sizeof(int) * kLightWarps));
+    set_smem_limit((const void*)k_gibbs_eval, std::max(smem, (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps));
     k_gibbs_eval<<<grid_for(nh, 1, 64 * c.num_sms), 32, smem, c.stream>>>(
-        g.view(), bm.view(), plan.order.p + plan.heavy_begin[bt], nh, rng, sweep, bm.prop.p, bm.moved.p,
-        bm.n_moved.p, c.counters, g.heavy_cap, c.status);
+        g.view(), bm.view(), plan.order.p + plan.heavy_begin[bt], nh, rng, sweep, bm.prop.p, bm.moved.p, n_cur,
+        c.counters, g.heavy_cap, c.status);
     SBP_CHECK_LAUNCH();
   }
   const int batch = nl + nh;
+  const unsigned gen = ++bm.gen;
   const int gw = grid_for((long long)batch * 32, 256, 64 * c.num_sms);
-  k_apply_edges<<<gw, 256, 0, c.stream>>>(g.view(), bm.view(), bm.moved.p, bm.n_moved.p, bm.prop.p, bm.qr.p, bm.qs.p,
-                                          bm.last.p);
+  k_apply_edges<<<gw, 256, 0, c.stream>>>(g.view(), bm.view(), bm.moved.p, n_cur, bm.prop.p, bm.qr.p, bm.qs.p,
+                                          bm.last.p, gen);
   SBP_CHECK_LAUNCH();
-  const int gt = grid_for(batch, 256, 64 * c.num_sms);
-  k_apply_degrees<<<gt, 256, 0, c.stream>>>(bm.view(), bm.moved.p, bm.n_moved.p, bm.prop.p, bm.qr.p, bm.qs.p,
-                                            bm.last.p);
+  k_apply_finish<<<grid_for(batch, 256, 64 * c.num_sms), 256, 0, c.stream>>>(
+      bm.view(), bm.moved.p, n_cur, n_next, bm.prop.p, bm.qr.p, bm.qs.p, bm.last.p, gen);
   SBP_CHECK_LAUNCH();
-  k_apply_finish<<<gt, 256, 0, c.stream>>>(bm.view(), bm.moved.p, bm.n_moved.p, bm.prop.p, bm.last.p);
-  SBP_CHECK_LAUNCH();
-  SBP_CUDA(cudaMemsetAsync(bm.n_moved.p, 0, sizeof(int), c.stream));
 }
 
 struct ReplayDev {
@@ -558,6 +562,27 @@ struct MergeScratch {
   DevBuf<double> best_dS;
 };
 
+// block_map of the reference's carry-out loops: block_map[x] is the current name of x's group,
+// and merging `from` into `to` renames every entry equal to `from` (src/blockmodel/blockmodel.cpp:
+// 61-66).  Member lists make a rename cost the size of the renamed group instead of O(B).
+struct GroupMap {
+  std::vector<int> name;                    // block -> group name
+  std::vector<std::vector<int>> members;    // group name -> blocks carrying it
+  explicit GroupMap(int B) : name(B), members(B) {
+    for (int i = 0; i < B; ++i) {
+      name[i] = i;
+      members[i].push_back(i);
+    }
+  }
+  void rename(int from, int to) {
+    auto& src = members[from];
+    auto& dst = members[to];
+    for (int x : src) name[x] = to;
+    dst.insert(dst.end(), src.begin(), src.end());
+    std::vector<int>().swap(src);
+  }
+};
+
 // block_merge::carry_out_best_merges_advanced (src/block_merge.cpp:123-217) on a host copy
 // of the sparse matrix (serial by construction); heap order (dS, block).
 static void carry_out_advanced(int B, int to_merge, const std::vector<int>& rptr, const std::vector<int>& ridx,
@@ -609,15 +634,14 @@ static void carry_out_advanced(int B, int to_merge, const std::vector<int>& rptr
   std::vector<Item> heap;
   for (int i = 0; i < B; ++i) heap.push_back({i, best[i], dS[i]});
   std::make_heap(heap.begin(), heap.end(), cmp);
-  block_map.resize(B);
-  std::iota(block_map.begin(), block_map.end(), 0);
+  GroupMap gm(B);
   int merged = 0;
   while (merged < to_merge && !heap.empty()) {
     std::pop_heap(heap.begin(), heap.end(), cmp);
     Item m = heap.back();
     heap.pop_back();
     if (m.to < 0) continue;
-    const int from = m.from, to = block_map[m.to];
+    const int from = m.from, to = gm.name[m.to];
     if (from == to) continue;
     const double actual = delta(std::min(from, to), std::max(from, to));
     if (!heap.empty() && actual > heap.front().dS) {
@@ -626,8 +650,7 @@ static void carry_out_advanced(int B, int to_merge, const std::vector<int>& rptr
       std::push_heap(heap.begin(), heap.end(), cmp);
       continue;
     }
-    for (int i = 0; i < B; ++i)
-      if (block_map[i] == from) block_map[i] = to;
+    gm.rename(from, to);
     // move row/col `from` into `to`
     std::vector<std::pair<int, int>> rf(rows[from].begin(), rows[from].end());
     std::vector<std::pair<int, int>> cf(cols[from].begin(), cols[from].end());
@@ -656,6 +679,7 @@ static void carry_out_advanced(int B, int to_merge, const std::vector<int>& rptr
     d_in[from] = 0;
     merged++;
   }
+  block_map = gm.name;
 }
 
 static void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& opt, const SbpReplay* replay,
@@ -726,19 +750,19 @@ static void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& 
     std::vector<int> order(B);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b2) { return dS[a] < dS[b2]; });
-    std::iota(block_map.begin(), block_map.end(), 0);
+    GroupMap gm(B);
     int merged = 0, counter = 0;
     while (merged < to_merge) {
       if (counter >= B) throw Error(SBP_ERR_DEVICE, "not enough mergeable blocks for num_blocks_to_merge");
       const int from = order[counter++];
       if (best[from] < 0) continue;
-      const int to = block_map[best[from]];
+      const int to = gm.name[best[from]];
       if (to != from) {
-        for (int i = 0; i < B; ++i)
-          if (block_map[i] == from) block_map[i] = to;
+        gm.rename(from, to);
         merged++;
       }
     }
+    block_map = gm.name;
   } else {
     std::vector<int> rptr(B + 1), ridx(nnz[0]), rval(nnz[0]), dout(B), din(B);
     SBP_CUDA(SBP_COPY_ASYNC(rptr.data(), ms.rptr.p, (B + 1) * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
@@ -1039,6 +1063,8 @@ SbpStatus sbp_graph_create(int32_t V, int64_t n, const int32_t* src, const int32
     g->h_k[v] = (op[v + 1] - op[v]) + (ip[v + 1] - ip[v]);
     g->max_k = std::max(g->max_k, g->h_k[v]);
   }
+  // one table size for every vertex when it stays small; larger degrees go to the 1-warp path
+  g->light_cap = std::min(kLightCapMax, std::max(kLightCap, pow2_at_least(2 * g->max_k)));
   g->heavy_cap = std::max(512, pow2_at_least(2 * g->max_k));
   if (g->heavy_cap > kMaxCap) {
     if (V <= kMaxCap) g->heavy_cap = kMaxCap;   // distinct neighbour blocks <= B <= V
@@ -1055,6 +1081,7 @@ SbpStatus sbp_graph_create(int32_t V, int64_t n, const int32_t* src, const int32
   g->out_ptr.reserve(V + 1);
   g->in_ptr.reserve(V + 1);
   g->out_idx.reserve(m);
+  g->out_src.reserve(m);
   g->in_idx.reserve(m);
   g->self.reserve(V);
   g->identity.reserve(V);
@@ -1062,6 +1089,10 @@ SbpStatus sbp_graph_create(int32_t V, int64_t n, const int32_t* src, const int32
   SBP_CUDA(SBP_COPY(g->out_ptr.p, op.data(), (V + 1) * sizeof(int), cudaMemcpyHostToDevice));
   SBP_CUDA(SBP_COPY(g->in_ptr.p, ip.data(), (V + 1) * sizeof(int), cudaMemcpyHostToDevice));
   if (m) {
+    std::vector<int> osrc(m);
+    for (int v = 0; v < V; ++v)
+      for (int e = op[v]; e < op[v + 1]; ++e) osrc[e] = v;
+    SBP_CUDA(SBP_COPY(g->out_src.p, osrc.data(), m * sizeof(int), cudaMemcpyHostToDevice));
     SBP_CUDA(SBP_COPY(g->out_idx.p, oi.data(), m * sizeof(int), cudaMemcpyHostToDevice));
     if (ip[V]) SBP_CUDA(SBP_COPY(g->in_idx.p, ii.data(), ip[V] * sizeof(int), cudaMemcpyHostToDevice));
   }

@@ -97,29 +97,32 @@ __global__ void k_mdl_cells(BlockView bm, double* partial) {
   if (threadIdx.x == 0) partial[blockIdx.x] = t;
 }
 
-// Edge form: sum_cells M log M = sum over edges of log M[b_src, b_dst].
-__global__ void k_mdl_edges(GraphView g, BlockView bm, double* partial) {
+// Edge form: sum_cells M log M = sum over edges of log M[b_src, b_dst]; one thread per edge.
+__global__ void k_mdl_edges(GraphView g, BlockView bm, const int* __restrict__ out_src, double* partial) {
   __shared__ double red[32];
   double acc = 0.0;
-  const int stride = gridDim.x * blockDim.x;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < g.V; v += stride) {
-    const int bv = bm.b[v];
-    const int* row = bm.M + (size_t)bv * bm.ld;
-    for (int e = g.out_ptr[v]; e < g.out_ptr[v + 1]; ++e) acc += log((double)row[bm.b[__ldg(g.out_idx + e)]]);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < g.E; e += stride) {
+    const int bv = bm.b[__ldg(out_src + e)], bu = bm.b[__ldg(g.out_idx + e)];
+    acc += log((double)bm.M[(size_t)bv * bm.ld + bu]);
   }
-  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < bm.B; x += stride)
+  for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < bm.B; x += stride)
     acc -= xlogx((double)bm.d_out[x]) + xlogx((double)bm.d_in[x]);
   const double t = block_sum(acc, red);
   if (threadIdx.x == 0) partial[blockIdx.x] = t;
 }
 
+// Sum of the partials in a fixed order (one CTA of 256 threads) and the MDL formula.
 __global__ void k_mdl_final(const double* partial, int n, int V, long long E, int B, double* out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double L = 0.0;
-  for (int i = 0; i < n; ++i) L += partial[i];
-  const double x = pow((double)B, 2) / (double)E;
-  const double h = ((1 + x) * log(1 + x)) - (x * log(x));
-  *out = ((double)E * h) + ((double)V * log((double)B)) - L;
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+  const double L = block_sum(acc, red);
+  if (threadIdx.x == 0) {
+    const double x = pow((double)B, 2) / (double)E;
+    const double h = ((1 + x) * log(1 + x)) - (x * log(x));
+    *out = ((double)E * h) + ((double)V * log((double)B)) - L;
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -152,7 +155,7 @@ __device__ __forceinline__ void init_table(const WarpTable& t, int lane) {
 // Asynchronous Gibbs: evaluate a list of vertices against the frozen state.  Accepted moves
 // go to prop[v] and the moved list; counters: [0] visits [1] proposals_moved [2] accepted.
 // ------------------------------------------------------------------------------------------
-__global__ void k_gibbs_eval(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng,
+__global__ void __launch_bounds__(256, 2) k_gibbs_eval(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng,
                              int sweep, int* prop, int* moved_list, int* n_moved, unsigned long long* counters,
                              int cap, int* status) {
   extern __shared__ int smem[];
@@ -205,8 +208,12 @@ __device__ __forceinline__ void cell_add_owned(const BlockView& bm, int row, int
 // its old cell to its new cell; the result equals the reference's one-by-one application.
 // qr/qs keep the reference's diagonal delta of each move as seen at its turn in vertex order,
 // which Blockmodel::move_vertex folds into d[r], d[s] (blockmodel.cpp:348-359).
+// Every edge incident to a moved vertex moves once from its old cell to its new cell; the
+// result equals the reference's one-by-one application.  qr/qs keep the reference's diagonal
+// delta of each move as seen at its turn in vertex order, which Blockmodel::move_vertex folds
+// into d[r], d[s] (blockmodel.cpp:348-359); last[x] keeps (batch generation, last mover of x).
 __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, const int* n_moved, const int* prop,
-                              int* qr, int* qs, int* last) {
+                              int* qr, int* qs, unsigned long long* last, unsigned gen) {
   const int lane = threadIdx.x & 31;
   const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -254,30 +261,26 @@ __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, 
       atomicAdd(bm.d_in + s, k_in_self);
       qr[v] = -(cr + self);
       qs[v] = cs + self;
-      atomicMax(last + r, v);
-      atomicMax(last + s, v);
+      const unsigned long long key = ((unsigned long long)gen << 32) | (unsigned)v;
+      atomicMax(last + r, key);
+      atomicMax(last + s, key);
     }
   }
 }
 
-__global__ void k_apply_degrees(BlockView bm, const int* moved_list, const int* n_moved, const int* prop,
-                                const int* qr, const int* qs, const int* last) {
+// d[r], d[s] from the last mover of each block, then the new assignment; clears the other
+// moved-count slot for the next batch.
+__global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved, int* prop,
+                               const int* qr, const int* qs, const unsigned long long* last, unsigned gen) {
   const int n = *n_moved;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *next_n_moved = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int v = moved_list[i];
     const int r = bm.b[v], s = prop[v];
-    if (last[r] == v) bm.d[r] = bm.d_out[r] + bm.d_in[r] - bm.M[(size_t)r * bm.ld + r] - qr[v];
-    if (last[s] == v) bm.d[s] = bm.d_out[s] + bm.d_in[s] - bm.M[(size_t)s * bm.ld + s] - qs[v];
-  }
-}
-
-__global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n_moved, int* prop, int* last) {
-  const int n = *n_moved;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int v = moved_list[i];
-    last[bm.b[v]] = -1;
-    last[prop[v]] = -1;
-    bm.b[v] = prop[v];
+    const unsigned long long key = ((unsigned long long)gen << 32) | (unsigned)v;
+    if (last[r] == key) bm.d[r] = bm.d_out[r] + bm.d_in[r] - bm.M[(size_t)r * bm.ld + r] - qr[v];
+    if (last[s] == key) bm.d[s] = bm.d_out[s] + bm.d_in[s] - bm.M[(size_t)s * bm.ld + s] - qs[v];
+    bm.b[v] = s;
     prop[v] = -1;
   }
 }

@@ -17,16 +17,15 @@ __global__ void k_rebuild_global(GraphView g, BlockView bm);
 __global__ void k_rebuild_smem(GraphView g, BlockView bm);
 __global__ void k_rebuild_degrees(BlockView bm);
 __global__ void k_mdl_cells(BlockView bm, double* partial);
-__global__ void k_mdl_edges(GraphView g, BlockView bm, double* partial);
+__global__ void k_mdl_edges(GraphView g, BlockView bm, const int* __restrict__ out_src, double* partial);
 __global__ void k_mdl_final(const double* partial, int n, int V, long long E, int B, double* out);
-__global__ void k_gibbs_eval(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng,
+__global__ void __launch_bounds__(256, 2) k_gibbs_eval(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng,
                              int sweep, int* prop, int* moved_list, int* n_moved, unsigned long long* counters,
                              int cap, int* status);
 __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, const int* n_moved, const int* prop,
-                              int* qr, int* qs, int* last);
-__global__ void k_apply_degrees(BlockView bm, const int* moved_list, const int* n_moved, const int* prop,
-                                const int* qr, const int* qs, const int* last);
-__global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n_moved, int* prop, int* last);
+                              int* qr, int* qs, unsigned long long* last, unsigned gen);
+__global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved, int* prop,
+                               const int* qr, const int* qs, const unsigned long long* last, unsigned gen);
 __global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
                      int cap, double* out, int* status);
 __global__ void k_move_vertex(GraphView g, BlockView bm, int v, int s, int cap, int* status);
