@@ -29,7 +29,7 @@ EXPORTED = [
     "sbp_graph_get_split", "sbp_graph_set_split", "sbp_blockmodel_create", "sbp_blockmodel_copy",
     "sbp_blockmodel_destroy", "sbp_blockmodel_num_blocks", "sbp_blockmodel_set_num_blocks_to_merge",
     "sbp_blockmodel_overall_entropy", "sbp_get_assignment", "sbp_get_block_matrix", "sbp_get_degrees", "sbp_mdl",
-    "sbp_evaluate_vertices", "sbp_move_vertex", "sbp_finetune", "sbp_merge_blocks", "sbp_partition",
+    "sbp_evaluate_vertices", "sbp_move_vertex", "sbp_finetune", "sbp_merge_blocks", "sbp_partition", "sbp_mdl_device_noalloc",
 ]
 
 
@@ -119,6 +119,8 @@ def load(path=LIB_PATH):
     L.sbp_merge_blocks.argtypes = [vp, vp, ctypes.POINTER(MergeOptions), ctypes.POINTER(Replay), _i32p, _f64p,
                                    ctypes.POINTER(Stats)]
     L.sbp_partition.argtypes = [vp, ctypes.POINTER(Options), _i32p, ctypes.POINTER(Stats)]
+    L.sbp_mdl_device_noalloc.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, vp, vp, ctypes.c_int32, ctypes.c_int64,
+                                         vp, vp]
     _lib = L
     return L
 
@@ -327,6 +329,18 @@ class block_merge:
                                      _p(dS, _f64p), ctypes.byref(st)))
         del keep
         return dict(best=best, dS=dS, **st.as_dict())
+
+
+def mdl_device_noalloc(d_matrix, num_blocks, ld, d_degrees_out, d_degrees_in, num_vertices, num_edges, d_result,
+                       stream=None):
+    """MDL of device-resident counts without any GPU allocation (sbp_mdl_device_noalloc).
+    Pointer arguments are raw device addresses (ints); the result is written to d_result on
+    `stream` (a cudaStream_t as int, or None for the legacy default stream)."""
+    rc = load().sbp_mdl_device_noalloc(d_matrix, int(num_blocks), int(ld), d_degrees_out, d_degrees_in,
+                                       int(num_vertices), int(num_edges), d_result, stream)
+    if rc != 0:
+        raise SbpError(rc, "sbp_mdl_device_noalloc rejected the call (limit: 32768 blocks)"
+                       if rc == 3 else "sbp_mdl_device_noalloc failed")
 
 
 class sbp:

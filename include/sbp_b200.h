@@ -178,6 +178,24 @@ SbpStatus sbp_merge_blocks(SbpBlockmodel *bm, const SbpGraph *graph, const SbpMe
  * merge + finetune rounds.  out_assignment: V ints. */
 SbpStatus sbp_partition(const SbpGraph *graph, const SbpOptions *opt, int32_t *out_assignment, SbpStats *stats);
 
+/* MDL (entropy::mdl semantics, FP64 log terms) of block counts that are already on the device,
+ * for callers that cannot allocate GPU memory: code running under a device-memory budget fixed
+ * at start-up, or code that must not call cudaMalloc/cudaFree because those synchronize the
+ * whole device while it has work in flight.  No counterpart in the reference (a CPU-only code
+ * base).  It allocates nothing: the caller passes the inputs and the output, and the only
+ * scratch is a static device array of one double per block row, held by every GPU that loads
+ * this library until the process exits.
+ *   d_matrix: num_blocks rows of counts, row stride `ld` ints (ld >= num_blocks), on the device;
+ *   d_degrees_out / d_degrees_in: num_blocks ints each, on the device;
+ *   d_result: one double on the device; `stream`: a cudaStream_t (NULL = legacy default stream).
+ * Limit: num_blocks <= 32768 (SBP_ERR_UNSUPPORTED above it).  The work is queued on `stream`;
+ * the result is ready when the stream reaches it.  Calls share the scratch array, so calls
+ * that overlap on the GPU race and must be serialised.  The first call on a device looks up
+ * the scratch array's address on that device; make it before any stream capture. */
+SbpStatus sbp_mdl_device_noalloc(const int32_t *d_matrix, int32_t num_blocks, int64_t ld, const int32_t *d_degrees_out,
+                                 const int32_t *d_degrees_in, int32_t num_vertices, int64_t num_edges,
+                                 double *d_result, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
