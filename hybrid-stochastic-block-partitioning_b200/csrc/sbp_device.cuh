@@ -124,6 +124,17 @@ constexpr int kChunk = 128;   // columns per chunk-sum entry
 
 struct BlockView {
   int B;
+  int sparse;             // 0: dense M/MT below; 1: row-hashed regions (large B)
+  // row-hashed storage: row r of M lives in rslot[rbase[r] .. rbase[r] + rmask[r]], slots
+  // (col, count), col = -1 for an empty slot; MT likewise in cslot.  Keys are never removed
+  // (a count can drop to 0).  An insertion that finds its row full sets *overflow.
+  const long long* rbase;
+  const int* rmask;
+  int2* rslot;
+  const long long* cbase;
+  const int* cmask;
+  int2* cslot;
+  int* overflow;
   int ld;                 // row stride of M and MT (multiple of kChunk ints)
   int nch;                // chunks per row = ceil(B / kChunk)
   int* CS;                // [B*nch] CS[row*nch+c] = sum of M[row, c*kChunk .. c*kChunk+kChunk)
@@ -153,6 +164,80 @@ __device__ __forceinline__ int warp_select_dense(const int* row, int n, long lon
     target -= tot;
   }
   return -1;
+}
+
+// ---- row-hashed storage ------------------------------------------------------------------
+__device__ __forceinline__ unsigned slot_hash(int key) { return (unsigned)key * 2654435761u; }
+
+__device__ __forceinline__ int hashed_get(const long long* base, const int* mask, const int2* slot, int row, int col) {
+  const long long b0 = base[row];
+  const int m = mask[row];
+  unsigned h = slot_hash(col) & (unsigned)m;
+  for (int probe = 0; probe <= m; ++probe) {
+    const int2 e = slot[b0 + h];
+    if (e.x == col) return e.y;
+    if (e.x == -1) return 0;
+    h = (h + 1) & (unsigned)m;
+  }
+  return 0;
+}
+
+__device__ __forceinline__ void hashed_add(const long long* base, const int* mask, int2* slot, int row, int col,
+                                           int delta, int* overflow) {
+  const long long b0 = base[row];
+  const int m = mask[row];
+  unsigned h = slot_hash(col) & (unsigned)m;
+  for (int probe = 0; probe <= m; ++probe) {
+    int* key = &slot[b0 + h].x;
+    int k = *(volatile int*)key;
+    if (k == -1) {
+      const int prev = atomicCAS(key, -1, col);
+      k = prev == -1 ? col : prev;
+    }
+    if (k == col) {
+      atomicAdd(&slot[b0 + h].y, delta);
+      return;
+    }
+    h = (h + 1) & (unsigned)m;
+  }
+  atomicOr(overflow, 1);
+}
+
+// M[row, col] and MT[row, col] = M[col, row] in either representation.
+__device__ __forceinline__ int bm_get(const BlockView& bm, int row, int col) {
+  return bm.sparse ? hashed_get(bm.rbase, bm.rmask, bm.rslot, row, col) : bm.M[(size_t)row * bm.ld + col];
+}
+__device__ __forceinline__ int bm_getT(const BlockView& bm, int row, int col) {
+  return bm.sparse ? hashed_get(bm.cbase, bm.cmask, bm.cslot, row, col) : bm.MT[(size_t)row * bm.ld + col];
+}
+
+// Walk of a hashed row in ascending column order: bisection over the column space for the
+// first column whose running count exceeds `target`.  Same result as the dense walks.
+__device__ __forceinline__ int warp_select_hashed(const long long* base, const int* mask, const int2* slot, int row,
+                                                  int B, long long target, int lane) {
+  const long long b0 = base[row];
+  const int cap = mask[row] + 1;
+  int lo = 0, hi = B - 1;
+  while (lo < hi) {
+    const int mid = lo + ((hi - lo) >> 1);
+    long long cnt = 0;
+    for (int i = lane; i < cap; i += kWarp) {
+      const int2 e = slot[b0 + i];
+      if (e.x >= 0 && e.x <= mid) cnt += e.y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFull, cnt, o);
+    if (cnt > target) hi = mid;
+    else lo = mid + 1;
+  }
+  long long cnt = 0;
+  for (int i = lane; i < cap; i += kWarp) {
+    const int2 e = slot[b0 + i];
+    if (e.x >= 0 && e.x <= lo) cnt += e.y;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFull, cnt, o);
+  return cnt > target ? lo : -1;
 }
 
 // Two-level walk: find the chunk through the chunk sums, then the column inside the chunk
@@ -395,11 +480,15 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
     const int dot = bm.d_out[tblk];
     const long long total = (long long)dot + (long long)bm.d_in[tblk];
     const long long target = scale32(x.y, total);
-    if (target < dot)
+    if (bm.sparse) {
+      if (target < dot) s = warp_select_hashed(bm.rbase, bm.rmask, bm.rslot, tblk, bm.B, target, lane);
+      else s = warp_select_hashed(bm.cbase, bm.cmask, bm.cslot, tblk, bm.B, target - dot, lane);
+    } else if (target < dot) {
       s = warp_select_chunked(bm.M + (size_t)tblk * bm.ld, bm.CS + (size_t)tblk * bm.nch, bm.nch, target, lane);
-    else
+    } else {
       s = warp_select_chunked(bm.MT + (size_t)tblk * bm.ld, bm.CST + (size_t)tblk * bm.nch, bm.nch, target - dot,
                               lane);
+    }
     if (s < 0) {
       if (lane == 0) atomicOr(status, kErrScan);
       s = r;
@@ -415,23 +504,20 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
   const int d_rs = -mc.co_s + mc.ci_r;
   const int d_sr = mc.co_r - mc.ci_s;
   const int d_ss = mc.co_s + mc.ci_s + self;
-  const int M_rr = bm.M[(size_t)r * ld + r], M_rs = bm.M[(size_t)r * ld + s];
-  const int M_sr = bm.M[(size_t)s * ld + r], M_ss = bm.M[(size_t)s * ld + s];
+  const int M_rr = bm_get(bm, r, r), M_rs = bm_get(bm, r, s);
+  const int M_sr = bm_get(bm, s, r), M_ss = bm_get(bm, s, s);
   const int dout_r = bm.d_out[r], dout_s = bm.d_out[s], din_r = bm.d_in[r], din_s = bm.d_in[s];
   const int kin_self = k_in + self;
+  (void)ld;
 
   double fwd = 0.0, bwd = 0.0, dS = 0.0;
   long long T = 0;   // integer scale of the changed cells and degrees (zero snap below)
   const int n = *t.nlist;
-  const int* Mr = bm.M + (size_t)r * ld;
-  const int* Ms = bm.M + (size_t)s * ld;
-  const int* MTr = bm.MT + (size_t)r * ld;
-  const int* MTs = bm.MT + (size_t)s * ld;
   for (int i = lane; i < n; i += kWarp) {
     const int h = t.list[i];
     const int u = t.keys[h];
     const int co = t.cout[h], ci = t.cin[h];
-    const int M_su = Ms[u], M_us = MTs[u], M_ru = Mr[u], M_ur = MTr[u];
+    const int M_su = bm_get(bm, s, u), M_us = bm_getT(bm, s, u), M_ru = bm_get(bm, r, u), M_ur = bm_getT(bm, r, u);
     const int du = bm.d[u];
     const bool is_r = (u == r), is_s = (u == s), corner = is_r || is_s;
     const double c = (double)(co + ci + (is_r ? self : 0));

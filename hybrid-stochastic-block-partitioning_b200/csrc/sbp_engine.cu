@@ -17,6 +17,7 @@
 
 #include "../../include/sbp_b200.h"
 #include "sbp_kernels.cuh"
+#include "sbp_sort.cuh"
 
 namespace sbpb {
 
@@ -106,12 +107,12 @@ struct Context {
       SBP_CUDA(cudaGetDevice(&dev));
       SBP_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
       c->npartial = 4 * c->num_sms;
-      SBP_CUDA(cudaMalloc(&c->status, sizeof(int)));
+      SBP_CUDA(cudaMalloc(&c->status, 8 * sizeof(int)));
       SBP_CUDA(cudaMalloc(&c->counters, 8 * sizeof(unsigned long long)));
       SBP_CUDA(cudaMalloc(&c->partial, c->npartial * sizeof(double)));
       SBP_CUDA(cudaMalloc(&c->scalar, sizeof(double)));
-      SBP_CUDA(cudaMalloc(&c->mh_out, 4 * sizeof(double)));
-      SBP_CUDA(cudaMemset(c->status, 0, sizeof(int)));
+      SBP_CUDA(cudaMalloc(&c->mh_out, 16 * sizeof(double)));
+      SBP_CUDA(cudaMemset(c->status, 0, 8 * sizeof(int)));
       SBP_CUDA(cudaEventCreate(&c->ev0));
       SBP_CUDA(cudaEventCreate(&c->ev1));
       ctx = c;
@@ -185,6 +186,10 @@ constexpr int kLightWarps = 8;
 constexpr int kMaxCap = 8192;         // largest per-warp table
 constexpr size_t kSmemBudget = 200 * 1024;
 constexpr int kSmemRebuildMaxB = 100;
+
+// Blocks above which the block matrix is row-hashed instead of dense (sbp_set_option).
+static int g_dense_max_blocks = 16384;
+static long long g_overflow_rebuilds = 0;   // rebuilds forced by a full hashed row
 
 }  // namespace sbpb
 
@@ -279,17 +284,32 @@ struct SbpGraph {
 // ------------------------------------------------------------------------------------------
 struct SbpBlockmodel {
   int V = 0, B = 0, ld = 0;
+  const SbpGraph* graph = nullptr;   // the graph the blockmodel was created on (must outlive it)
   DevBuf<int> b, M, MT, CS, CST, d_out, d_in, d;
   DevBuf<int> prop, qr, qs, moved, n_moved;   // n_moved: two slots, alternating per batch
   DevBuf<unsigned long long> last;           // (batch generation << 32 | last mover) per block
   unsigned gen = 0;                          // batch generation
   int nch = 0;
+  // row-hashed representation (B > dense_max_blocks)
+  bool sparse = false;
+  DevBuf<long long> rbase, cbase;
+  DevBuf<int> rmask, cmask, overflow, old_block;
+  DevBuf<int2> rslot, cslot;
+  DevBuf<int> csr_rptr, csr_ridx, csr_rval, csr_cptr, csr_cidx, csr_cval;   // sorted rows after a rebuild
   float overall_entropy = 3.40282347e+38f;
   int num_blocks_to_merge = 0;
 
   BlockView view() {
     BlockView v;
     v.B = B;
+    v.sparse = sparse ? 1 : 0;
+    v.rbase = rbase.p;
+    v.rmask = rmask.p;
+    v.rslot = rslot.p;
+    v.cbase = cbase.p;
+    v.cmask = cmask.p;
+    v.cslot = cslot.p;
+    v.overflow = overflow.p;
     v.ld = ld;
     v.nch = nch;
     v.CS = CS.p;
@@ -311,7 +331,10 @@ struct SbpBlockmodel {
     qr.reserve(V);
     qs.reserve(V);
     moved.reserve(V);
+    old_block.reserve(V);
     n_moved.reserve(2);
+    overflow.reserve(1);
+    SBP_CUDA(cudaMemsetAsync(overflow.p, 0, sizeof(int), c.stream));
     SBP_CUDA(cudaMemsetAsync(prop.p, 0xff, sizeof(int) * V, c.stream));
     SBP_CUDA(cudaMemsetAsync(n_moved.p, 0, 2 * sizeof(int), c.stream));
   }
@@ -319,13 +342,21 @@ struct SbpBlockmodel {
   void set_blocks(int nb) {
     Context& c = Context::get();
     B = nb;
+    sparse = B > g_dense_max_blocks;
     ld = ((B + kChunk - 1) / kChunk) * kChunk;
     nch = (B + kChunk - 1) / kChunk;
-    const size_t cells = (size_t)B * (size_t)ld;
-    M.reserve(cells);
-    MT.reserve(cells);
-    CS.reserve((size_t)B * nch);
-    CST.reserve((size_t)B * nch);
+    if (sparse) {
+      rbase.reserve(B);
+      cbase.reserve(B);
+      rmask.reserve(B);
+      cmask.reserve(B);
+    } else {
+      const size_t cells = (size_t)B * (size_t)ld;
+      M.reserve(cells);
+      MT.reserve(cells);
+      CS.reserve((size_t)B * nch);
+      CST.reserve((size_t)B * nch);
+    }
     d_out.reserve(B);
     d_in.reserve(B);
     d.reserve(B);
@@ -336,8 +367,106 @@ struct SbpBlockmodel {
 
 namespace sbpb {
 
-// Blockmodel::initialize_edge_counts (src/blockmodel/blockmodel.cpp:187-255).
-static void rebuild(SbpBlockmodel& bm, const SbpGraph& g) {
+// Scratch of the sparse rebuild (grow-only, shared by all blockmodels).
+struct SortScratch {
+  DevBuf<unsigned long long> keys, keysT, tmp, ukeys, partial;
+  DevBuf<unsigned> hist, flags, rowcnt, caps;
+  DevBuf<long long> pos, heads, rowptr;
+};
+static SortScratch g_sort;
+
+static int key_bits(int B) {
+  const unsigned long long maxkey = (unsigned long long)B * (unsigned long long)B;
+  int bits = 1;
+  while (bits < 64 && (1ull << bits) < maxkey) ++bits;
+  return bits;
+}
+
+// One orientation of the sparse rebuild: sort keys, unique them, size the rows, fill them.
+static void rebuild_hashed_side(SbpBlockmodel& bm, long long E, unsigned long long* keys, DevBuf<long long>& base,
+                                DevBuf<int>& mask, DevBuf<int2>& slot, DevBuf<int>& cptr, DevBuf<int>& cidx,
+                                DevBuf<int>& cval) {
+  Context& c = Context::get();
+  const int B = bm.B;
+  long long nu = 0;
+  unsigned long long* sorted = keys;
+  if (E > 0) {
+    radix_sort_u64(keys, g_sort.tmp.p, E, key_bits(B), g_sort.hist.p, g_sort.partial.p, c.num_sms, c.stream, &sorted);
+    rle(sorted, E, g_sort.flags.p, g_sort.pos.p, g_sort.ukeys.p, g_sort.heads.p, g_sort.partial.p, c.num_sms, c.stream);
+    long long lastpos = 0;
+    unsigned lastflag = 0;
+    SBP_CUDA(SBP_COPY_ASYNC(&lastpos, g_sort.pos.p + E - 1, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    SBP_CUDA(SBP_COPY_ASYNC(&lastflag, g_sort.flags.p + E - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream));
+    SBP_CHECK_LAUNCH();
+    c.sync();
+    nu = lastpos + lastflag;
+  }
+  SBP_CUDA(cudaMemsetAsync(g_sort.rowcnt.p, 0, B * sizeof(unsigned), c.stream));
+  if (nu > 0) {
+    k_unique_rows<<<grid_for(nu, 256, 8 * c.num_sms), 256, 0, c.stream>>>(g_sort.ukeys.p, nu, B, g_sort.rowcnt.p);
+    SBP_CHECK_LAUNCH();
+  }
+  exclusive_scan_u32(g_sort.rowcnt.p, g_sort.rowptr.p, B, g_sort.partial.p, c.num_sms, c.stream);
+  k_row_caps<<<grid_for(B, 256, 8 * c.num_sms), 256, 0, c.stream>>>(g_sort.rowcnt.p, B, g_sort.caps.p, mask.p);
+  exclusive_scan_u32(g_sort.caps.p, base.p, B, g_sort.partial.p, c.num_sms, c.stream);
+  SBP_CHECK_LAUNCH();
+  long long lastbase = 0;
+  unsigned lastcap = 0;
+  SBP_CUDA(SBP_COPY_ASYNC(&lastbase, base.p + B - 1, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(&lastcap, g_sort.caps.p + B - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  const long long total = lastbase + lastcap;
+  slot.reserve(total);
+  cptr.reserve(B + 1);
+  cidx.reserve(std::max(nu, 1LL));
+  cval.reserve(std::max(nu, 1LL));
+  k_fill_empty<<<grid_for(total, 256, 16 * c.num_sms), 256, 0, c.stream>>>(slot.p, total);
+  k_fill_rows<<<grid_for(B, 128, 16 * c.num_sms), 128, 0, c.stream>>>(g_sort.rowptr.p, g_sort.ukeys.p, g_sort.heads.p,
+                                                                     nu, E, B, base.p, mask.p, slot.p, cptr.p,
+                                                                     cidx.p, cval.p);
+  SBP_CHECK_LAUNCH();
+}
+
+// Sparse Blockmodel::initialize_edge_counts: rows of M and MT from sorted (b_src, b_dst) keys.
+static void rebuild_sparse(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_d) {
+  Context& c = Context::get();
+  const long long E = g.E;
+  const int B = bm.B;
+  g_sort.keys.reserve(std::max(E, 1LL));
+  g_sort.keysT.reserve(std::max(E, 1LL));
+  g_sort.tmp.reserve(std::max(E, 1LL));
+  g_sort.ukeys.reserve(std::max(E, 1LL));
+  g_sort.flags.reserve(std::max(E, 1LL));
+  g_sort.pos.reserve(std::max(E, 1LL));
+  g_sort.heads.reserve(std::max(E, 1LL));
+  g_sort.hist.reserve(radix_hist_capacity(std::max(E, 1LL), c.num_sms));
+  g_sort.partial.reserve(scan_partial_capacity(c.num_sms));
+  g_sort.rowcnt.reserve(B);
+  g_sort.caps.reserve(B);
+  g_sort.rowptr.reserve(B);
+  SBP_CUDA(cudaMemsetAsync(bm.d_out.p, 0, B * sizeof(int), c.stream));
+  SBP_CUDA(cudaMemsetAsync(bm.d_in.p, 0, B * sizeof(int), c.stream));
+  SBP_CUDA(cudaMemsetAsync(bm.overflow.p, 0, sizeof(int), c.stream));
+  k_block_degrees<<<grid_for(g.V, 256, 8 * c.num_sms), 256, 0, c.stream>>>(g.view(), bm.b.p, bm.d_out.p, bm.d_in.p);
+  if (E > 0)
+    k_edge_keys<<<grid_for(E, 256, 16 * c.num_sms), 256, 0, c.stream>>>(g.view(), bm.b.p, g.out_src.p, B,
+                                                                       g_sort.keys.p, g_sort.keysT.p);
+  SBP_CHECK_LAUNCH();
+  rebuild_hashed_side(bm, E, g_sort.keys.p, bm.rbase, bm.rmask, bm.rslot, bm.csr_rptr, bm.csr_ridx, bm.csr_rval);
+  rebuild_hashed_side(bm, E, g_sort.keysT.p, bm.cbase, bm.cmask, bm.cslot, bm.csr_cptr, bm.csr_cidx, bm.csr_cval);
+  if (recompute_d) {
+    k_rebuild_degrees<<<grid_for(B, 256, 1 << 20), 256, 0, c.stream>>>(bm.view());
+    SBP_CHECK_LAUNCH();
+  }
+}
+
+// Blockmodel::initialize_edge_counts (src/blockmodel/blockmodel.cpp:187-255).  recompute_d =
+// false keeps d (the reference's drifting block degree) when only the storage is rebuilt.
+static void rebuild(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_d = true) {
+  if (bm.sparse) {
+    rebuild_sparse(bm, g, recompute_d);
+    return;
+  }
   Context& c = Context::get();
   const size_t cells = (size_t)bm.B * (size_t)bm.ld;
   SBP_CUDA(cudaMemsetAsync(bm.M.p, 0, cells * sizeof(int), c.stream));
@@ -363,7 +492,7 @@ static void rebuild(SbpBlockmodel& bm, const SbpGraph& g) {
 static double mdl(SbpBlockmodel& bm, const SbpGraph& g) {
   Context& c = Context::get();
   const int grid = c.npartial;
-  if ((long long)bm.B * bm.B <= 4LL * g.E) k_mdl_cells<<<grid, 256, 0, c.stream>>>(bm.view(), c.partial);
+  if (!bm.sparse && (long long)bm.B * bm.B <= 4LL * g.E) k_mdl_cells<<<grid, 256, 0, c.stream>>>(bm.view(), c.partial);
   else k_mdl_edges<<<grid, 256, 0, c.stream>>>(g.view(), bm.view(), g.out_src.p, c.partial);
   SBP_CHECK_LAUNCH();
   k_mdl_final<<<1, 256, 0, c.stream>>>(c.partial, grid, g.V, g.E, bm.B, c.scalar);
@@ -412,15 +541,26 @@ static MhResult mh_pass(SbpBlockmodel& bm, const SbpGraph& g, const int* verts, 
   if (W < 1) throw Error(SBP_ERR_UNSUPPORTED, "vertex degree too large for the Metropolis-Hastings kernel");
   const size_t smem = per_warp * W;
   set_smem_limit((const void*)k_mh, smem);
-  k_mh<<<1, W * 32, smem, c.stream>>>(g.view(), bm.view(), verts, n, rng, sweep, cap, c.mh_out, c.status);
-  SBP_CHECK_LAUNCH();
-  double out[4];
-  SBP_CUDA(SBP_COPY_ASYNC(out, c.mh_out, sizeof(out), cudaMemcpyDeviceToHost, c.stream));
-  c.sync();
-  res.visits = (long long)out[0];
-  res.moved = (long long)out[1];
-  res.accepted = (long long)out[2];
-  res.sum_dS = out[3];
+  int start = 0;
+  while (start < n) {
+    k_mh<<<1, W * 32, smem, c.stream>>>(g.view(), bm.view(), verts, n, start, rng, sweep, cap, c.mh_out, c.status);
+    SBP_CHECK_LAUNCH();
+    double out[10];
+    SBP_CUDA(SBP_COPY_ASYNC(out, c.mh_out, sizeof(out), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    res.visits += (long long)out[0];
+    res.moved += (long long)out[1];
+    res.accepted += (long long)out[2];
+    res.sum_dS += out[3];
+    if (out[4] == 0.0) break;
+    // a hashed row ran out of room at list position out[5]: rebuild the rows with more room
+    // (keeping d), finish that move's d[r], d[s] and resume after it
+    rebuild(bm, g, false);
+    ++g_overflow_rebuilds;
+    k_fix_move_degrees<<<1, 1, 0, c.stream>>>(bm.view(), (int)out[6], (int)out[7], (int)out[8], (int)out[9]);
+    SBP_CHECK_LAUNCH();
+    start = (int)out[5] + 1;
+  }
   return res;
 }
 
@@ -468,6 +608,24 @@ static void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& p
   k_apply_edges<<<gw, 256, 0, c.stream>>>(g.view(), bm.view(), bm.moved.p, n_cur, bm.prop.p, bm.qr.p, bm.qs.p,
                                           bm.last.p, gen);
   SBP_CHECK_LAUNCH();
+  if (bm.sparse) {
+    int ovf = 0;
+    SBP_CUDA(SBP_COPY_ASYNC(&ovf, bm.overflow.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    if (ovf) {
+      // a hashed row ran out of room: move the assignment, rebuild the rows with more room
+      // (keeping d) and run the degree step on the rebuilt rows
+      k_recover_assign<<<grid_for(batch, 256, 64 * c.num_sms), 256, 0, c.stream>>>(bm.b.p, bm.moved.p, n_cur,
+                                                                                    bm.prop.p, bm.old_block.p);
+      SBP_CHECK_LAUNCH();
+      rebuild(bm, g, false);
+      ++g_overflow_rebuilds;
+      k_recover_finish<<<grid_for(batch, 256, 64 * c.num_sms), 256, 0, c.stream>>>(
+          bm.view(), bm.moved.p, n_cur, n_next, bm.prop.p, bm.old_block.p, bm.qr.p, bm.qs.p, bm.last.p, gen);
+      SBP_CHECK_LAUNCH();
+      return;
+    }
+  }
   k_apply_finish<<<grid_for(batch, 256, 64 * c.num_sms), 256, 0, c.stream>>>(
       bm.view(), bm.moved.p, n_cur, n_next, bm.prop.p, bm.qr.p, bm.qs.p, bm.last.p, gen);
   SBP_CHECK_LAUNCH();
@@ -507,6 +665,7 @@ static void finetune(SbpBlockmodel& bm, SbpGraph& g, int algo, const SbpFinetune
   const int max_sweeps = (opt.max_sweeps <= 0 || opt.max_sweeps > kMaxIterations) ? kMaxIterations : opt.max_sweeps;
   const bool bracket = opt.bracket_established != 0;
   SBP_CUDA(cudaMemsetAsync(c.counters, 0, 8 * sizeof(unsigned long long), c.stream));
+  const long long ovf0 = g_overflow_rebuilds;
   bm.overall_entropy = (float)mdl(bm, g);
   const double initial_entropy = bm.overall_entropy;
   std::vector<double> deltas;
@@ -552,6 +711,7 @@ static void finetune(SbpBlockmodel& bm, SbpGraph& g, int algo, const SbpFinetune
   st.mdl = bm.overall_entropy;
   st.mcmc_seconds = ms * 1e-3;
   st.num_blocks = bm.B;
+  st.overflow_rebuilds = (int)(g_overflow_rebuilds - ovf0);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -691,6 +851,14 @@ static void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& 
   MergeScratch ms;
   ReplayDev rp;
   rp.upload(replay);
+  int nnz[2] = {0, 0};
+  Csr rows, cols;
+  if (bm.sparse) {
+    // the sorted rows come with a rebuild (which also folds in any finetune updates)
+    rebuild(bm, g, true);
+    rows = Csr{bm.csr_rptr.p, bm.csr_ridx.p, bm.csr_rval.p};
+    cols = Csr{bm.csr_cptr.p, bm.csr_cidx.p, bm.csr_cval.p};
+  } else {
   // compressed rows of M and of MT (outgoing_edges / incoming_edges views)
   ms.rcnt.reserve(B);
   ms.ccnt.reserve(B);
@@ -702,7 +870,6 @@ static void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& 
   k_excl_scan<<<1, 1024, 0, c.stream>>>(ms.rcnt.p, ms.rptr.p, B);
   k_excl_scan<<<1, 1024, 0, c.stream>>>(ms.ccnt.p, ms.cptr.p, B);
   SBP_CHECK_LAUNCH();
-  int nnz[2];
   SBP_CUDA(SBP_COPY_ASYNC(&nnz[0], ms.rptr.p + B, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
   SBP_CUDA(SBP_COPY_ASYNC(&nnz[1], ms.cptr.p + B, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
   c.sync();
@@ -713,6 +880,10 @@ static void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& 
   k_row_fill<<<gw, 256, 0, c.stream>>>(bm.M.p, B, bm.ld, ms.rptr.p, ms.ridx.p, ms.rval.p);
   k_row_fill<<<gw, 256, 0, c.stream>>>(bm.MT.p, B, bm.ld, ms.cptr.p, ms.cidx.p, ms.cval.p);
   SBP_CHECK_LAUNCH();
+  rows = Csr{ms.rptr.p, ms.ridx.p, ms.rval.p};
+  cols = Csr{ms.cptr.p, ms.cidx.p, ms.cval.p};
+  }
+  const int gw = grid_for((long long)B * 32, 256, 64 * c.num_sms);
   RngParams rng;
   rng.seed = opt.seed;
   rng.replay = rp.records ? rp.buf.p : nullptr;
@@ -721,7 +892,6 @@ static void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& 
   ms.best_s.reserve(B);
   ms.best_dS.reserve(B);
   SBP_CUDA(cudaMemsetAsync(c.counters, 0, 8 * sizeof(unsigned long long), c.stream));
-  Csr rows{ms.rptr.p, ms.ridx.p, ms.rval.p}, cols{ms.cptr.p, ms.cidx.p, ms.cval.p};
   k_merge_propose<<<gw, 256, 0, c.stream>>>(bm.view(), rows, cols, rng, ms.best_s.p, ms.best_dS.p, c.counters,
                                             c.status);
   SBP_CHECK_LAUNCH();
@@ -764,10 +934,13 @@ static void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& 
     }
     block_map = gm.name;
   } else {
-    std::vector<int> rptr(B + 1), ridx(nnz[0]), rval(nnz[0]), dout(B), din(B);
-    SBP_CUDA(SBP_COPY_ASYNC(rptr.data(), ms.rptr.p, (B + 1) * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    SBP_CUDA(SBP_COPY_ASYNC(ridx.data(), ms.ridx.p, nnz[0] * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    SBP_CUDA(SBP_COPY_ASYNC(rval.data(), ms.rval.p, nnz[0] * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    std::vector<int> rptr(B + 1), dout(B), din(B);
+    SBP_CUDA(SBP_COPY_ASYNC(rptr.data(), rows.ptr, (B + 1) * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    nnz[0] = rptr[B];
+    std::vector<int> ridx(std::max(nnz[0], 1)), rval(std::max(nnz[0], 1));
+    SBP_CUDA(SBP_COPY_ASYNC(ridx.data(), rows.idx, nnz[0] * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    SBP_CUDA(SBP_COPY_ASYNC(rval.data(), rows.val, nnz[0] * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     SBP_CUDA(SBP_COPY_ASYNC(dout.data(), bm.d_out.p, B * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     SBP_CUDA(SBP_COPY_ASYNC(din.data(), bm.d_in.p, B * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     c.sync();
@@ -1001,6 +1174,19 @@ SbpStatus sbp_profile_read(SbpProfile* out, int32_t reset) {
   SBP_API_END
 }
 
+SbpStatus sbp_set_option(const char* name, int64_t value) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(name, "NULL option name");
+  const std::string n(name);
+  if (n == "dense_max_blocks") {
+    SBP_REQUIRE(value >= 1 && value <= (1 << 30), "dense_max_blocks out of range");
+    g_dense_max_blocks = (int)value;
+  } else {
+    throw Error(SBP_ERR_INVALID_ARGUMENT, "unknown option: " + n);
+  }
+  SBP_API_END
+}
+
 SbpStatus sbp_graph_create(int32_t V, int64_t n, const int32_t* src, const int32_t* dst, SbpGraph** out) {
   SBP_API_BEGIN
   SBP_REQUIRE(out, "out is NULL");
@@ -1158,6 +1344,7 @@ SbpStatus sbp_blockmodel_create(const SbpGraph* g, int32_t B, const int32_t* ass
   for (int v = 0; v < g->V; ++v) SBP_REQUIRE(assignment[v] >= 0 && assignment[v] < B, "block id out of range");
   Context& c = Context::get();
   auto bm = std::make_unique<SbpBlockmodel>();
+  bm->graph = g;
   bm->init_vertex_scratch(g->V);
   SBP_CUDA(SBP_COPY_ASYNC(bm->b.p, assignment, g->V * sizeof(int), cudaMemcpyHostToDevice, c.stream));
   bm->set_blocks(B);
@@ -1175,6 +1362,19 @@ SbpStatus sbp_blockmodel_copy(const SbpBlockmodel* src, SbpBlockmodel** out) {
   auto bm = std::make_unique<SbpBlockmodel>();
   bm->init_vertex_scratch(src->V);
   bm->set_blocks(src->B);
+  bm->graph = src->graph;
+  if (src->sparse) {
+    SBP_REQUIRE(src->graph, "copying a row-hashed blockmodel needs its graph");
+    SBP_CUDA(SBP_COPY_ASYNC(bm->b.p, src->b.p, src->V * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+    bm->graph = src->graph;
+    rebuild(*bm, *src->graph, false);
+    SBP_CUDA(SBP_COPY_ASYNC(bm->d.p, src->d.p, src->B * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+    bm->overall_entropy = src->overall_entropy;
+    bm->num_blocks_to_merge = 0;
+    c.sync();
+    *out = bm.release();
+    return SBP_OK;
+  }
   const size_t cells = (size_t)src->B * src->ld;
   SBP_CUDA(SBP_COPY_ASYNC(bm->b.p, src->b.p, src->V * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
   SBP_CUDA(SBP_COPY_ASYNC(bm->M.p, src->M.p, cells * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
@@ -1233,6 +1433,23 @@ SbpStatus sbp_get_block_matrix(const SbpBlockmodel* bm, int32_t* out) {
   SBP_API_BEGIN
   SBP_REQUIRE(bm && out, "NULL argument");
   Context& c = Context::get();
+  if (bm->sparse) {   // scatter the hashed rows into a dense device band, band by band
+    const int B = bm->B;
+    const int band = (int)std::max<long long>(1, std::min<long long>(B, (64LL << 20) / B));
+    DevBuf<int> dense;
+    dense.reserve((size_t)band * B);
+    for (int r0 = 0; r0 < B; r0 += band) {
+      const int rows = std::min(band, B - r0);
+      SBP_CUDA(cudaMemsetAsync(dense.p, 0, (size_t)rows * B * sizeof(int), c.stream));
+      k_hashed_to_dense<<<std::min(rows, 4096), 128, 0, c.stream>>>(bm->rbase.p, bm->rmask.p, bm->rslot.p, B, r0,
+                                                                   rows, dense.p);
+      SBP_CHECK_LAUNCH();
+      SBP_CUDA(SBP_COPY_ASYNC(out + (size_t)r0 * B, dense.p, (size_t)rows * B * sizeof(int), cudaMemcpyDeviceToHost,
+                              c.stream));
+      c.sync();
+    }
+    return SBP_OK;
+  }
   SBP_CUDA(cudaMemcpy2DAsync(out, bm->B * sizeof(int), bm->M.p, bm->ld * sizeof(int), bm->B * sizeof(int), bm->B,
                              cudaMemcpyDeviceToHost, c.stream));
   c.sync();
@@ -1304,9 +1521,24 @@ SbpStatus sbp_move_vertex(SbpBlockmodel* bm, const SbpGraph* g, int32_t vertex, 
   const int cap = mh_cap(g->h_k[vertex]);
   const size_t smem = (size_t)table_ints(cap) * sizeof(int);
   set_smem_limit((const void*)k_move_vertex, smem);
+  int r0 = 0;
+  SBP_CUDA(SBP_COPY_ASYNC(&r0, bm->b.p + vertex, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
   k_move_vertex<<<1, 32, smem, c.stream>>>(g->view(), bm->view(), vertex, block, cap, c.status);
   SBP_CHECK_LAUNCH();
   c.sync();
+  if (bm->sparse && r0 != block) {
+    int flags[3] = {0, 0, 0};
+    SBP_CUDA(SBP_COPY_ASYNC(&flags[0], bm->overflow.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    SBP_CUDA(SBP_COPY_ASYNC(&flags[1], c.status + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    if (flags[0]) {   // a hashed row ran out of room: rebuild with more room, keep d, finish d[r], d[s]
+      rebuild(*bm, *g, false);
+      ++g_overflow_rebuilds;
+      k_fix_move_degrees<<<1, 1, 0, c.stream>>>(bm->view(), r0, block, flags[1], flags[2]);
+      SBP_CHECK_LAUNCH();
+      c.sync();
+    }
+  }
   c.check_status();
   SBP_API_END
 }

@@ -62,7 +62,7 @@ __global__ void k_rebuild_smem(GraphView g, BlockView bm) {
 
 __global__ void k_rebuild_degrees(BlockView bm) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  if (x < bm.B) bm.d[x] = bm.d_out[x] + bm.d_in[x] - bm.M[(size_t)x * bm.ld + x];
+  if (x < bm.B) bm.d[x] = bm.d_out[x] + bm.d_in[x] - bm_get(bm, x, x);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -104,7 +104,7 @@ __global__ void k_mdl_edges(GraphView g, BlockView bm, const int* __restrict__ o
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < g.E; e += stride) {
     const int bv = bm.b[__ldg(out_src + e)], bu = bm.b[__ldg(g.out_idx + e)];
-    acc += log((double)bm.M[(size_t)bv * bm.ld + bu]);
+    acc += log((double)bm_get(bm, bv, bu));
   }
   for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < bm.B; x += stride)
     acc -= xlogx((double)bm.d_out[x]) + xlogx((double)bm.d_in[x]);
@@ -187,17 +187,28 @@ __global__ void __launch_bounds__(256, 2) k_gibbs_eval(GraphView g, BlockView bm
   }
 }
 
-// M[row,col] += delta with the transpose and both chunk sums kept in step (atomic).
+// M[row,col] += delta with the transpose kept in step: dense cells and both chunk sums, or the
+// two hashed rows (atomic).
 __device__ __forceinline__ void cell_add(const BlockView& bm, int row, int col, int delta) {
+  if (bm.sparse) {
+    hashed_add(bm.rbase, bm.rmask, bm.rslot, row, col, delta, bm.overflow);
+    hashed_add(bm.cbase, bm.cmask, bm.cslot, col, row, delta, bm.overflow);
+    return;
+  }
   atomicAdd(bm.M + (size_t)row * bm.ld + col, delta);
   atomicAdd(bm.MT + (size_t)col * bm.ld + row, delta);
   chunk_add(bm.CS, bm.nch, row, col, delta);
   chunk_add(bm.CST, bm.nch, col, row, delta);
 }
 
-// Same for a cell owned by one thread (plain update of M/MT, atomic chunk sums, which lanes share).
+// Same for a dense cell owned by one thread (plain update of M/MT, atomic chunk sums, which
+// lanes share); hashed rows are always updated atomically (lanes share their slots).
 __device__ __forceinline__ void cell_add_owned(const BlockView& bm, int row, int col, int delta) {
   if (!delta) return;
+  if (bm.sparse) {
+    cell_add(bm, row, col, delta);
+    return;
+  }
   bm.M[(size_t)row * bm.ld + col] += delta;
   bm.MT[(size_t)col * bm.ld + row] += delta;
   chunk_add(bm.CS, bm.nch, row, col, delta);
@@ -278,8 +289,8 @@ __global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n
     const int v = moved_list[i];
     const int r = bm.b[v], s = prop[v];
     const unsigned long long key = ((unsigned long long)gen << 32) | (unsigned)v;
-    if (last[r] == key) bm.d[r] = bm.d_out[r] + bm.d_in[r] - bm.M[(size_t)r * bm.ld + r] - qr[v];
-    if (last[s] == key) bm.d[s] = bm.d_out[s] + bm.d_in[s] - bm.M[(size_t)s * bm.ld + s] - qs[v];
+    if (last[r] == key) bm.d[r] = bm.d_out[r] + bm.d_in[r] - bm_get(bm, r, r) - qr[v];
+    if (last[s] == key) bm.d[s] = bm.d_out[s] + bm.d_in[s] - bm_get(bm, s, s) - qs[v];
     bm.b[v] = s;
     prop[v] = -1;
   }
@@ -293,19 +304,23 @@ __global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n
 // random record of a visit depends only on (vertex, sweep), so re-evaluation is idempotent.
 // out: [0] visits [1] proposals_moved [2] accepted (as doubles), [3] sum of accepted dS.
 // ------------------------------------------------------------------------------------------
-__global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
-                     int cap, double* out, int* status) {
+__global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, int n, int start, RngParams rng,
+                     int sweep, int cap, double* out, int* status) {
   extern __shared__ int smem[];
   __shared__ int s_acc[32], s_moved[32];
   __shared__ double s_dS[32];
-  __shared__ int s_first;
+  __shared__ int s_first, s_stop;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int W = blockDim.x >> 5;
   WarpTable t = carve_table(smem, cap, warp);
   init_table(t, lane);
   long long visits = 0, moved = 0, accepted = 0;
   double sum_dS = 0.0;
-  int pos = 0;
+  int pos = start;
+  if (threadIdx.x == 0) {
+    s_stop = 0;
+    out[4] = 0.0;
+  }
   __syncthreads();
   while (pos < n) {
     const int i = pos + warp;
@@ -340,7 +355,6 @@ __global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, i
       const int self = g.self[v];
       const MoveCounts mc = corner_counts(t, r, s);
       const int nl = *t.nlist;
-      const int ld = bm.ld;
       for (int j = lane; j < nl; j += kWarp) {
         const int h = t.list[j];
         const int u = t.keys[h], co = t.cout[h], ci = t.cin[h];
@@ -365,9 +379,22 @@ __global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, i
         bm.d_out[s] += k_out;
         bm.d_in[r] -= k_in + self;
         bm.d_in[s] += k_in + self;
-        // Blockmodel::move_vertex reads the already-updated diagonal and adds the delta again
-        bm.d[r] = bm.d_out[r] + bm.d_in[r] - (bm.M[(size_t)r * ld + r] + d_rr);
-        bm.d[s] = bm.d_out[s] + bm.d_in[s] - (bm.M[(size_t)s * ld + s] + d_ss);
+        __threadfence_block();
+        if (*bm.overflow) {
+          // a hashed row is full: stop here; the host rebuilds the rows with more room, sets
+          // d[r], d[s] from the rebuilt diagonal and these deltas, and resumes at pos+first+1
+          s_stop = 1;
+          out[4] = 1.0;
+          out[5] = (double)(pos + first);
+          out[6] = (double)r;
+          out[7] = (double)s;
+          out[8] = (double)d_rr;
+          out[9] = (double)d_ss;
+        } else {
+          // Blockmodel::move_vertex reads the already-updated diagonal and adds the delta again
+          bm.d[r] = bm.d_out[r] + bm.d_in[r] - (bm_get(bm, r, r) + d_rr);
+          bm.d[s] = bm.d_out[s] + bm.d_in[s] - (bm_get(bm, s, s) + d_ss);
+        }
       }
     }
     if (threadIdx.x == 0) {
@@ -382,6 +409,7 @@ __global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, i
     pos += first >= 0 ? first + 1 : W;
     table_reset(t, lane);
     __syncthreads();
+    if (s_stop) break;
   }
   if (threadIdx.x == 0) {
     out[0] = (double)visits;
@@ -406,7 +434,7 @@ __global__ void k_move_vertex(GraphView g, BlockView bm, int v, int s, int cap, 
   const int k_out = g.out_ptr[v + 1] - g.out_ptr[v];
   const int k_in = g.in_ptr[v + 1] - g.in_ptr[v];
   const MoveCounts mc = corner_counts(t, r, s);
-  const int nl = *t.nlist, ld = bm.ld;
+  const int nl = *t.nlist;
   for (int j = lane; j < nl; j += kWarp) {
     const int h = t.list[j];
     const int u = t.keys[h], co = t.cout[h], ci = t.cin[h];
@@ -429,8 +457,13 @@ __global__ void k_move_vertex(GraphView g, BlockView bm, int v, int s, int cap, 
     bm.d_out[s] += k_out;
     bm.d_in[r] -= k_in + self;
     bm.d_in[s] += k_in + self;
-    bm.d[r] = bm.d_out[r] + bm.d_in[r] - (bm.M[(size_t)r * ld + r] + d_rr);
-    bm.d[s] = bm.d_out[s] + bm.d_in[s] - (bm.M[(size_t)s * ld + s] + d_ss);
+    __threadfence_block();
+    if (!*bm.overflow) {
+      bm.d[r] = bm.d_out[r] + bm.d_in[r] - (bm_get(bm, r, r) + d_rr);
+      bm.d[s] = bm.d_out[s] + bm.d_in[s] - (bm_get(bm, s, s) + d_ss);
+    }
+    status[1] = d_rr;   // kept for the d fix-up after a row-capacity rebuild
+    status[2] = d_ss;
   }
 }
 
@@ -535,15 +568,12 @@ __global__ void k_row_fill(const int* A, int B, int ld, const int* ptr, int* idx
 //      - [g(do_r)+g(do_s)-g(do_r+do_s)] - [g(di_r)+g(di_s)-g(di_r+di_s)]
 // which equals entropy::block_merge_delta_mdl (src/entropy.cpp:127-180).
 __device__ double merge_delta(const BlockView& bm, const Csr& rows, const Csr& cols, int r, int s, int lane) {
-  const int ld = bm.ld;
   double dS = 0.0;
-  const int* Ms = bm.M + (size_t)s * ld;
-  const int* MTs = bm.MT + (size_t)s * ld;
   for (int j = rows.ptr[r] + lane; j < rows.ptr[r + 1]; j += kWarp) {
     const int c = rows.idx[j], m = rows.val[j];
     dS += xlogx((double)m);
     if (c != r && c != s) {
-      const int msc = Ms[c];
+      const int msc = bm_get(bm, s, c);
       dS += dxlogx((double)msc, (double)(msc + m));
     }
   }
@@ -552,13 +582,13 @@ __device__ double merge_delta(const BlockView& bm, const Csr& rows, const Csr& c
     if (c == r) continue;
     dS += xlogx((double)m);
     if (c != s) {
-      const int mcs = MTs[c];
+      const int mcs = bm_getT(bm, s, c);
       dS += dxlogx((double)mcs, (double)(mcs + m));
     }
   }
   dS = warp_sum(dS);
-  const int M_rr = bm.M[(size_t)r * ld + r], M_rs = bm.M[(size_t)r * ld + s];
-  const int M_sr = bm.M[(size_t)s * ld + r], M_ss = bm.M[(size_t)s * ld + s];
+  const int M_rr = bm_get(bm, r, r), M_rs = bm_get(bm, r, s);
+  const int M_sr = bm_get(bm, s, r), M_ss = bm_get(bm, s, s);
   dS += dxlogx((double)M_ss, (double)(M_ss + M_rr + M_rs + M_sr));
   const double dor = bm.d_out[r], dos = bm.d_out[s], dir = bm.d_in[r], dis = bm.d_in[s];
   dS -= xlogx(dor) + xlogx(dos) - xlogx(dor + dos);
@@ -595,7 +625,7 @@ __global__ void k_merge_propose(BlockView bm, Csr rows, Csr cols, RngParams rng,
           if (lane == 0) atomicOr(status, kErrScan);
           t = r;
         }
-        const long long m_tr = bm.M[(size_t)t * bm.ld + r], m_rt = bm.M[(size_t)r * bm.ld + t];
+        const long long m_tr = bm_get(bm, t, r), m_rt = bm_get(bm, r, t);
         const long long rowpart = (long long)bm.d_out[t] - m_tr;
         const long long total = rowpart + (long long)bm.d_in[t] - m_rt;
         if (total == 0) {

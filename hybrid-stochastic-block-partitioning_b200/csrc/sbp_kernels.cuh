@@ -26,8 +26,8 @@ __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, 
                               int* qr, int* qs, unsigned long long* last, unsigned gen);
 __global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved, int* prop,
                                const int* qr, const int* qs, const unsigned long long* last, unsigned gen);
-__global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
-                     int cap, double* out, int* status);
+__global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, int n, int start, RngParams rng,
+                     int sweep, int cap, double* out, int* status);
 __global__ void k_move_vertex(GraphView g, BlockView bm, int v, int s, int cap, int* status);
 __global__ void k_eval_list(GraphView g, BlockView bm, const int* verts, int n, const uint4* records, int cap,
                             int* out_s, double* out_dS, double* out_H, int* out_acc, int* status);
@@ -38,6 +38,25 @@ __global__ void k_merge_propose(BlockView bm, Csr rows, Csr cols, RngParams rng,
                                 unsigned long long* counters, int* status);
 __global__ void k_block_sizes(const int* b, int V, int* size);
 __global__ void k_relabel(int* b, int V, const int* map);
+
+// row-hashed block matrix (sbp_sparse.cu)
+__global__ void k_edge_keys(GraphView g, const int* __restrict__ b, const int* __restrict__ out_src, int B,
+                            unsigned long long* keys, unsigned long long* keysT);
+__global__ void k_unique_rows(const unsigned long long* __restrict__ ukeys, long long n, int B, unsigned* rowcnt);
+__global__ void k_row_caps(const unsigned* __restrict__ rowcnt, int B, unsigned* cap, int* mask);
+__global__ void k_fill_empty(int2* slot, long long n);
+__global__ void k_fill_rows(const long long* __restrict__ rowptr, const unsigned long long* __restrict__ ukeys,
+                            const long long* __restrict__ heads, long long nu, long long nedges, int B,
+                            const long long* __restrict__ base, const int* __restrict__ mask, int2* slot,
+                            int* csr_ptr, int* csr_idx, int* csr_val);
+__global__ void k_block_degrees(GraphView g, const int* __restrict__ b, int* d_out, int* d_in);
+__global__ void k_recover_assign(int* b, const int* moved, const int* n_moved, const int* prop, int* old_block);
+__global__ void k_recover_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved,
+                                 int* prop, const int* old_block, const int* qr, const int* qs,
+                                 const unsigned long long* last, unsigned gen);
+__global__ void k_fix_move_degrees(BlockView bm, int r, int s, int d_rr, int d_ss);
+__global__ void k_hashed_to_dense(const long long* __restrict__ base, const int* __restrict__ mask,
+                                  const int2* __restrict__ slot, int B, int row0, int rows, int* dense);
 
 // Shared-memory ints per warp table of `cap` slots (keys, out counts, in counts, used list, count).
 inline int table_ints(int cap) { return 4 * cap + 32; }

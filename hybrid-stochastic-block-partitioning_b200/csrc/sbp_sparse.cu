@@ -1,0 +1,120 @@
+// Kernels of the row-hashed (sparse) block matrix used when B is large: rebuild from the edge
+// list (Blockmodel::initialize_edge_counts, src/blockmodel/blockmodel.cpp:187-255, through a
+// sort of (b_src, b_dst) keys), and the repair steps after a hashed row ran out of room.
+#include "sbp_kernels.cuh"
+
+namespace sbpb {
+
+// (b[src], b[dst]) and (b[dst], b[src]) keys of every edge.
+__global__ void k_edge_keys(GraphView g, const int* __restrict__ b, const int* __restrict__ out_src, int B,
+                            unsigned long long* keys, unsigned long long* keysT) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < g.E; e += stride) {
+    const unsigned long long bs = (unsigned)b[__ldg(out_src + e)], bd = (unsigned)b[__ldg(g.out_idx + e)];
+    keys[e] = bs * (unsigned long long)B + bd;
+    keysT[e] = bd * (unsigned long long)B + bs;
+  }
+}
+
+// Non-zero cells per row from the unique sorted keys.
+__global__ void k_unique_rows(const unsigned long long* __restrict__ ukeys, long long n, int B, unsigned* rowcnt) {
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x)
+    atomicAdd(rowcnt + (ukeys[j] / (unsigned long long)B), 1u);
+}
+
+// Row capacity: a power of two with at least half free after the rebuild (room to grow).
+__global__ void k_row_caps(const unsigned* __restrict__ rowcnt, int B, unsigned* cap, int* mask) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < B; r += gridDim.x * blockDim.x) {
+    unsigned want = 2u * rowcnt[r] + 8u, c = 8u;
+    while (c < want) c <<= 1;
+    cap[r] = c;
+    mask[r] = (int)c - 1;
+  }
+}
+
+__global__ void k_fill_empty(int2* slot, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    slot[i] = make_int2(-1, 0);
+}
+
+// One thread per row inserts its cells in ascending column order, so the slot layout of a
+// rebuilt row is the same on every run.  Also writes the compressed (sorted) row.
+__global__ void k_fill_rows(const long long* __restrict__ rowptr, const unsigned long long* __restrict__ ukeys,
+                            const long long* __restrict__ heads, long long nu, long long nedges, int B,
+                            const long long* __restrict__ base, const int* __restrict__ mask, int2* slot,
+                            int* csr_ptr, int* csr_idx, int* csr_val) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < B; r += gridDim.x * blockDim.x) {
+    const long long j0 = rowptr[r], j1 = (r + 1 < B) ? rowptr[r + 1] : nu;
+    csr_ptr[r] = (int)j0;
+    if (r == B - 1) csr_ptr[B] = (int)nu;
+    const long long b0 = base[r];
+    const int m = mask[r];
+    for (long long j = j0; j < j1; ++j) {
+      const int col = (int)(ukeys[j] % (unsigned long long)B);
+      const int cnt = (int)(((j + 1 < nu) ? heads[j + 1] : nedges) - heads[j]);
+      csr_idx[j] = col;
+      csr_val[j] = cnt;
+      unsigned h = slot_hash(col) & (unsigned)m;
+      while (slot[b0 + h].x != -1) h = (h + 1) & (unsigned)m;   // capacity >= 2 * count + 8
+      slot[b0 + h] = make_int2(col, cnt);
+    }
+  }
+}
+
+// Block degrees from the vertices (out-degree; in-degree with the self loop).
+__global__ void k_block_degrees(GraphView g, const int* __restrict__ b, int* d_out, int* d_in) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < g.V; v += gridDim.x * blockDim.x) {
+    const int bv = b[v];
+    atomicAdd(d_out + bv, g.out_ptr[v + 1] - g.out_ptr[v]);
+    atomicAdd(d_in + bv, (g.in_ptr[v + 1] - g.in_ptr[v]) + g.self[v]);
+  }
+}
+
+// Gibbs batch whose apply overflowed a row: move the assignment now (keeping the old block),
+// so the rows can be rebuilt from it before the degree step.
+__global__ void k_recover_assign(int* b, const int* moved, const int* n_moved, const int* prop, int* old_block) {
+  const int n = *n_moved;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int v = moved[i];
+    old_block[v] = b[v];
+    b[v] = prop[v];
+  }
+}
+
+// The degree step of k_apply_finish on the rebuilt rows.
+__global__ void k_recover_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved,
+                                 int* prop, const int* old_block, const int* qr, const int* qs,
+                                 const unsigned long long* last, unsigned gen) {
+  const int n = *n_moved;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *next_n_moved = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int v = moved_list[i];
+    const int r = old_block[v], s = prop[v];
+    const unsigned long long key = ((unsigned long long)gen << 32) | (unsigned)v;
+    if (last[r] == key) bm.d[r] = bm.d_out[r] + bm.d_in[r] - bm_get(bm, r, r) - qr[v];
+    if (last[s] == key) bm.d[s] = bm.d_out[s] + bm.d_in[s] - bm_get(bm, s, s) - qs[v];
+    prop[v] = -1;
+  }
+}
+
+// d[r], d[s] of one move (Blockmodel::move_vertex) after its rows were rebuilt.
+__global__ void k_fix_move_degrees(BlockView bm, int r, int s, int d_rr, int d_ss) {
+  if (threadIdx.x || blockIdx.x) return;
+  bm.d[r] = bm.d_out[r] + bm.d_in[r] - (bm_get(bm, r, r) + d_rr);
+  bm.d[s] = bm.d_out[s] + bm.d_in[s] - (bm_get(bm, s, s) + d_ss);
+}
+
+// Dense dump of the hashed rows of M (for sbp_get_block_matrix): one thread per slot.
+__global__ void k_hashed_to_dense(const long long* __restrict__ base, const int* __restrict__ mask,
+                                  const int2* __restrict__ slot, int B, int row0, int rows, int* dense) {
+  for (int r = row0 + blockIdx.x; r < row0 + rows && r < B; r += gridDim.x) {
+    const long long b0 = base[r];
+    const int cap = mask[r] + 1;
+    for (int i = threadIdx.x; i < cap; i += blockDim.x) {
+      const int2 e = slot[b0 + i];
+      if (e.x >= 0) dense[(size_t)(r - row0) * B + e.x] = e.y;
+    }
+  }
+}
+
+}  // namespace sbpb

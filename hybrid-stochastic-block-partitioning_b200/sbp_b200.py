@@ -24,7 +24,7 @@ STATUS = {0: "SBP_OK", 1: "SBP_ERR_INVALID_ARGUMENT", 2: "SBP_ERR_CUDA", 3: "SBP
           4: "SBP_ERR_REPLAY", 5: "SBP_ERR_DEVICE", 6: "SBP_ERR_OUT_OF_MEMORY"}
 
 EXPORTED = [
-    "sbp_last_error", "sbp_device_count", "sbp_get_stream", "sbp_profile_enable", "sbp_profile_read",
+    "sbp_last_error", "sbp_device_count", "sbp_set_option", "sbp_get_stream", "sbp_profile_enable", "sbp_profile_read",
     "sbp_graph_create", "sbp_graph_destroy", "sbp_graph_num_edges",
     "sbp_graph_get_split", "sbp_graph_set_split", "sbp_blockmodel_create", "sbp_blockmodel_copy",
     "sbp_blockmodel_destroy", "sbp_blockmodel_num_blocks", "sbp_blockmodel_set_num_blocks_to_merge",
@@ -46,7 +46,7 @@ class Replay(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("visits", ctypes.c_int64), ("proposals_moved", ctypes.c_int64), ("accepted", ctypes.c_int64),
                 ("sweeps", ctypes.c_int32), ("outer_iterations", ctypes.c_int32), ("num_blocks", ctypes.c_int32),
-                ("_pad", ctypes.c_int32), ("mdl", ctypes.c_double), ("mcmc_seconds", ctypes.c_double),
+                ("overflow_rebuilds", ctypes.c_int32), ("mdl", ctypes.c_double), ("mcmc_seconds", ctypes.c_double),
                 ("merge_seconds", ctypes.c_double), ("merge_proposals", ctypes.c_int64),
                 ("merge_avoided", ctypes.c_int64), ("total_seconds", ctypes.c_double)]
 
@@ -94,6 +94,7 @@ def load(path=LIB_PATH):
     L.sbp_device_count.restype = ctypes.c_int32
     for name in EXPORTED[2:]:
         getattr(L, name).restype = ctypes.c_int
+    L.sbp_set_option.argtypes = [ctypes.c_char_p, ctypes.c_int64]
     L.sbp_get_stream.argtypes = [pp]
     L.sbp_profile_enable.argtypes = [ctypes.c_int32]
     L.sbp_profile_read.argtypes = [ctypes.POINTER(Profile), ctypes.c_int32]
@@ -144,6 +145,11 @@ def _replay(records):
 
 def device_count():
     return load().sbp_device_count()
+
+
+def set_option(name, value):
+    """Engine option, e.g. set_option("dense_max_blocks", 16384)."""
+    _check(load().sbp_set_option(name.encode(), int(value)))
 
 
 def stream_handle():

@@ -55,7 +55,7 @@ typedef struct {
     int32_t sweeps;            /* MCMC iterations */
     int32_t outer_iterations;  /* partition only: merge+finetune rounds */
     int32_t num_blocks;        /* blocks after the call */
-    int32_t _pad;
+    int32_t overflow_rebuilds; /* row-hashed storage rebuilt because a row ran out of room */
     double mdl;                /* overall entropy after the call (the reference stores it as float) */
     double mcmc_seconds;       /* device time spent in finetune */
     double merge_seconds;      /* device time spent in block merge */
@@ -106,6 +106,12 @@ const char *sbp_last_error(void);
 /* Number of usable CUDA devices (0 if none). */
 int32_t sbp_device_count(void);
 
+/* Engine options (no reference counterpart).  "dense_max_blocks": blockmodels with more blocks
+ * than this keep their block matrix as row-hashed regions (a sparse device-resident matrix with
+ * integer counts updated by atomics) instead of dense B x B arrays; default 16384.  Applies to
+ * blockmodels whose block count is set after the call. */
+SbpStatus sbp_set_option(const char *name, int64_t value);
+
 /* The CUDA stream every call of this library runs on (cudaStream_t), for interop and timing.
  * No reference counterpart (the reference is CPU-only). */
 SbpStatus sbp_get_stream(void **out);
@@ -132,7 +138,8 @@ SbpStatus sbp_graph_set_split(SbpGraph *graph, int32_t num_high, const int32_t *
  * counts rebuilt on the device (Blockmodel::initialize_edge_counts, blockmodel.cpp:187-255). */
 SbpStatus sbp_blockmodel_create(const SbpGraph *graph, int32_t num_blocks, const int32_t *assignment,
                                 SbpBlockmodel **out);
-/* Blockmodel::copy (src/blockmodel/blockmodel.cpp:95-105). */
+/* Blockmodel::copy (src/blockmodel/blockmodel.cpp:95-105).  A blockmodel keeps a reference to
+ * the graph it was created on; the graph must outlive it and its copies. */
 SbpStatus sbp_blockmodel_copy(const SbpBlockmodel *src, SbpBlockmodel **out);
 SbpStatus sbp_blockmodel_destroy(SbpBlockmodel *bm);
 SbpStatus sbp_blockmodel_num_blocks(const SbpBlockmodel *bm, int32_t *out);

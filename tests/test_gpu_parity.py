@@ -13,6 +13,14 @@ pytestmark = pytest.mark.gpu
 RTOL_MDL = 1e-9
 
 
+@pytest.fixture(params=["dense", "hashed"])
+def storage(request, S):
+    """Run the test with dense B x B counts and again with the row-hashed block matrix."""
+    S.set_option("dense_max_blocks", 16384 if request.param == "dense" else 1)
+    yield request.param
+    S.set_option("dense_max_blocks", 16384)
+
+
 def pair(S, O, V, s, d, B, a):
     g, og = S.Graph(V, s, d), O.Graph(V, s, d)
     return g, og, S.Blockmodel(g, B, a), O.Blockmodel(og, B, a)
@@ -46,7 +54,7 @@ def test_toy_known_answers_on_gpu(S, O):
         assert diff[r, c] == v
 
 
-def test_complex_move_matches_oracle(S, O):
+def test_complex_move_matches_oracle(S, O, storage):
     fx = toy_fixture()
     e = np.array(fx["edges"], np.int32)
     a = np.array(fx["complex_assignment"], np.int32)
@@ -58,7 +66,7 @@ def test_complex_move_matches_oracle(S, O):
 
 
 @pytest.mark.parametrize("V,K,B,seed", [(60, 3, 5, 1), (500, 6, 40, 2), (2000, 10, 300, 3), (3000, 20, 1200, 4)])
-def test_mdl_matches_oracle(S, O, V, K, B, seed):
+def test_mdl_matches_oracle(S, O, storage, V, K, B, seed):
     V, s, d, _ = random_graph(V, K, seed)
     a = random_assignment(V, B, seed)
     g, og, bm, obm = pair(S, O, V, s, d, B, a)
@@ -67,7 +75,7 @@ def test_mdl_matches_oracle(S, O, V, K, B, seed):
 
 
 @pytest.mark.parametrize("V,K,B,seed", [(300, 5, 12, 1), (1500, 8, 200, 2), (800, 6, 3, 3)])
-def test_evaluate_vertices_matches_oracle(S, O, V, K, B, seed):
+def test_evaluate_vertices_matches_oracle(S, O, storage, V, K, B, seed):
     V, s, d, _ = random_graph(V, K, seed)
     a = random_assignment(V, B, seed)
     g, og, bm, obm = pair(S, O, V, s, d, B, a)
@@ -90,7 +98,7 @@ def test_evaluate_vertices_matches_oracle(S, O, V, K, B, seed):
 
 @pytest.mark.parametrize("algo", ["metropolis_hastings", "asynchronous_gibbs", "hybrid_mcmc"])
 @pytest.mark.parametrize("V,K,B,batches,seed", [(400, 5, 20, 4, 11), (1200, 8, 150, 10, 12), (900, 6, 6, 3, 13)])
-def test_finetune_bit_exact(S, O, algo, V, K, B, batches, seed):
+def test_finetune_bit_exact(S, O, storage, algo, V, K, B, batches, seed):
     V, s, d, _ = random_graph(V, K, seed)
     a = random_assignment(V, B, seed)
     g, og, bm, obm = pair(S, O, V, s, d, B, a)
@@ -106,7 +114,7 @@ def test_finetune_bit_exact(S, O, algo, V, K, B, batches, seed):
 
 
 @pytest.mark.parametrize("algo", [0, 1, 2])
-def test_finetune_replay_bit_exact(S, O, algo):
+def test_finetune_replay_bit_exact(S, O, storage, algo):
     V, s, d, _ = random_graph(700, 6, 21)
     a = random_assignment(V, 30, 21)
     g, og, bm, obm = pair(S, O, V, s, d, 30, a)
@@ -129,7 +137,7 @@ def test_replay_too_short_is_an_error(S):
 
 @pytest.mark.parametrize("approximate", [True, False])
 @pytest.mark.parametrize("V,K,B,merge,seed", [(500, 5, 60, 30, 31), (1500, 8, 700, 350, 32), (300, 4, 9, 4, 33)])
-def test_merge_blocks_bit_exact(S, O, approximate, V, K, B, merge, seed):
+def test_merge_blocks_bit_exact(S, O, storage, approximate, V, K, B, merge, seed):
     V, s, d, _ = random_graph(V, K, seed)
     a = random_assignment(V, B, seed)
     g, og, bm, obm = pair(S, O, V, s, d, B, a)
@@ -157,7 +165,7 @@ def test_merge_replay_bit_exact(S, O):
 
 
 @pytest.mark.parametrize("algo", ["metropolis_hastings", "async_gibbs", "hybrid_mcmc"])
-def test_partition_bit_exact(S, O, algo):
+def test_partition_bit_exact(S, O, storage, algo):
     V, s, d, truth = random_graph(500, 5, 51, kmin=6, kmax=40, w=0.85, alpha=10.0)
     g, og = S.Graph(V, s, d), O.Graph(V, s, d)
     out, st = S.sbp.stochastic_block_partition(g, algorithm=algo, batches=5, seed=9)
@@ -170,7 +178,7 @@ def test_partition_bit_exact(S, O, algo):
     assert O.nmi(out, truth) > 0.8
 
 
-def test_edge_cases(S, O):
+def test_edge_cases(S, O, storage):
     # isolated vertices and a vertex with only a self loop
     s = np.array([0, 1, 2, 5, 5, 6], np.int32)
     d = np.array([1, 2, 0, 5, 6, 5], np.int32)
@@ -220,3 +228,23 @@ def test_config2_sweeps_keep_invariants(S, O):
         rdo, rdi, _ = rebuilt.degrees_all()
         assert np.array_equal(do, rdo) and np.array_equal(di, rdi)
         assert S.entropy.mdl(bm) == pytest.approx(S.entropy.mdl(rebuilt), rel=1e-12)
+
+
+def test_hashed_rows_grow_and_stay_exact(S, O):
+    """Finetune from many tiny blocks on the row-hashed matrix: rows fill up as blocks grow,
+    the storage is rebuilt with more room, and the chain stays bit-exact with the oracle."""
+    S.set_option("dense_max_blocks", 1)
+    try:
+        V, s, d, _ = random_graph(2000, 8, 61, kmin=6, kmax=60, w=0.8)
+        a = random_assignment(V, 900, 61)
+        g, og, bm, obm = pair(S, O, V, s, d, 900, a)
+        total = 0
+        for algo in (1, 2, 0):
+            st = S.finetune.run(bm, algo, batches=4, seed=algo + 3, call=algo, max_sweeps=8)
+            ost = obm.finetune(algo, batches=4, seed=algo + 3, call=algo, max_sweeps=8)
+            assert_same_state(bm, obm)
+            assert st["accepted"] == ost["accepted"]
+            total += st["overflow_rebuilds"]
+        assert total > 0, "the test no longer drives the rows past their capacity"
+    finally:
+        S.set_option("dense_max_blocks", 16384)
