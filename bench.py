@@ -219,6 +219,7 @@ def main():
     prof0 = S.profile_read()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     visits, outs = 0, []
+    torch.cuda.profiler.start()   # a profiler run with --profile-from-start off sees the timed steps only
     e0.record(ext)
     step_s = []
     for k in range(a.steps):
@@ -228,6 +229,7 @@ def main():
         step_s.append(round(st["total_seconds"], 4))
     e1.record(ext)
     barrier()
+    torch.cuda.profiler.stop()
     prof1 = S.profile_read()
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
