@@ -5,8 +5,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-SOURCES = ["sbp_kernels.cu", "sbp_sparse.cu", "sbp_sort.cu", "sbp_engine.cu", "sbp_noalloc.cu"]
-HEADERS = ["sbp_device.cuh", "sbp_kernels.cuh", "sbp_sort.cuh", os.path.join("..", "..", "include", "sbp_b200.h")]
+SOURCES = ["sbp_kernels.cu", "sbp_sparse.cu", "sbp_sort.cu", "sbp_engine.cu", "sbp_mlp.cu", "sbp_learned.cu",
+           "sbp_noalloc.cu"]
+HEADERS = ["sbp_device.cuh", "sbp_kernels.cuh", "sbp_sort.cuh", "sbp_engine.cuh", "sbp_mlp.cuh", os.path.join("..", "..", "include", "sbp_b200.h")]
 LIB = os.path.join(HERE, "libsbp_b200.so")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared"]

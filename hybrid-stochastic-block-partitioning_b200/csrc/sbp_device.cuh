@@ -355,6 +355,30 @@ __device__ __forceinline__ void table_add(const WarpTable& t, int key, bool vali
   }
 }
 
+// Per-warp table of `cap` slots carved from a CTA's dynamic shared memory (table_ints(cap) ints per warp).
+__device__ __forceinline__ WarpTable carve_table(int* base, int cap, int warp) {
+  int* p = base + (size_t)warp * (4 * cap + 32);
+  WarpTable t;
+  t.keys = p;
+  t.cout = p + cap;
+  t.cin = p + 2 * cap;
+  t.list = p + 3 * cap;
+  t.nlist = p + 4 * cap;
+  t.mask = cap - 1;
+  return t;
+}
+
+__device__ __forceinline__ void init_table(const WarpTable& t, int lane) {
+  const int cap = t.mask + 1;
+  for (int i = lane; i < cap; i += kWarp) {
+    t.keys[i] = -1;
+    t.cout[i] = 0;
+    t.cin[i] = 0;
+  }
+  if (lane == 0) *t.nlist = 0;
+  __syncwarp();
+}
+
 __device__ __forceinline__ void table_reset(const WarpTable& t, int lane) {
   __syncwarp();
   const int n = *t.nlist;
@@ -434,30 +458,13 @@ __device__ __forceinline__ void table_add_dir(const WarpTable& t, int key, bool 
   }
 }
 
-// Full evaluation of vertex v against the current state, table left filled on return
-// (caller resets it). Every lane returns the same result.
-//  1. one pass over the virtual neighbour list (out list incl. the self loop, then in list
-//     without it) gathers every neighbour's block into the table; the proposal's neighbour
-//     (element floor(x0 * k)) is one of these elements, so its block comes from the same gather;
-//  2. the multinomial walk over M[t,:] + M[:,t] picks s;
-//  3. one load round over the distinct neighbour blocks gives the Hastings sums and the changed
-//     cells; the corner cells, degree terms and the net-zero double count are spread over lanes.
-__device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const BlockView& bm, int v, uint4 x,
-                                                      const WarpTable& t, int lane, int* status, int* r_out,
-                                                      int* k_out_out, int* k_in_out) {
-  EvalResult res;
-  const int r = bm.b[v];
-  const int o0 = g.out_ptr[v], o1 = g.out_ptr[v + 1];
-  const int i0 = g.in_ptr[v], i1 = g.in_ptr[v + 1];
-  const int self = g.self[v];
-  const int k_out = o1 - o0, k_in = i1 - i0, k = k_out + k_in;
-  *r_out = r;
-  *k_out_out = k_out;
-  *k_in_out = k_in;
-  res.accepted = 0;
-  res.dS = 0.0;
-  res.H = 1.0;
-  const int idx = k > 0 ? (int)scale32(x.x, k) : -1;
+// One pass over v's virtual neighbour list (out list incl. the self loop, then in list without
+// it) gathers every neighbour's block into the table (self loop excluded from the counts, its
+// block r inserted with zero counts).  Returns the block of neighbour element `idx` (-1 when
+// idx is out of range), the proposal's neighbour of src/common.cpp:11-26.
+__device__ __forceinline__ int gather_neighbour_blocks(const GraphView& g, const BlockView& bm, int v, int r, int o0,
+                                                       int k_out, int i0, int k, int self, int idx,
+                                                       const WarpTable& t, int lane, int* status) {
   int tblk = -1;
   for (int base = 0; base < k; base += 2 * kWarp) {   // two elements per lane in flight
     const int e0 = base + lane, e1 = base + kWarp + lane;
@@ -472,34 +479,19 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
     table_add_dir(t, b1, u1 >= 0 && u1 != v, e1 >= k_out, status);
   }
   if (lane == 0 && self) table_slot(t, r, status);
+  return tblk;
+}
 
-  int s;
-  if (k == 0) {
-    s = random_block(r, bm.B, x.y);
-  } else {
-    const int dot = bm.d_out[tblk];
-    const long long total = (long long)dot + (long long)bm.d_in[tblk];
-    const long long target = scale32(x.y, total);
-    if (bm.sparse) {
-      if (target < dot) s = warp_select_hashed(bm.rbase, bm.rmask, bm.rslot, tblk, bm.B, target, lane);
-      else s = warp_select_hashed(bm.cbase, bm.cmask, bm.cslot, tblk, bm.B, target - dot, lane);
-    } else if (target < dot) {
-      s = warp_select_chunked(bm.M + (size_t)tblk * bm.ld, bm.CS + (size_t)tblk * bm.nch, bm.nch, target, lane);
-    } else {
-      s = warp_select_chunked(bm.MT + (size_t)tblk * bm.ld, bm.CST + (size_t)tblk * bm.nch, bm.nch, target - dot,
-                              lane);
-    }
-    if (s < 0) {
-      if (lane == 0) atomicOr(status, kErrScan);
-      s = r;
-    }
-  }
-  res.s = s;
-  if (s == r) return res;
+// Delta-MDL of moving v from r to s (s != r) against the current state, with the gathered
+// table of v's neighbour blocks, and the reference's Hastings correction (*H).  One load round
+// over the distinct neighbour blocks gives the Hastings sums and the changed cells; the corner
+// cells, degree terms and the net-zero double count are spread over lanes.  Every lane
+// returns the same values.
+__device__ __forceinline__ double move_delta(const GraphView& g, const BlockView& bm, int r, int s, int k_out,
+                                             int k_in, int self, const WarpTable& t, int lane, double* H) {
   __syncwarp();
-
   const MoveCounts mc = corner_counts(t, r, s);
-  const int B = bm.B, ld = bm.ld;
+  const int B = bm.B;
   const int d_rr = -mc.co_r - mc.ci_r - self;
   const int d_rs = -mc.co_s + mc.ci_r;
   const int d_sr = mc.co_r - mc.ci_s;
@@ -508,7 +500,6 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
   const int M_sr = bm_get(bm, s, r), M_ss = bm_get(bm, s, s);
   const int dout_r = bm.d_out[r], dout_s = bm.d_out[s], din_r = bm.d_in[r], din_s = bm.d_in[s];
   const int kin_self = k_in + self;
-  (void)ld;
 
   double fwd = 0.0, bwd = 0.0, dS = 0.0;
   long long T = 0;   // integer scale of the changed cells and degrees (zero snap below)
@@ -559,8 +550,60 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
   // A mathematically zero change reads as exactly 0 whatever the summation order: the
   // Metropolis-Hastings early stop tests `delta == 0.0` (src/finetune.cpp:147).
   if (fabs(dS) <= 0x1p-40 * (double)T * log(g.E > 2 ? (double)g.E : 2.0)) dS = 0.0;
+  *H = bwd / fwd;
+  return dS;
+}
 
-  const double H = (k == 0) ? 1.0 : bwd / fwd;
+// Full evaluation of vertex v against the current state, table left filled on return
+// (caller resets it). Every lane returns the same result.
+//  1. gather_neighbour_blocks; the proposal's neighbour (element floor(x0 * k)) is one of the
+//     gathered elements, so its block comes from the same pass;
+//  2. the multinomial walk over M[t,:] + M[:,t] picks s;
+//  3. move_delta gives delta-MDL and the Hastings correction.
+__device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const BlockView& bm, int v, uint4 x,
+                                                      const WarpTable& t, int lane, int* status, int* r_out,
+                                                      int* k_out_out, int* k_in_out) {
+  EvalResult res;
+  const int r = bm.b[v];
+  const int o0 = g.out_ptr[v], o1 = g.out_ptr[v + 1];
+  const int i0 = g.in_ptr[v], i1 = g.in_ptr[v + 1];
+  const int self = g.self[v];
+  const int k_out = o1 - o0, k_in = i1 - i0, k = k_out + k_in;
+  *r_out = r;
+  *k_out_out = k_out;
+  *k_in_out = k_in;
+  res.accepted = 0;
+  res.dS = 0.0;
+  res.H = 1.0;
+  const int idx = k > 0 ? (int)scale32(x.x, k) : -1;
+  const int tblk = gather_neighbour_blocks(g, bm, v, r, o0, k_out, i0, k, self, idx, t, lane, status);
+
+  int s;
+  if (k == 0) {
+    s = random_block(r, bm.B, x.y);
+  } else {
+    const int dot = bm.d_out[tblk];
+    const long long total = (long long)dot + (long long)bm.d_in[tblk];
+    const long long target = scale32(x.y, total);
+    if (bm.sparse) {
+      if (target < dot) s = warp_select_hashed(bm.rbase, bm.rmask, bm.rslot, tblk, bm.B, target, lane);
+      else s = warp_select_hashed(bm.cbase, bm.cmask, bm.cslot, tblk, bm.B, target - dot, lane);
+    } else if (target < dot) {
+      s = warp_select_chunked(bm.M + (size_t)tblk * bm.ld, bm.CS + (size_t)tblk * bm.nch, bm.nch, target, lane);
+    } else {
+      s = warp_select_chunked(bm.MT + (size_t)tblk * bm.ld, bm.CST + (size_t)tblk * bm.nch, bm.nch, target - dot,
+                              lane);
+    }
+    if (s < 0) {
+      if (lane == 0) atomicOr(status, kErrScan);
+      s = r;
+    }
+  }
+  res.s = s;
+  if (s == r) return res;
+  double Hp;
+  const double dS = move_delta(g, bm, r, s, k_out, k_in, self, t, lane, &Hp);
+  const double H = (k == 0) ? 1.0 : Hp;
   double ap = exp(-3.0 * dS) * H;
   ap = ap >= 1.0 ? 1.0 : ap;
   res.dS = dS;

@@ -4,366 +4,8 @@
 // src/blockmodel/blockmodel_triplet.cpp:3-100, src/finetune.cpp:31-162,342-444,
 // src/block_merge.cpp:123-311); all per-vertex and per-block work runs in the kernels of
 // sbp_kernels.cu.  No CPU fallback: every compute entry point needs a CUDA device.
-#include <algorithm>
-#include <cmath>
-#include <cstdio>
-#include <cstring>
-#include <memory>
-#include <numeric>
-#include <stdexcept>
-#include <string>
-#include <unordered_map>
-#include <vector>
+#include "sbp_engine.cuh"
 
-#include "../../include/sbp_b200.h"
-#include "sbp_kernels.cuh"
-#include "sbp_sort.cuh"
-
-namespace sbpb {
-
-// ------------------------------------------------------------------------------------------
-// Errors
-// ------------------------------------------------------------------------------------------
-struct Error : std::runtime_error {
-  SbpStatus code;
-  Error(SbpStatus c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
-
-static thread_local std::string g_last_error;
-
-#define SBP_CUDA(x)                                                                                     \
-  do {                                                                                                  \
-    cudaError_t e_ = (x);                                                                               \
-    if (e_ != cudaSuccess) {                                                                            \
-      if (e_ == cudaErrorMemoryAllocation) throw Error(SBP_ERR_OUT_OF_MEMORY, std::string(#x) + ": " + cudaGetErrorString(e_)); \
-      throw Error(SBP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));                       \
-    }                                                                                                   \
-  } while (0)
-
-static long long g_launches = 0;   // kernels launched by this library (all entry points)
-static long long g_h2d = 0, g_d2h = 0;   // bytes copied host->device / device->host
-
-#define SBP_CHECK_LAUNCH() \
-  do {                     \
-    ++g_launches;          \
-    SBP_CUDA(cudaGetLastError()); \
-  } while (0)
-
-static cudaError_t count_copy(cudaError_t e, size_t bytes, cudaMemcpyKind kind) {
-  if (kind == cudaMemcpyHostToDevice) g_h2d += (long long)bytes;
-  if (kind == cudaMemcpyDeviceToHost) g_d2h += (long long)bytes;
-  return e;
-}
-#define SBP_COPY(dst, src, bytes, kind) count_copy(cudaMemcpy(dst, src, bytes, kind), bytes, kind)
-#define SBP_COPY_ASYNC(dst, src, bytes, kind, stream) \
-  count_copy(cudaMemcpyAsync(dst, src, bytes, kind, stream), bytes, kind)
-
-template <class T>
-struct DevBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  DevBuf() = default;
-  DevBuf(const DevBuf&) = delete;
-  DevBuf& operator=(const DevBuf&) = delete;
-  ~DevBuf() { release(); }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-  void reserve(size_t count) {   // grow-only, contents not preserved
-    if (count <= n && p) return;
-    release();
-    SBP_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
-    n = std::max<size_t>(count, 1);
-  }
-};
-
-// ------------------------------------------------------------------------------------------
-// Process-wide context: one stream, the device status word, counters and readback buffers.
-// ------------------------------------------------------------------------------------------
-struct Context {
-  cudaStream_t stream = nullptr;
-  int num_sms = 0;
-  int* status = nullptr;                 // device error bits
-  unsigned long long* counters = nullptr;  // device counters [8]
-  double* partial = nullptr;             // MDL partial sums
-  double* scalar = nullptr;              // MDL result
-  double* mh_out = nullptr;              // MH sweep outputs [4]
-  int npartial = 0;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-
-  static Context& get() {
-    static Context* ctx = nullptr;
-    if (!ctx) {
-      int n = 0;
-      if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
-        cudaGetLastError();
-        throw Error(SBP_ERR_CUDA, "no CUDA device available (the engine has no CPU fallback)");
-      }
-      auto* c = new Context();
-      SBP_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-      int dev = 0;
-      SBP_CUDA(cudaGetDevice(&dev));
-      SBP_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
-      c->npartial = 4 * c->num_sms;
-      SBP_CUDA(cudaMalloc(&c->status, 8 * sizeof(int)));
-      SBP_CUDA(cudaMalloc(&c->counters, 8 * sizeof(unsigned long long)));
-      SBP_CUDA(cudaMalloc(&c->partial, c->npartial * sizeof(double)));
-      SBP_CUDA(cudaMalloc(&c->scalar, sizeof(double)));
-      SBP_CUDA(cudaMalloc(&c->mh_out, 16 * sizeof(double)));
-      SBP_CUDA(cudaMemset(c->status, 0, 8 * sizeof(int)));
-      SBP_CUDA(cudaEventCreate(&c->ev0));
-      SBP_CUDA(cudaEventCreate(&c->ev1));
-      ctx = c;
-    }
-    return *ctx;
-  }
-  void sync() { SBP_CUDA(cudaStreamSynchronize(stream)); }
-  // Read and clear the device status word; throw on any error bit.
-  void check_status() {
-    int st = 0;
-    SBP_CUDA(SBP_COPY_ASYNC(&st, status, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    sync();
-    if (st) {
-      SBP_CUDA(cudaMemsetAsync(status, 0, sizeof(int), stream));
-      if (st & kErrReplay) throw Error(SBP_ERR_REPLAY, "replay stream shorter than the run needs");
-      char msg[160];
-      snprintf(msg, sizeof msg, "device status 0x%x (table overflow=1, multinomial walk=2, bounds=8)", st);
-      throw Error(SBP_ERR_DEVICE, msg);
-    }
-  }
-};
-
-// Optional timing of the vertex-evaluation kernel: CUDA events around every light-vertex
-// evaluation launch on the launching stream, resolved when the profile is read.
-struct EvalProfiler {
-  bool on = false;
-  std::vector<cudaEvent_t> pool;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
-  double ms = 0.0, bytes = 0.0;
-  long long launches = 0, visits = 0;
-  cudaEvent_t get() {
-    if (!pool.empty()) {
-      cudaEvent_t e = pool.back();
-      pool.pop_back();
-      return e;
-    }
-    cudaEvent_t e;
-    SBP_CUDA(cudaEventCreate(&e));
-    return e;
-  }
-  void resolve() {
-    for (auto& pr : pending) {
-      SBP_CUDA(cudaEventSynchronize(pr.second));
-      float t = 0.f;
-      SBP_CUDA(cudaEventElapsedTime(&t, pr.first, pr.second));
-      ms += t;
-      pool.push_back(pr.first);
-      pool.push_back(pr.second);
-    }
-    pending.clear();
-  }
-};
-static EvalProfiler g_prof;
-
-static int grid_for(long long work_items, int per_block, int max_blocks) {
-  long long g = (work_items + per_block - 1) / per_block;
-  if (g < 1) g = 1;
-  if (g > max_blocks) g = max_blocks;
-  return (int)g;
-}
-
-static int pow2_at_least(int x) {
-  int c = 1;
-  while (c < x) c <<= 1;
-  return c;
-}
-
-constexpr int kLightCap = 256;        // per-warp table slots for light vertices
-constexpr int kLightCapMax = 512;     // largest per-warp table of the 8-warp evaluation CTA
-constexpr int kLightWarps = 8;
-constexpr int kMaxCap = 8192;         // largest per-warp table
-constexpr size_t kSmemBudget = 200 * 1024;
-constexpr int kSmemRebuildMaxB = 100;
-
-// Blocks above which the block matrix is row-hashed instead of dense (sbp_set_option).
-static int g_dense_max_blocks = 16384;
-static long long g_overflow_rebuilds = 0;   // rebuilds forced by a full hashed row
-
-}  // namespace sbpb
-
-using namespace sbpb;
-
-// ------------------------------------------------------------------------------------------
-// Graph
-// ------------------------------------------------------------------------------------------
-struct BatchPlan {
-  DevBuf<int> order;                       // per batch: light vertices then heavy vertices
-  std::vector<int> light_begin, light_n, heavy_begin, heavy_n;
-  std::vector<double> light_bytes;         // algorithmic bytes of each light evaluation launch
-  int max_batch = 0;
-};
-
-struct SbpGraph {
-  int V = 0;
-  long long E = 0;
-  DevBuf<int> out_ptr, out_idx, out_src, in_ptr, in_idx, identity, high_dev;
-  DevBuf<unsigned char> self;
-  std::vector<int> h_k;        // k_out + k_in per vertex (self loop counted once, on the out side)
-  std::vector<int> high, low;  // hybrid split
-  int max_k = 0;
-  int heavy_cap = 512;         // table slots for heavy vertices
-  int light_cap = 256;         // table slots per warp for light vertices (k <= light_cap / 2)
-  std::unordered_map<long long, std::unique_ptr<BatchPlan>> plans;
-
-  GraphView view() const {
-    GraphView g;
-    g.V = V;
-    g.E = E;
-    g.out_ptr = out_ptr.p;
-    g.out_idx = out_idx.p;
-    g.in_ptr = in_ptr.p;
-    g.in_idx = in_idx.p;
-    g.self = self.p;
-    return g;
-  }
-
-  int max_k_of(const std::vector<int>& verts) const {
-    int m = 0;
-    for (int v : verts) m = std::max(m, h_k[v]);
-    return m;
-  }
-
-  // Batches of asynchronous Gibbs over `list` (src/finetune.cpp:43-47, 352-366): batch_size =
-  // ceil(n / batches), loop bound n / batch_size (a trailing partial batch is skipped).
-  BatchPlan& plan(int algo, int batches) {
-    const long long key = (long long)algo * 1000003LL + batches;
-    auto it = plans.find(key);
-    if (it != plans.end()) return *it->second;
-    std::vector<int> list;
-    if (algo == SBP_ASYNC_GIBBS) {
-      list.resize(V);
-      std::iota(list.begin(), list.end(), 0);
-    } else {
-      list = low;
-    }
-    auto p = std::make_unique<BatchPlan>();
-    const int n = (int)list.size();
-    const int batch_size = (int)std::ceil(n / (double)batches);
-    std::vector<int> order;
-    order.reserve(n);
-    if (batch_size > 0) {
-      for (int bt = 0; bt < n / batch_size; ++bt) {
-        const int start = bt * batch_size, end = std::min(n, (bt + 1) * batch_size);
-        p->light_begin.push_back((int)order.size());
-        for (int i = start; i < end; ++i)
-          if (h_k[list[i]] <= light_cap / 2) order.push_back(list[i]);
-        p->light_n.push_back((int)order.size() - p->light_begin.back());
-        double lb = 0.0;   // 12 B (CSR offsets + b[v]) + 8 B per neighbour (id + block gather)
-        for (int i = p->light_begin.back(); i < (int)order.size(); ++i) lb += 12.0 + 8.0 * h_k[order[i]];
-        p->light_bytes.push_back(lb);
-        p->heavy_begin.push_back((int)order.size());
-        for (int i = start; i < end; ++i)
-          if (h_k[list[i]] > light_cap / 2) order.push_back(list[i]);
-        p->heavy_n.push_back((int)order.size() - p->heavy_begin.back());
-        p->max_batch = std::max(p->max_batch, end - start);
-      }
-    }
-    p->order.reserve(order.size());
-    if (!order.empty())
-      SBP_CUDA(SBP_COPY(p->order.p, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
-    auto& ref = *p;
-    plans[key] = std::move(p);
-    return ref;
-  }
-};
-
-// ------------------------------------------------------------------------------------------
-// Blockmodel
-// ------------------------------------------------------------------------------------------
-struct SbpBlockmodel {
-  int V = 0, B = 0, ld = 0;
-  const SbpGraph* graph = nullptr;   // the graph the blockmodel was created on (must outlive it)
-  DevBuf<int> b, M, MT, CS, CST, d_out, d_in, d;
-  DevBuf<int> prop, qr, qs, moved, n_moved;   // n_moved: two slots, alternating per batch
-  DevBuf<unsigned long long> last;           // (batch generation << 32 | last mover) per block
-  unsigned gen = 0;                          // batch generation
-  int nch = 0;
-  // row-hashed representation (B > dense_max_blocks)
-  bool sparse = false;
-  DevBuf<long long> rbase, cbase;
-  DevBuf<int> rmask, cmask, overflow, old_block;
-  DevBuf<int2> rslot, cslot;
-  DevBuf<int> csr_rptr, csr_ridx, csr_rval, csr_cptr, csr_cidx, csr_cval;   // sorted rows after a rebuild
-  float overall_entropy = 3.40282347e+38f;
-  int num_blocks_to_merge = 0;
-
-  BlockView view() {
-    BlockView v;
-    v.B = B;
-    v.sparse = sparse ? 1 : 0;
-    v.rbase = rbase.p;
-    v.rmask = rmask.p;
-    v.rslot = rslot.p;
-    v.cbase = cbase.p;
-    v.cmask = cmask.p;
-    v.cslot = cslot.p;
-    v.overflow = overflow.p;
-    v.ld = ld;
-    v.nch = nch;
-    v.CS = CS.p;
-    v.CST = CST.p;
-    v.b = b.p;
-    v.M = M.p;
-    v.MT = MT.p;
-    v.d_out = d_out.p;
-    v.d_in = d_in.p;
-    v.d = d.p;
-    return v;
-  }
-
-  void init_vertex_scratch(int nv) {
-    Context& c = Context::get();
-    V = nv;
-    b.reserve(V);
-    prop.reserve(V);
-    qr.reserve(V);
-    qs.reserve(V);
-    moved.reserve(V);
-    old_block.reserve(V);
-    n_moved.reserve(2);
-    overflow.reserve(1);
-    SBP_CUDA(cudaMemsetAsync(overflow.p, 0, sizeof(int), c.stream));
-    SBP_CUDA(cudaMemsetAsync(prop.p, 0xff, sizeof(int) * V, c.stream));
-    SBP_CUDA(cudaMemsetAsync(n_moved.p, 0, 2 * sizeof(int), c.stream));
-  }
-
-  void set_blocks(int nb) {
-    Context& c = Context::get();
-    B = nb;
-    sparse = B > g_dense_max_blocks;
-    ld = ((B + kChunk - 1) / kChunk) * kChunk;
-    nch = (B + kChunk - 1) / kChunk;
-    if (sparse) {
-      rbase.reserve(B);
-      cbase.reserve(B);
-      rmask.reserve(B);
-      cmask.reserve(B);
-    } else {
-      const size_t cells = (size_t)B * (size_t)ld;
-      M.reserve(cells);
-      MT.reserve(cells);
-      CS.reserve((size_t)B * nch);
-      CST.reserve((size_t)B * nch);
-    }
-    d_out.reserve(B);
-    d_in.reserve(B);
-    d.reserve(B);
-    last.reserve(B);
-    SBP_CUDA(cudaMemsetAsync(last.p, 0, sizeof(unsigned long long) * B, c.stream));
-  }
-};
 
 namespace sbpb {
 
@@ -462,7 +104,7 @@ static void rebuild_sparse(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_
 
 // Blockmodel::initialize_edge_counts (src/blockmodel/blockmodel.cpp:187-255).  recompute_d =
 // false keeps d (the reference's drifting block degree) when only the storage is rebuilt.
-static void rebuild(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_d = true) {
+void rebuild(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_d) {
   if (bm.sparse) {
     rebuild_sparse(bm, g, recompute_d);
     return;
@@ -489,7 +131,7 @@ static void rebuild(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_d = tru
 }
 
 // entropy::mdl (src/entropy.cpp:584-589).
-static double mdl(SbpBlockmodel& bm, const SbpGraph& g) {
+double mdl(SbpBlockmodel& bm, const SbpGraph& g) {
   Context& c = Context::get();
   const int grid = c.npartial;
   if (!bm.sparse && (long long)bm.B * bm.B <= 4LL * g.E) k_mdl_cells<<<grid, 256, 0, c.stream>>>(bm.view(), c.partial);
@@ -504,7 +146,7 @@ static double mdl(SbpBlockmodel& bm, const SbpGraph& g) {
 }
 
 // finetune::early_stop (src/finetune.cpp:144-162).
-static bool early_stop(int iteration, bool bracket, double initial_entropy, const std::vector<double>& deltas) {
+bool early_stop(int iteration, bool bracket, double initial_entropy, const std::vector<double>& deltas) {
   const size_t last = deltas.size() - 1;
   if (deltas[last] == 0.0) return true;
   if (iteration < 3) return false;
@@ -514,23 +156,18 @@ static bool early_stop(int iteration, bool bracket, double initial_entropy, cons
   return average < threshold;
 }
 
-struct MhResult {
-  long long visits = 0, moved = 0, accepted = 0;
-  double sum_dS = 0.0;
-};
-
 static int mh_cap(int max_k) {
   int cap = pow2_at_least(std::max(2 * max_k, kLightCap));
   if (cap > kMaxCap) throw Error(SBP_ERR_UNSUPPORTED, "vertex degree too large for the Metropolis-Hastings kernel");
   return cap;
 }
 
-static void set_smem_limit(const void* fn, size_t bytes) {
+void set_smem_limit(const void* fn, size_t bytes) {
   SBP_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
 // One sequential Metropolis-Hastings pass over verts (device list of n vertices).
-static MhResult mh_pass(SbpBlockmodel& bm, const SbpGraph& g, const int* verts, int n, int max_k, RngParams rng,
+MhResult mh_pass(SbpBlockmodel& bm, const SbpGraph& g, const int* verts, int n, int max_k, RngParams rng,
                         int sweep) {
   Context& c = Context::get();
   MhResult res;
@@ -565,13 +202,11 @@ static MhResult mh_pass(SbpBlockmodel& bm, const SbpGraph& g, const int* verts, 
 }
 
 // One asynchronous-Gibbs batch: evaluate every vertex of the batch, then apply the moves.
-static void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, int bt, RngParams rng,
+void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, int bt, RngParams rng,
                         int sweep) {
   Context& c = Context::get();
   const int nl = plan.light_n[bt], nh = plan.heavy_n[bt];
-  const int slot = bm.gen & 1;
-  int* n_cur = bm.n_moved.p + slot;
-  int* n_next = bm.n_moved.p + (slot ^ 1);
+  int* n_cur = bm.n_moved.p + (bm.gen & 1);
   if (nl > 0) {
     const size_t smem = (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps;
     set_smem_limit((const void*)k_gibbs_eval, smem);
@@ -602,7 +237,14 @@ static void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& p
         c.counters, g.heavy_cap, c.status);
     SBP_CHECK_LAUNCH();
   }
-  const int batch = nl + nh;
+  gibbs_apply(bm, g, nl + nh);
+}
+
+void gibbs_apply(SbpBlockmodel& bm, const SbpGraph& g, int batch) {
+  Context& c = Context::get();
+  const int slot = bm.gen & 1;
+  int* n_cur = bm.n_moved.p + slot;
+  int* n_next = bm.n_moved.p + (slot ^ 1);
   const unsigned gen = ++bm.gen;
   const int gw = grid_for((long long)batch * 32, 256, 64 * c.num_sms);
   k_apply_edges<<<gw, 256, 0, c.stream>>>(g.view(), bm.view(), bm.moved.p, n_cur, bm.prop.p, bm.qr.p, bm.qs.p,
@@ -631,20 +273,10 @@ static void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& p
   SBP_CHECK_LAUNCH();
 }
 
-struct ReplayDev {
-  DevBuf<uint4> buf;
-  long long records = 0;
-  void upload(const SbpReplay* r) {
-    if (!r || !r->words || r->records <= 0) return;
-    buf.reserve((size_t)r->records);
-    SBP_CUDA(SBP_COPY(buf.p, r->words, (size_t)r->records * sizeof(uint4), cudaMemcpyHostToDevice));
-    records = r->records;
-  }
-};
 
 // finetune::{metropolis_hastings, asynchronous_gibbs, hybrid_mcmc}.
-static void finetune(SbpBlockmodel& bm, SbpGraph& g, int algo, const SbpFinetuneOptions& opt, const SbpReplay* replay,
-                     SbpStats& st) {
+void finetune(SbpBlockmodel& bm, SbpGraph& g, int algo, const SbpFinetuneOptions& opt, const SbpReplay* replay,
+              SbpStats& st) {
   Context& c = Context::get();
   std::memset(&st, 0, sizeof st);
   st.num_blocks = bm.B;
@@ -1041,7 +673,7 @@ static void restore(SbpBlockmodel& bm, SbpGraph& g, const Snapshot& x) {
 }
 
 // sbp::stochastic_block_partition (src/sbp.cpp:61-98).
-static void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st) {
+void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st, const FinetuneStep* step) {
   Context& c = Context::get();
   std::memset(&st, 0, sizeof st);
   cudaEvent_t t0, t1;
@@ -1075,7 +707,8 @@ static void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st
     fo.call = call;
     fo.seed = opt.seed;
     SbpStats fs;
-    finetune(bm, g, algo, fo, nullptr, fs);
+    if (step) (*step)(bm, g, algo, fo, fs);
+    else finetune(bm, g, algo, fo, nullptr, fs);
     st.visits += fs.visits;
     st.proposals_moved += fs.proposals_moved;
     st.accepted += fs.accepted;

@@ -126,32 +126,6 @@ __global__ void k_mdl_final(const double* partial, int n, int V, long long E, in
 }
 
 // ------------------------------------------------------------------------------------------
-// Per-warp table carving from dynamic shared memory.
-// ------------------------------------------------------------------------------------------
-__device__ __forceinline__ WarpTable carve_table(int* base, int cap, int warp) {
-  int* p = base + (size_t)warp * (4 * cap + 32);
-  WarpTable t;
-  t.keys = p;
-  t.cout = p + cap;
-  t.cin = p + 2 * cap;
-  t.list = p + 3 * cap;
-  t.nlist = p + 4 * cap;
-  t.mask = cap - 1;
-  return t;
-}
-
-__device__ __forceinline__ void init_table(const WarpTable& t, int lane) {
-  const int cap = t.mask + 1;
-  for (int i = lane; i < cap; i += kWarp) {
-    t.keys[i] = -1;
-    t.cout[i] = 0;
-    t.cin[i] = 0;
-  }
-  if (lane == 0) *t.nlist = 0;
-  __syncwarp();
-}
-
-// ------------------------------------------------------------------------------------------
 // Asynchronous Gibbs: evaluate a list of vertices against the frozen state.  Accepted moves
 // go to prop[v] and the moved list; counters: [0] visits [1] proposals_moved [2] accepted.
 // ------------------------------------------------------------------------------------------

@@ -29,8 +29,14 @@ EXPORTED = [
     "sbp_graph_get_split", "sbp_graph_set_split", "sbp_blockmodel_create", "sbp_blockmodel_copy",
     "sbp_blockmodel_destroy", "sbp_blockmodel_num_blocks", "sbp_blockmodel_set_num_blocks_to_merge",
     "sbp_blockmodel_overall_entropy", "sbp_get_assignment", "sbp_get_block_matrix", "sbp_get_degrees", "sbp_mdl",
-    "sbp_evaluate_vertices", "sbp_move_vertex", "sbp_finetune", "sbp_merge_blocks", "sbp_partition", "sbp_mdl_device_noalloc",
+    "sbp_evaluate_vertices", "sbp_move_vertex", "sbp_finetune", "sbp_merge_blocks", "sbp_partition",
+    "sbp_mlp_create", "sbp_mlp_destroy", "sbp_mlp_get_params", "sbp_mlp_set_params", "sbp_mlp_forward",
+    "sbp_mlp_gradients", "sbp_mlp_train", "sbp_dataset_create", "sbp_dataset_destroy", "sbp_dataset_size",
+    "sbp_dataset_append", "sbp_dataset_read", "sbp_vertex_features", "sbp_learned_evaluate", "sbp_learned_q",
+    "sbp_collect_moves", "sbp_finetune_learned", "sbp_partition_learned", "sbp_mdl_device_noalloc",
 ]
+
+MLP_FEATURES, MLP_OUTPUTS, MLP_SLOTS, MLP_ESCAPE, MLP_PARAMS = 64, 16, 14, 14, 26896
 
 
 class SbpError(RuntimeError):
@@ -48,7 +54,8 @@ class Stats(ctypes.Structure):
                 ("sweeps", ctypes.c_int32), ("outer_iterations", ctypes.c_int32), ("num_blocks", ctypes.c_int32),
                 ("overflow_rebuilds", ctypes.c_int32), ("mdl", ctypes.c_double), ("mcmc_seconds", ctypes.c_double),
                 ("merge_seconds", ctypes.c_double), ("merge_proposals", ctypes.c_int64),
-                ("merge_avoided", ctypes.c_int64), ("total_seconds", ctypes.c_double)]
+                ("merge_avoided", ctypes.c_int64), ("total_seconds", ctypes.c_double),
+                ("learned_sweeps", ctypes.c_int32), ("_reserved", ctypes.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("_")}
@@ -72,6 +79,26 @@ class FinetuneOptions(ctypes.Structure):
 
 class MergeOptions(ctypes.Structure):
     _fields_ = [("approximate", ctypes.c_int32), ("call", ctypes.c_uint32), ("seed", ctypes.c_uint64)]
+
+
+class TrainOptions(ctypes.Structure):
+    _fields_ = [("epochs", ctypes.c_int32), ("batch", ctypes.c_int32), ("lr", ctypes.c_float),
+                ("_pad", ctypes.c_int32), ("seed", ctypes.c_uint64)]
+
+
+class TrainStats(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int64), ("first_loss", ctypes.c_double), ("last_loss", ctypes.c_double),
+                ("seconds", ctypes.c_double)]
+
+
+class LearnedOptions(ctypes.Structure):
+    _fields_ = [("epsilon", ctypes.c_float), ("fallback_acceptance", ctypes.c_float), ("stop_rule", ctypes.c_int32),
+                ("_pad", ctypes.c_int32)]
+
+
+class Trace(ctypes.Structure):
+    _fields_ = [("capacity", ctypes.c_int32), ("count", ctypes.c_int32), ("seconds", ctypes.POINTER(ctypes.c_double)),
+                ("mdl", ctypes.POINTER(ctypes.c_double))]
 
 
 _lib = None
@@ -122,6 +149,28 @@ def load(path=LIB_PATH):
     L.sbp_partition.argtypes = [vp, ctypes.POINTER(Options), _i32p, ctypes.POINTER(Stats)]
     L.sbp_mdl_device_noalloc.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, vp, vp, ctypes.c_int32, ctypes.c_int64,
                                          vp, vp]
+    f32p = ctypes.POINTER(ctypes.c_float)
+    L.sbp_mlp_create.argtypes = [ctypes.c_uint64, pp]
+    L.sbp_mlp_destroy.argtypes = [vp]
+    L.sbp_mlp_get_params.argtypes = [vp, f32p]
+    L.sbp_mlp_set_params.argtypes = [vp, f32p]
+    L.sbp_mlp_forward.argtypes = [vp, ctypes.c_int64, f32p, f32p]
+    L.sbp_mlp_gradients.argtypes = [vp, ctypes.c_int64, f32p, _i32p, _i32p, f32p, _f64p]
+    L.sbp_mlp_train.argtypes = [vp, vp, ctypes.POINTER(TrainOptions), ctypes.POINTER(TrainStats)]
+    L.sbp_dataset_create.argtypes = [ctypes.c_int64, pp]
+    L.sbp_dataset_destroy.argtypes = [vp]
+    L.sbp_dataset_size.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    L.sbp_dataset_append.argtypes = [vp, ctypes.c_int64, f32p, _i32p, _i32p]
+    L.sbp_dataset_read.argtypes = [vp, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(ctypes.c_uint16), _i32p, _i32p]
+    L.sbp_vertex_features.argtypes = [vp, vp, ctypes.c_int32, _i32p, f32p, _i32p, _i32p]
+    L.sbp_learned_evaluate.argtypes = [vp, vp, vp, ctypes.c_int32, _i32p, _u32p, ctypes.c_float, _i32p, _f64p, _f64p,
+                                       _f64p, _i32p]
+    L.sbp_learned_q.argtypes = [vp, vp, vp, ctypes.c_int32, _i32p, _i32p, ctypes.c_float, _f64p]
+    L.sbp_collect_moves.argtypes = [vp, vp, vp, ctypes.POINTER(FinetuneOptions), ctypes.POINTER(Stats)]
+    L.sbp_finetune_learned.argtypes = [vp, vp, ctypes.c_int32, ctypes.POINTER(FinetuneOptions), vp,
+                                       ctypes.POINTER(LearnedOptions), ctypes.POINTER(Trace), ctypes.POINTER(Stats)]
+    L.sbp_partition_learned.argtypes = [vp, ctypes.POINTER(Options), vp, ctypes.POINTER(LearnedOptions), _i32p,
+                                        ctypes.POINTER(Stats)]
     _lib = L
     return L
 
@@ -358,4 +407,167 @@ class sbp:
         out = np.zeros(graph.V, np.int32)
         st = Stats()
         _check(_lib.sbp_partition(graph.h, ctypes.byref(opt), _p(out), ctypes.byref(st)))
+        return out, st.as_dict()
+
+
+# ------------------------------------------------------------------------------------------
+# Learned proposal (no counterpart in the reference)
+# ------------------------------------------------------------------------------------------
+_f32p = ctypes.POINTER(ctypes.c_float)
+
+
+class Mlp:
+    """Proposal network 64 -> 128 -> 128 -> 16 (BF16 weights, FP32 accumulation, tensor cores)."""
+
+    def __init__(self, seed=0):
+        L = load()
+        self.h = ctypes.c_void_p()
+        _check(L.sbp_mlp_create(int(seed), ctypes.byref(self.h)))
+
+    def params(self):
+        out = np.zeros(MLP_PARAMS, np.float32)
+        _check(_lib.sbp_mlp_get_params(self.h, _p(out, _f32p)))
+        return out
+
+    def set_params(self, params):
+        arr = np.ascontiguousarray(params, dtype=np.float32)
+        if arr.size != MLP_PARAMS:
+            raise ValueError(f"expected {MLP_PARAMS} parameters")
+        _check(_lib.sbp_mlp_set_params(self.h, _p(arr, _f32p)))
+
+    def forward(self, features):
+        X = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, MLP_FEATURES)
+        out = np.zeros((len(X), MLP_OUTPUTS), np.float32)
+        _check(_lib.sbp_mlp_forward(self.h, len(X), _p(X, _f32p), _p(out, _f32p)))
+        return out
+
+    def gradients(self, features, target, nvalid):
+        X = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, MLP_FEATURES)
+        t = np.ascontiguousarray(target, dtype=np.int32)
+        nv = np.ascontiguousarray(nvalid, dtype=np.int32)
+        g = np.zeros(MLP_PARAMS, np.float32)
+        loss = ctypes.c_double()
+        _check(_lib.sbp_mlp_gradients(self.h, len(X), _p(X, _f32p), _p(t), _p(nv), _p(g, _f32p), ctypes.byref(loss)))
+        return g, loss.value
+
+    def train(self, dataset, epochs=1, batch=1024, lr=1e-3, seed=0):
+        opt = TrainOptions(int(epochs), int(batch), float(lr), 0, int(seed))
+        st = TrainStats()
+        _check(_lib.sbp_mlp_train(self.h, dataset.h, ctypes.byref(opt), ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def __del__(self):
+        if _lib is not None and getattr(self, "h", None):
+            _lib.sbp_mlp_destroy(self.h)
+            self.h = None
+
+
+class Dataset:
+    """Device-resident training samples (features, target slot, valid slots)."""
+
+    def __init__(self, capacity):
+        L = load()
+        self.h = ctypes.c_void_p()
+        _check(L.sbp_dataset_create(int(capacity), ctypes.byref(self.h)))
+
+    def __len__(self):
+        n = ctypes.c_int64()
+        _check(_lib.sbp_dataset_size(self.h, ctypes.byref(n)))
+        return n.value
+
+    def append(self, features, target, nvalid):
+        X = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, MLP_FEATURES)
+        t = np.ascontiguousarray(target, dtype=np.int32)
+        nv = np.ascontiguousarray(nvalid, dtype=np.int32)
+        _check(_lib.sbp_dataset_append(self.h, len(X), _p(X, _f32p), _p(t), _p(nv)))
+
+    def read(self, offset=0, n=None):
+        n = len(self) - offset if n is None else n
+        fb = np.zeros((n, MLP_FEATURES), np.uint16)
+        t = np.zeros(n, np.int32)
+        nv = np.zeros(n, np.int32)
+        _check(_lib.sbp_dataset_read(self.h, int(offset), int(n), fb.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)),
+                                     _p(t), _p(nv)))
+        X = (fb.astype(np.uint32) << 16).view(np.float32)
+        return X, t, nv
+
+    def __del__(self):
+        if _lib is not None and getattr(self, "h", None):
+            _lib.sbp_dataset_destroy(self.h)
+            self.h = None
+
+
+class learned:
+    @staticmethod
+    def vertex_features(blockmodel, vertices):
+        v = np.ascontiguousarray(vertices, dtype=np.int32)
+        n = len(v)
+        F = np.zeros((n, MLP_FEATURES), np.float32)
+        S = np.zeros((n, MLP_SLOTS), np.int32)
+        nv = np.zeros(n, np.int32)
+        _check(_lib.sbp_vertex_features(blockmodel.h, blockmodel.graph.h, n, _p(v), _p(F, _f32p), _p(S), _p(nv)))
+        return F, S, nv
+
+    @staticmethod
+    def evaluate(blockmodel, mlp, vertices, records, epsilon=0.05):
+        v = np.ascontiguousarray(vertices, dtype=np.int32)
+        rec = np.ascontiguousarray(records, dtype=np.uint32).reshape(-1, 4)
+        n = len(v)
+        s = np.zeros(n, np.int32)
+        qf = np.zeros(n, np.float64)
+        dS = np.zeros(n, np.float64)
+        H = np.zeros(n, np.float64)
+        acc = np.zeros(n, np.int32)
+        _check(_lib.sbp_learned_evaluate(blockmodel.h, blockmodel.graph.h, mlp.h, n, _p(v), _p(rec, _u32p),
+                                         float(epsilon), _p(s), _p(qf, _f64p), _p(dS, _f64p), _p(H, _f64p), _p(acc)))
+        return s, qf, dS, H, acc
+
+    @staticmethod
+    def q(blockmodel, mlp, vertices, blocks, epsilon=0.05):
+        v = np.ascontiguousarray(vertices, dtype=np.int32)
+        b = np.ascontiguousarray(blocks, dtype=np.int32)
+        out = np.zeros(len(v), np.float64)
+        _check(_lib.sbp_learned_q(blockmodel.h, blockmodel.graph.h, mlp.h, len(v), _p(v), _p(b), float(epsilon),
+                                  _p(out, _f64p)))
+        return out
+
+    @staticmethod
+    def collect_moves(blockmodel, dataset, batches=10, sweeps=10, seed=0, call=0):
+        opt = FinetuneOptions(int(batches), 0, int(sweeps), int(call), int(seed))
+        st = Stats()
+        _check(_lib.sbp_collect_moves(blockmodel.h, blockmodel.graph.h, dataset.h, ctypes.byref(opt),
+                                      ctypes.byref(st)))
+        return st.as_dict()
+
+    @staticmethod
+    def finetune(blockmodel, mlp=None, algorithm="async_gibbs", batches=10, bracket=False, seed=0, call=0,
+                 max_sweeps=0, epsilon=0.05, fallback_acceptance=0.0, stop_rule=0, trace=True):
+        algo = ALGORITHMS[algorithm] if isinstance(algorithm, str) else int(algorithm)
+        opt = FinetuneOptions(int(batches), int(bool(bracket)), int(max_sweeps), int(call), int(seed))
+        lo = LearnedOptions(float(epsilon), float(fallback_acceptance), int(stop_rule), 0)
+        cap = 128
+        secs = np.zeros(cap, np.float64)
+        mdls = np.zeros(cap, np.float64)
+        tr = Trace(cap, 0, secs.ctypes.data_as(_f64p), mdls.ctypes.data_as(_f64p)) if trace else None
+        st = Stats()
+        _check(_lib.sbp_finetune_learned(blockmodel.h, blockmodel.graph.h, algo, ctypes.byref(opt),
+                                         mlp.h if mlp is not None else None, ctypes.byref(lo),
+                                         ctypes.byref(tr) if tr is not None else None, ctypes.byref(st)))
+        out = st.as_dict()
+        if tr is not None:
+            out["trace_seconds"] = secs[:tr.count].copy()
+            out["trace_mdl"] = mdls[:tr.count].copy()
+        return out
+
+    @staticmethod
+    def stochastic_block_partition(graph, mlp=None, algorithm="async_gibbs", batches=10, approximate=True,
+                                   asynciterations=2**31 - 1, seed=0, epsilon=0.05, fallback_acceptance=0.0,
+                                   stop_rule=1):
+        algo = ALGORITHMS[algorithm] if isinstance(algorithm, str) else int(algorithm)
+        opt = Options(algo, int(batches), int(bool(approximate)), int(asynciterations), int(seed))
+        lo = LearnedOptions(float(epsilon), float(fallback_acceptance), int(stop_rule), 0)
+        out = np.zeros(graph.V, np.int32)
+        st = Stats()
+        _check(_lib.sbp_partition_learned(graph.h, ctypes.byref(opt), mlp.h if mlp is not None else None,
+                                          ctypes.byref(lo), _p(out), ctypes.byref(st)))
         return out, st.as_dict()

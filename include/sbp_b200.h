@@ -62,6 +62,8 @@ typedef struct {
     int64_t merge_proposals;   /* block-merge proposals drawn */
     int64_t merge_avoided;     /* proposals skipped as duplicates */
     double total_seconds;      /* partition only: device-clock time of the whole call */
+    int32_t learned_sweeps;    /* sweeps that used the learned proposal (sbp_finetune_learned) */
+    int32_t _reserved;
 } SbpStats;
 
 /* Launch and timing counters of this library (process-wide). */
@@ -202,6 +204,105 @@ SbpStatus sbp_partition(const SbpGraph *graph, const SbpOptions *opt, int32_t *o
 SbpStatus sbp_mdl_device_noalloc(const int32_t *d_matrix, int32_t num_blocks, int64_t ld, const int32_t *d_degrees_out,
                                  const int32_t *d_degrees_in, int32_t num_vertices, int64_t num_edges,
                                  double *d_result, void *stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Learned proposal (no counterpart in the reference).  A network maps 64 features of a vertex
+ * and its 14 candidate neighbour blocks to 15 logits (14 candidates + "uniformly random
+ * block"); the draw mixes them with weight (1 - epsilon) with a uniform block (epsilon), and the
+ * Hastings factor q(r | state after the move) / q(s | state) is computed exactly from the same
+ * network, so the MCMC keeps the plain method's stationary distribution.  Network: 64 -> 128
+ * -> 128 -> 16 with ReLU, BF16 weights and activations, FP32 accumulation on the tensor cores.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct SbpMlp SbpMlp;           /* network weights and optimiser state (device) */
+typedef struct SbpDataset SbpDataset;   /* training samples (device) */
+
+#define SBP_MLP_FEATURES 64
+#define SBP_MLP_OUTPUTS 16
+#define SBP_MLP_SLOTS 14
+#define SBP_MLP_ESCAPE 14
+/* parameter vector: W1[128][64], b1[128], W2[128][128], b2[128], W3[16][128], b3[16] */
+#define SBP_MLP_PARAMS 26896
+
+typedef struct {
+    int32_t epochs;
+    int32_t batch;             /* rows per Adam step */
+    float lr;
+    int32_t _pad;
+    uint64_t seed;             /* shuffling */
+} SbpTrainOptions;
+
+typedef struct {
+    int64_t steps;
+    double first_loss;         /* mean cross-entropy of the first epoch */
+    double last_loss;          /* of the last epoch */
+    double seconds;
+} SbpTrainStats;
+
+typedef struct {
+    float epsilon;             /* uniform weight of the proposal mixture, (0, 1] */
+    float fallback_acceptance; /* a learned sweep accepting less than this fraction of its visits
+                                  switches the rest of the call to the plain proposal */
+    int32_t stop_rule;         /* 0: early stop of sbp_finetune for the algorithm; 1: per-sweep MDL
+                                  changes (the metropolis_hastings rule) */
+    int32_t _pad;
+} SbpLearnedOptions;
+
+typedef struct {               /* MDL after every sweep (caller-owned arrays of `capacity`) */
+    int32_t capacity;
+    int32_t count;
+    double *seconds;           /* host wall time since the call started, stream synchronised */
+    double *mdl;
+} SbpTrace;
+
+SbpStatus sbp_mlp_create(uint64_t seed, SbpMlp **out);
+SbpStatus sbp_mlp_destroy(SbpMlp *mlp);
+SbpStatus sbp_mlp_get_params(const SbpMlp *mlp, float *params);
+SbpStatus sbp_mlp_set_params(SbpMlp *mlp, const float *params);   /* also resets the optimiser */
+/* logits[n][16] of features[n][64] (host buffers; features are rounded to BF16). */
+SbpStatus sbp_mlp_forward(const SbpMlp *mlp, int64_t n, const float *features, float *logits);
+/* Gradient of the mean masked cross-entropy over the rows with target >= 0 (targets: a
+ * candidate slot < nvalid, or 14 = escape; -1 = row ignored).  Slots >= nvalid and logit 15
+ * are masked.  grads[SBP_MLP_PARAMS] in parameter-vector order. */
+SbpStatus sbp_mlp_gradients(const SbpMlp *mlp, int64_t n, const float *features, const int32_t *target,
+                            const int32_t *nvalid, float *grads, double *mean_loss);
+/* Adam on the samples of `data` (shuffled each epoch). */
+SbpStatus sbp_mlp_train(SbpMlp *mlp, const SbpDataset *data, const SbpTrainOptions *opt, SbpTrainStats *stats);
+
+SbpStatus sbp_dataset_create(int64_t capacity, SbpDataset **out);
+SbpStatus sbp_dataset_destroy(SbpDataset *data);
+SbpStatus sbp_dataset_size(const SbpDataset *data, int64_t *out);
+SbpStatus sbp_dataset_append(SbpDataset *data, int64_t n, const float *features, const int32_t *target,
+                             const int32_t *nvalid);
+SbpStatus sbp_dataset_read(const SbpDataset *data, int64_t offset, int64_t n, uint16_t *features_bf16,
+                           int32_t *target, int32_t *nvalid);
+
+/* Features of vertices against the blockmodel: features[n][64] (BF16 values), the candidate
+ * blocks slots[n][14] (-1 past nvalid) and nvalid[n]. */
+SbpStatus sbp_vertex_features(const SbpBlockmodel *bm, const SbpGraph *g, int32_t n, const int32_t *vertices,
+                              float *features, int32_t *slots, int32_t *nvalid);
+/* One learned-proposal evaluation of distinct vertices against the frozen blockmodel with
+ * caller records (4 words per vertex: x_choice, x_uniform_block, u_hi, u_lo): proposal[n],
+ * q_forward[n] (0 when the proposal is the current block), delta_mdl[n], hastings[n],
+ * accepted[n].  The blockmodel is not changed. */
+SbpStatus sbp_learned_evaluate(const SbpBlockmodel *bm, const SbpGraph *g, const SbpMlp *mlp, int32_t n,
+                               const int32_t *vertices, const uint32_t *records, float epsilon, int32_t *proposal,
+                               double *q_forward, double *delta_mdl, double *hastings, int32_t *accepted);
+/* q(block | vertex, blockmodel) of the learned proposal for given (vertex, block) pairs. */
+SbpStatus sbp_learned_q(const SbpBlockmodel *bm, const SbpGraph *g, const SbpMlp *mlp, int32_t n, const int32_t *vertices,
+                        const int32_t *blocks, float epsilon, double *q);
+/* Plain asynchronous-Gibbs sweeps (opt->max_sweeps of them) that append the features and chosen
+ * candidate slot of every accepted move to `data` (samples past its capacity are dropped). */
+SbpStatus sbp_collect_moves(SbpBlockmodel *bm, const SbpGraph *g, SbpDataset *data, const SbpFinetuneOptions *opt,
+                            SbpStats *stats);
+/* Asynchronous-Gibbs or hybrid finetune with the learned proposal (mlp != NULL) or the plain one
+ * (mlp == NULL), same sweeps as sbp_finetune, early stop per lopt->stop_rule; optional per-sweep
+ * MDL trace. */
+SbpStatus sbp_finetune_learned(SbpBlockmodel *bm, const SbpGraph *g, int32_t algorithm, const SbpFinetuneOptions *opt,
+                               const SbpMlp *mlp, const SbpLearnedOptions *lopt, SbpTrace *trace, SbpStats *stats);
+/* sbp_partition with the learned proposal in every asynchronous-Gibbs / hybrid finetune
+ * (mlp == NULL: the plain proposal, with lopt->stop_rule). */
+SbpStatus sbp_partition_learned(const SbpGraph *g, const SbpOptions *opt, const SbpMlp *mlp,
+                                const SbpLearnedOptions *lopt, int32_t *out_assignment, SbpStats *stats);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,256 @@
+"""GPU tests of the learned proposal: the tensor-core network against the numpy oracle (forward
+and gradients), the features, the proposal and its exact Hastings factor, training, the
+learned finetune and partition, and the fallback to the plain proposal."""
+import numpy as np
+import pytest
+
+from conftest import random_assignment, random_graph, random_records
+import learned_oracle as LO
+
+pytestmark = pytest.mark.gpu
+
+
+def random_params(seed, scale=1.0):
+    rng = np.random.default_rng(seed)
+    p = np.zeros(LO.PARAMS, np.float32)
+    p[LO.OFF_W1:LO.OFF_B1] = rng.normal(0, scale * np.sqrt(2 / 64), 128 * 64)
+    p[LO.OFF_B1:LO.OFF_W2] = rng.normal(0, 0.1, 128)
+    p[LO.OFF_W2:LO.OFF_B2] = rng.normal(0, scale * np.sqrt(2 / 128), 128 * 128)
+    p[LO.OFF_B2:LO.OFF_W3] = rng.normal(0, 0.1, 128)
+    p[LO.OFF_W3:LO.OFF_B3] = rng.normal(0, scale * np.sqrt(1 / 128), 16 * 128)
+    p[LO.OFF_B3:] = rng.normal(0, 0.5, 16)
+    return p
+
+
+@pytest.fixture
+def mlp(S):
+    m = S.Mlp(seed=1)
+    m.set_params(random_params(11))
+    return m
+
+
+@pytest.mark.parametrize("n", [1, 300, 19021])   # one row, a partial tile, more tiles than SMs
+def test_mlp_forward_matches_oracle(S, mlp, n):
+    X = np.random.default_rng(n).random((n, 64)).astype(np.float32)
+    got = mlp.forward(X)
+    ref = LO.forward(mlp.params(), X)
+    assert np.isfinite(got).all()
+    err = np.abs(got - ref)
+    # FP32 accumulation on the tensor cores vs exact accumulation here; an occasional hidden
+    # activation rounds to the neighbouring BF16 value
+    assert err.max() <= 2e-2 * max(1.0, np.abs(ref).max()), err.max()
+    assert np.median(err) <= 1e-3
+
+
+def test_mlp_gradients_match_oracle(S, mlp):
+    rng = np.random.default_rng(4)
+    n = 700
+    X = rng.random((n, 64)).astype(np.float32)
+    nv = rng.integers(0, 15, n).astype(np.int32)
+    t = np.array([rng.integers(0, k) if k > 0 and rng.random() < 0.8 else LO.ESCAPE for k in nv], np.int32)
+    t[rng.random(n) < 0.05] = -1
+    g, loss = mlp.gradients(X, t, nv)
+    ref, rloss = LO.gradients(mlp.params(), X, t, nv)
+    assert loss == pytest.approx(rloss, rel=2e-3)
+    parts = {"W1": (LO.OFF_W1, LO.OFF_B1), "b1": (LO.OFF_B1, LO.OFF_W2), "W2": (LO.OFF_W2, LO.OFF_B2),
+             "b2": (LO.OFF_B2, LO.OFF_W3), "W3": (LO.OFF_W3, LO.OFF_B3), "b3": (LO.OFF_B3, LO.PARAMS)}
+    for name, (a, b) in parts.items():
+        x, y = g[a:b].astype(np.float64), ref[a:b]
+        rel = np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-30)
+        cos = np.dot(x, y) / max(np.linalg.norm(x) * np.linalg.norm(y), 1e-30)
+        assert rel < 2e-2 and cos > 0.9995, (name, rel, cos)
+
+
+def test_mlp_gradients_reject_masked_targets(S, mlp):
+    X = np.zeros((2, 64), np.float32)
+    with pytest.raises(S.SbpError):
+        mlp.gradients(X, np.array([3, 0], np.int32), np.array([2, 1], np.int32))
+
+
+def test_training_learns_a_rule(S):
+    """Target = the slot with the most out-edges: the network must learn it from samples."""
+    rng = np.random.default_rng(8)
+    n = 24000
+    nv = rng.integers(1, 15, n).astype(np.int32)
+    X = np.zeros((n, 64), np.float32)
+    for j in range(14):
+        on = j < nv
+        X[on, 4 * j] = rng.random(on.sum())
+        X[on, 4 * j + 1] = rng.random(on.sum())
+    X[:, 63] = 1.0
+    t = np.array([np.argmax(X[i, 0:4 * k:4]) for i, k in enumerate(nv)], np.int32)
+    ds = S.Dataset(n)
+    ds.append(X[:20000], t[:20000], nv[:20000])
+    assert len(ds) == 20000
+    Xr, tr, nr = ds.read(0, 5)
+    assert np.array_equal(tr, t[:5]) and np.array_equal(nr, nv[:5])
+    assert np.array_equal(Xr, LO.bf16(X[:5]))
+    m = S.Mlp(seed=2)
+    st = m.train(ds, epochs=6, batch=512, lr=3e-3, seed=1)
+    assert st["steps"] == 6 * ((20000 + 511) // 512)
+    assert st["last_loss"] < 0.5 * st["first_loss"]
+    L = m.forward(X[20000:])
+    mask = LO.mask(nv[20000:])
+    pred = np.argmax(np.where(mask, L, -np.inf), axis=1)
+    assert (pred == t[20000:]).mean() > 0.8
+
+
+def oracle_state(bm, g_orc):
+    b = bm.block_assignment()
+    d_out, d_in = LO.block_degrees(g_orc, b, bm.B)
+    return b, d_out, d_in
+
+
+def test_vertex_features_match_oracle(S):
+    V, s, d, _ = random_graph(500, 8, 21, kmin=4, kmax=60)
+    g = S.Graph(V, s, d)
+    bm = S.Blockmodel(g, 25, random_assignment(V, 25, 21))
+    go = LO.Graph(V, s, d)
+    b, d_out, d_in = oracle_state(bm, go)
+    verts = np.arange(V, dtype=np.int32)
+    F, slots, nv = S.learned.vertex_features(bm, verts)
+    mism = 0
+    for v in range(V):
+        f, sl, *_ = LO.vertex_features(go, b, bm.B, d_out, d_in, v)
+        assert nv[v] == len(sl)
+        assert slots[v, :nv[v]].tolist() == [x[0] for x in sl]
+        assert (slots[v, nv[v]:] == -1).all()
+        diff = F[v] != f
+        # log1pf here and on the device may differ in the last FP32 bit, and BF16 rounding of a
+        # value on a tie boundary then differs by one BF16 step
+        assert np.all(np.abs(F[v][diff] - f[diff]) <= 2.0**-7 * np.abs(f[diff]) + 1e-12)
+        mism += int(diff.sum())
+    assert mism <= 0.002 * V * 64
+
+
+def test_learned_proposal_and_hastings_match_oracle(S, O, mlp):
+    V, s, d, _ = random_graph(800, 10, 31, kmin=4, kmax=50)
+    g = S.Graph(V, s, d)
+    B = 30
+    a = random_assignment(V, B, 31)
+    bm = S.Blockmodel(g, B, a)
+    obm = O.Blockmodel(O.Graph(V, s, d), B, a)
+    go = LO.Graph(V, s, d)
+    b, d_out, d_in = oracle_state(bm, go)
+    verts = np.arange(V, dtype=np.int32)
+    rec = random_records(V, 5)
+    eps = 0.05
+    prop, qf, dS, H, acc = S.learned.evaluate(bm, mlp, verts, rec, epsilon=eps)
+    F, slots, nv = S.learned.vertex_features(bm, verts)
+    L1 = mlp.forward(F)
+    moved = 0
+    for v in range(V):
+        _, sl, r, k_out, k_in, self = LO.vertex_features(go, b, B, d_out, d_in, v)
+        want = LO.draw(L1[v], nv[v], sl, rec[v, 0], rec[v, 1], eps, B)
+        assert prop[v] == want, v
+        if want == r:
+            assert qf[v] == 0.0 and not acc[v]
+            continue
+        moved += 1
+        slot_s = next((j for j, x in enumerate(sl) if x[0] == want), -1)
+        assert qf[v] == pytest.approx(LO.q_of(L1[v], nv[v], slot_s, eps, B), rel=1e-12)
+        F2 = LO.reverse_features(F[v], sl, r, want, k_out, k_in, self, B, d_out, d_in, go.E)
+        L2 = mlp.forward(F2[None, :])[0]
+        slot_r = next((j for j, x in enumerate(sl) if x[0] == r), -1)
+        assert H[v] == pytest.approx(LO.q_of(L2, nv[v], slot_r, eps, B) / qf[v], rel=1e-12)
+        assert dS[v] == pytest.approx(obm.delta_mdl_move(v, int(want))[0], rel=1e-9, abs=1e-9)
+        u = (int(rec[v, 2]) * 2.0**21 + (int(rec[v, 3]) >> 11)) * 2.0**-53
+        ap = min(1.0, np.exp(-3.0 * dS[v]) * H[v])
+        if abs(u - ap) > 1e-9:
+            assert bool(acc[v]) == (u <= ap), v
+    assert moved > V // 3
+
+
+def test_hastings_factor_is_the_exact_reverse_probability(S, mlp):
+    """H = q(r | v, state after the move) / q(s | v, state), with q(r | ...) computed by the
+    forward path on the moved blockmodel, bit for bit."""
+    V, s, d, _ = random_graph(400, 8, 41, kmin=4, kmax=40)
+    g = S.Graph(V, s, d)
+    B = 16
+    a = random_assignment(V, B, 41)
+    bm = S.Blockmodel(g, B, a)
+    rng = np.random.default_rng(2)
+    verts = rng.choice(V, 40, replace=False).astype(np.int32)
+    prop, qf, dS, H, acc = S.learned.evaluate(bm, mlp, verts, random_records(40, 9), epsilon=0.1)
+    checked = 0
+    for i, v in enumerate(verts):
+        r = int(a[v])
+        if prop[i] == r:
+            continue
+        assert S.learned.q(bm, mlp, [v], [prop[i]], epsilon=0.1)[0] == qf[i]
+        moved = bm.copy()
+        moved.move_vertex(int(v), int(prop[i]))
+        q_back = S.learned.q(moved, mlp, [v], [r], epsilon=0.1)[0]
+        assert H[i] == q_back / qf[i]
+        checked += 1
+    assert checked >= 15
+
+
+def test_learned_finetune_keeps_the_blockmodel_consistent(S, O, mlp):
+    V, s, d, _ = random_graph(3000, 12, 51, kmin=4, kmax=60)
+    g = S.Graph(V, s, d)
+    B = 40
+    bm = S.Blockmodel(g, B, random_assignment(V, B, 51))
+    st = S.learned.finetune(bm, mlp, algorithm="async_gibbs", batches=5, seed=3, max_sweeps=6)
+    assert st["learned_sweeps"] == st["sweeps"] == len(st["trace_mdl"])
+    assert st["accepted"] > 0
+    ob = O.Blockmodel(O.Graph(V, s, d), B, bm.block_assignment())
+    assert np.array_equal(bm.blockmatrix(), ob.matrix())
+    do, di, _ = bm.degrees_all()
+    odo, odi, _ = ob.degrees()
+    assert np.array_equal(do, odo) and np.array_equal(di, odi)
+    assert st["mdl"] == pytest.approx(ob.mdl(), rel=1e-6)
+    # hybrid: high-degree vertices keep plain Metropolis-Hastings
+    st2 = S.learned.finetune(bm, mlp, algorithm="hybrid_mcmc", batches=5, seed=4, max_sweeps=3, stop_rule=1)
+    assert 1 <= st2["sweeps"] <= 3
+    with pytest.raises(S.SbpError):
+        S.learned.finetune(bm, mlp, algorithm="metropolis_hastings")
+
+
+def test_fallback_to_the_plain_proposal(S, mlp):
+    V, s, d, _ = random_graph(1500, 8, 61)
+    g = S.Graph(V, s, d)
+    bm = S.Blockmodel(g, 20, random_assignment(V, 20, 61))
+    st = S.learned.finetune(bm, mlp, batches=4, seed=1, max_sweeps=5, fallback_acceptance=1.01)
+    assert st["learned_sweeps"] == 1 and st["sweeps"] >= 2
+
+
+def test_plain_mode_of_the_learned_finetune_is_the_plain_finetune(S):
+    """mlp = None and the asynchronous-Gibbs stop rule: the same chain as sbp_finetune."""
+    V, s, d, _ = random_graph(1200, 8, 81)
+    g = S.Graph(V, s, d)
+    a = random_assignment(V, 30, 81)
+    bm1, bm2 = S.Blockmodel(g, 30, a), S.Blockmodel(g, 30, a)
+    st1 = S.finetune.asynchronous_gibbs(bm1, batches=5, seed=7, call=2, max_sweeps=8)
+    st2 = S.learned.finetune(bm2, None, batches=5, seed=7, call=2, max_sweeps=8)
+    assert np.array_equal(bm1.block_assignment(), bm2.block_assignment())
+    assert st1["sweeps"] == st2["sweeps"] and st1["accepted"] == st2["accepted"]
+    assert st2["learned_sweeps"] == 0
+
+
+def test_collect_moves_records_the_accepted_moves(S):
+    V, s, d, truth = random_graph(4000, 10, 71, kmin=6, kmax=60, w=0.8)
+    g = S.Graph(V, s, d)
+    rng = np.random.default_rng(71)
+    a = truth.astype(np.int32).copy()
+    flip = rng.random(V) < 0.3
+    a[flip] = rng.integers(0, 10, flip.sum())
+    bm = S.Blockmodel(g, 10, a)
+    ds = S.Dataset(10**6)
+    st = S.learned.collect_moves(bm, ds, batches=10, sweeps=3, seed=5)
+    assert len(ds) == st["accepted"] > 0
+    X, t, nv = ds.read()
+    assert ((t >= 0) & (t <= LO.ESCAPE)).all()
+    assert ((t < nv) | (t == LO.ESCAPE)).all()
+    assert (X[:, 63] == 1.0).all()
+
+
+def test_learned_partition_recovers_the_planted_blocks(S, O):
+    V, s, d, truth = random_graph(3000, 8, 91, kmin=8, kmax=60, w=0.8, alpha=10.0)
+    g = S.Graph(V, s, d)
+    m = S.Mlp(seed=3)
+    out, st = S.learned.stochastic_block_partition(g, m, batches=10, seed=2)
+    assert st["learned_sweeps"] > 0 and st["num_blocks"] >= 2
+    assert O.nmi(out, truth) > 0.9
+    ob = O.Blockmodel(O.Graph(V, s, d), int(out.max()) + 1, out)
+    assert st["mdl"] == pytest.approx(ob.mdl(), rel=1e-5)
