@@ -474,8 +474,8 @@ static void carry_out_advanced(int B, int to_merge, const std::vector<int>& rptr
   block_map = gm.name;
 }
 
-static void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& opt, const SbpReplay* replay,
-                         int* best_out, double* dS_out, SbpStats& st) {
+void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& opt, const SbpReplay* replay,
+                  int* best_out, double* dS_out, SbpStats& st) {
   Context& c = Context::get();
   const int B = bm.B;
   if (B < 2) throw Error(SBP_ERR_INVALID_ARGUMENT, "block merge needs at least two blocks");
@@ -602,56 +602,7 @@ static void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& 
   st.num_blocks = bm.B;
 }
 
-// ------------------------------------------------------------------------------------------
-// Golden-section triplet over B (src/blockmodel/blockmodel_triplet.cpp:3-100) holding
-// host copies of the assignment; a restored blockmodel is rebuilt on the device.
-// ------------------------------------------------------------------------------------------
-struct Snapshot {
-  bool empty = true;
-  std::vector<int> b;
-  int B = 0;
-  float entropy = 0.f;
-};
-
-struct Triplet {
-  Snapshot s[3];
-  bool optimal = false;
-  void update(const Snapshot& x) {
-    int index;
-    if (s[1].empty) index = 1;
-    else if (x.entropy <= s[1].entropy) {
-      const int old_index = (s[1].B > x.B) ? 0 : 2;
-      s[old_index] = s[1];
-      index = 1;
-    } else index = (s[1].B > x.B) ? 2 : 0;
-    s[index] = x;
-  }
-  // returns the snapshot to continue from and its num_blocks_to_merge
-  Snapshot next(const Snapshot& old, int* to_merge) {
-    update(old);
-    if (s[2].empty) {
-      Snapshot r = s[1];
-      *to_merge = (int)(r.B * 0.5);
-      if (*to_merge == 0) optimal = true;
-      return r;
-    }
-    if ((!s[0].empty && s[0].B - s[2].B == 2) || (s[0].empty && s[1].B - s[2].B == 1)) optimal = true;
-    if (optimal) {
-      *to_merge = 0;
-      return s[1];
-    }
-    int index;
-    if (s[0].empty && s[1].B > s[2].B) index = 1;
-    else if ((s[0].B - s[1].B) >= (s[1].B - s[2].B)) index = 0;
-    else index = 1;
-    int next_b = s[index + 1].B;
-    next_b += (int)((s[index].B - s[index + 1].B) * 0.618);
-    *to_merge = s[index].B - next_b;
-    return s[index];
-  }
-};
-
-static Snapshot snapshot(SbpBlockmodel& bm) {
+Snapshot snapshot(SbpBlockmodel& bm) {
   Context& c = Context::get();
   Snapshot x;
   x.empty = false;
@@ -663,7 +614,7 @@ static Snapshot snapshot(SbpBlockmodel& bm) {
   return x;
 }
 
-static void restore(SbpBlockmodel& bm, SbpGraph& g, const Snapshot& x) {
+void restore(SbpBlockmodel& bm, SbpGraph& g, const Snapshot& x) {
   Context& c = Context::get();
   SBP_CUDA(SBP_COPY_ASYNC(bm.b.p, x.b.data(), bm.V * sizeof(int), cudaMemcpyHostToDevice, c.stream));
   bm.set_blocks(x.B);
@@ -672,15 +623,12 @@ static void restore(SbpBlockmodel& bm, SbpGraph& g, const Snapshot& x) {
   c.sync();
 }
 
-// sbp::stochastic_block_partition (src/sbp.cpp:61-98).
-void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st, const FinetuneStep* step) {
+// sbp::stochastic_block_partition (src/sbp.cpp:61-98) as a per-graph state machine: the
+// single-graph driver below and the batched driver (sbp_batched.cu) run the same steps.
+void partition_begin(PartitionState& ps, SbpGraph& g) {
   Context& c = Context::get();
-  std::memset(&st, 0, sizeof st);
-  cudaEvent_t t0, t1;
-  SBP_CUDA(cudaEventCreate(&t0));
-  SBP_CUDA(cudaEventCreate(&t1));
-  SBP_CUDA(cudaEventRecord(t0, c.stream));
-  SbpBlockmodel bm;
+  std::memset(&ps.st, 0, sizeof ps.st);
+  SbpBlockmodel& bm = ps.bm;
   bm.init_vertex_scratch(g.V);
   std::vector<int> ident(g.V);
   std::iota(ident.begin(), ident.end(), 0);
@@ -689,45 +637,65 @@ void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st, const
   bm.num_blocks_to_merge = (int)(g.V * 0.5f);
   rebuild(bm, g);
   c.sync();
-  Triplet t;
-  float iteration = 0;
-  uint32_t call = 0;
-  while (!t.optimal) {
-    SbpMergeOptions mo;
-    mo.approximate = opt.approximate;
-    mo.call = call;
-    mo.seed = opt.seed;
-    merge_blocks(bm, g, mo, nullptr, nullptr, nullptr, st);
-    int algo = opt.algorithm;
-    if (algo == SBP_ASYNC_GIBBS && !(iteration < (float)opt.asynciterations)) algo = SBP_METROPOLIS_HASTINGS;
-    SbpFinetuneOptions fo;
-    fo.batches = opt.batches;
-    fo.bracket_established = !t.s[2].empty;
-    fo.max_sweeps = 0;
-    fo.call = call;
-    fo.seed = opt.seed;
-    SbpStats fs;
-    if (step) (*step)(bm, g, algo, fo, fs);
-    else finetune(bm, g, algo, fo, nullptr, fs);
-    st.visits += fs.visits;
-    st.proposals_moved += fs.proposals_moved;
-    st.accepted += fs.accepted;
-    st.sweeps += fs.sweeps;
-    st.mcmc_seconds += fs.mcmc_seconds;
-    ++iteration;
-    ++call;
-    st.outer_iterations++;
-    int to_merge = 0;
-    const Snapshot nxt = t.next(snapshot(bm), &to_merge);
-    if (t.optimal) {
-      std::memcpy(out, nxt.b.data(), g.V * sizeof(int));
-      st.mdl = nxt.entropy;
-      st.num_blocks = nxt.B;
-      break;
-    }
-    restore(bm, g, nxt);
-    bm.num_blocks_to_merge = to_merge;
+}
+
+int partition_merge(PartitionState& ps, SbpGraph& g, const SbpOptions& opt, SbpFinetuneOptions* fo) {
+  SbpMergeOptions mo;
+  mo.approximate = opt.approximate;
+  mo.call = ps.call;
+  mo.seed = opt.seed;
+  merge_blocks(ps.bm, g, mo, nullptr, nullptr, nullptr, ps.st);
+  int algo = opt.algorithm;
+  if (algo == SBP_ASYNC_GIBBS && !(ps.iteration < (float)opt.asynciterations)) algo = SBP_METROPOLIS_HASTINGS;
+  fo->batches = opt.batches;
+  fo->bracket_established = !ps.t.s[2].empty;
+  fo->max_sweeps = 0;
+  fo->call = ps.call;
+  fo->seed = opt.seed;
+  return algo;
+}
+
+void partition_finish_round(PartitionState& ps, SbpGraph& g, const SbpStats& fs, int* out) {
+  SbpStats& st = ps.st;
+  st.visits += fs.visits;
+  st.proposals_moved += fs.proposals_moved;
+  st.accepted += fs.accepted;
+  st.sweeps += fs.sweeps;
+  st.mcmc_seconds += fs.mcmc_seconds;
+  st.learned_sweeps += fs.learned_sweeps;
+  ++ps.iteration;
+  ++ps.call;
+  st.outer_iterations++;
+  int to_merge = 0;
+  const Snapshot nxt = ps.t.next(snapshot(ps.bm), &to_merge);
+  if (ps.t.optimal) {
+    std::memcpy(out, nxt.b.data(), g.V * sizeof(int));
+    st.mdl = nxt.entropy;
+    st.num_blocks = nxt.B;
+    ps.done = true;
+    return;
   }
+  restore(ps.bm, g, nxt);
+  ps.bm.num_blocks_to_merge = to_merge;
+}
+
+void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st, const FinetuneStep* step) {
+  Context& c = Context::get();
+  cudaEvent_t t0, t1;
+  SBP_CUDA(cudaEventCreate(&t0));
+  SBP_CUDA(cudaEventCreate(&t1));
+  SBP_CUDA(cudaEventRecord(t0, c.stream));
+  PartitionState ps;
+  partition_begin(ps, g);
+  while (!ps.done) {
+    SbpFinetuneOptions fo;
+    const int algo = partition_merge(ps, g, opt, &fo);
+    SbpStats fs;
+    if (step) (*step)(ps.bm, g, algo, fo, fs);
+    else finetune(ps.bm, g, algo, fo, nullptr, fs);
+    partition_finish_round(ps, g, fs, out);
+  }
+  st = ps.st;
   SBP_CUDA(cudaEventRecord(t1, c.stream));
   c.sync();
   float ms = 0.f;

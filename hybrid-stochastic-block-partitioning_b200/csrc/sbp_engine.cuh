@@ -382,7 +382,66 @@ struct ReplayDev {
   }
 };
 
-// Engine steps shared with the learned proposal (defined in sbp_engine.cu).
+// ------------------------------------------------------------------------------------------
+// Golden-section triplet over B (src/blockmodel/blockmodel_triplet.cpp:3-100) holding
+// host copies of the assignment; a restored blockmodel is rebuilt on the device.
+// ------------------------------------------------------------------------------------------
+struct Snapshot {
+  bool empty = true;
+  std::vector<int> b;
+  int B = 0;
+  float entropy = 0.f;
+};
+
+struct Triplet {
+  Snapshot s[3];
+  bool optimal = false;
+  void update(const Snapshot& x) {
+    int index;
+    if (s[1].empty) index = 1;
+    else if (x.entropy <= s[1].entropy) {
+      const int old_index = (s[1].B > x.B) ? 0 : 2;
+      s[old_index] = s[1];
+      index = 1;
+    } else index = (s[1].B > x.B) ? 2 : 0;
+    s[index] = x;
+  }
+  // returns the snapshot to continue from and its num_blocks_to_merge
+  Snapshot next(const Snapshot& old, int* to_merge) {
+    update(old);
+    if (s[2].empty) {
+      Snapshot r = s[1];
+      *to_merge = (int)(r.B * 0.5);
+      if (*to_merge == 0) optimal = true;
+      return r;
+    }
+    if ((!s[0].empty && s[0].B - s[2].B == 2) || (s[0].empty && s[1].B - s[2].B == 1)) optimal = true;
+    if (optimal) {
+      *to_merge = 0;
+      return s[1];
+    }
+    int index;
+    if (s[0].empty && s[1].B > s[2].B) index = 1;
+    else if ((s[0].B - s[1].B) >= (s[1].B - s[2].B)) index = 0;
+    else index = 1;
+    int next_b = s[index + 1].B;
+    next_b += (int)((s[index].B - s[index + 1].B) * 0.618);
+    *to_merge = s[index].B - next_b;
+    return s[index];
+  }
+};
+
+// One graph's partition in progress (sbp::stochastic_block_partition's loop state).
+struct PartitionState {
+  SbpBlockmodel bm;
+  Triplet t;
+  float iteration = 0;
+  uint32_t call = 0;
+  SbpStats st;
+  bool done = false;
+};
+
+// Engine steps shared by the translation units (defined in sbp_engine.cu).
 void rebuild(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_d = true);
 double mdl(SbpBlockmodel& bm, const SbpGraph& g);
 bool early_stop(int iteration, bool bracket, double initial_entropy, const std::vector<double>& deltas);
@@ -398,6 +457,17 @@ void finetune(SbpBlockmodel& bm, SbpGraph& g, int algo, const SbpFinetuneOptions
 using FinetuneStep = std::function<void(SbpBlockmodel&, SbpGraph&, int, const SbpFinetuneOptions&, SbpStats&)>;
 // sbp::stochastic_block_partition; `step` = nullptr runs the plain finetune.
 void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st, const FinetuneStep* step = nullptr);
+// The partition loop's steps: start at B = V; merge step of the next round (returns the
+// round's finetune algorithm and fills its options); statistics and golden-section step after
+// the round's finetune (writes `out` and sets done when the search ends).
+void partition_begin(PartitionState& ps, SbpGraph& g);
+int partition_merge(PartitionState& ps, SbpGraph& g, const SbpOptions& opt, SbpFinetuneOptions* fo);
+void partition_finish_round(PartitionState& ps, SbpGraph& g, const SbpStats& fs, int* out);
+// block_merge::merge_blocks; best_out / dS_out optional.
+void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& opt, const SbpReplay* replay,
+                  int* best_out, double* dS_out, SbpStats& st);
+Snapshot snapshot(SbpBlockmodel& bm);
+void restore(SbpBlockmodel& bm, SbpGraph& g, const Snapshot& x);
 // One sequential Metropolis-Hastings pass over a device list of n vertices.
 MhResult mh_pass(SbpBlockmodel& bm, const SbpGraph& g, const int* verts, int n, int max_k, RngParams rng, int sweep);
 

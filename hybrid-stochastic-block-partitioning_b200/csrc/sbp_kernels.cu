@@ -10,6 +10,7 @@
 //   k_merge_propose    merge_blocks proposal scoring          src/block_merge.cpp:278-301, 335-368
 //   k_relabel          carry-out relabel                      src/blockmodel/blockmodel.cpp:71-76
 #include "sbp_kernels.cuh"
+#include "sbp_steps.cuh"
 
 namespace sbpb {
 
@@ -69,60 +70,25 @@ __global__ void k_rebuild_degrees(BlockView bm) {
 // MDL: L = sum_cells g(M) - sum g(d_out) - sum g(d_in);
 // mdl = E h(B^2/E) + V log B - L.  Deterministic two-pass reduction.
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ double block_sum(double v, double* red) {
-  v = warp_sum(v);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) red[w] = v;
-  __syncthreads();
-  double t = 0.0;
-  if (threadIdx.x == 0)
-    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
-  __syncthreads();
-  return t;
-}
 
 __global__ void k_mdl_cells(BlockView bm, double* partial) {
   __shared__ double red[32];
-  double acc = 0.0;
-  const long long BB = (long long)bm.B * bm.B;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < BB; i += stride) {
-    const int row = (int)(i / bm.B), col = (int)(i - (long long)row * bm.B);
-    const int m = bm.M[(size_t)row * bm.ld + col];
-    if (m > 0) acc += xlogx((double)m);
-  }
-  for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < bm.B; x += stride)
-    acc -= xlogx((double)bm.d_out[x]) + xlogx((double)bm.d_in[x]);
-  const double t = block_sum(acc, red);
+  const double t = mdl_cells_part(bm, blockIdx.x, gridDim.x, red);
   if (threadIdx.x == 0) partial[blockIdx.x] = t;
 }
 
 // Edge form: sum_cells M log M = sum over edges of log M[b_src, b_dst]; one thread per edge.
 __global__ void k_mdl_edges(GraphView g, BlockView bm, const int* __restrict__ out_src, double* partial) {
   __shared__ double red[32];
-  double acc = 0.0;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < g.E; e += stride) {
-    const int bv = bm.b[__ldg(out_src + e)], bu = bm.b[__ldg(g.out_idx + e)];
-    acc += log((double)bm_get(bm, bv, bu));
-  }
-  for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < bm.B; x += stride)
-    acc -= xlogx((double)bm.d_out[x]) + xlogx((double)bm.d_in[x]);
-  const double t = block_sum(acc, red);
+  const double t = mdl_edges_part(g, bm, out_src, blockIdx.x, gridDim.x, red);
   if (threadIdx.x == 0) partial[blockIdx.x] = t;
 }
 
 // Sum of the partials in a fixed order (one CTA of 256 threads) and the MDL formula.
 __global__ void k_mdl_final(const double* partial, int n, int V, long long E, int B, double* out) {
   __shared__ double red[32];
-  double acc = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
-  const double L = block_sum(acc, red);
-  if (threadIdx.x == 0) {
-    const double x = pow((double)B, 2) / (double)E;
-    const double h = ((1 + x) * log(1 + x)) - (x * log(x));
-    *out = ((double)E * h) + ((double)V * log((double)B)) - L;
-  }
+  const double v = mdl_final_value(partial, n, V, E, B, red);
+  if (threadIdx.x == 0) *out = v;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -161,19 +127,6 @@ __global__ void __launch_bounds__(256, 2) k_gibbs_eval(GraphView g, BlockView bm
   }
 }
 
-// M[row,col] += delta with the transpose kept in step: dense cells and both chunk sums, or the
-// two hashed rows (atomic).
-__device__ __forceinline__ void cell_add(const BlockView& bm, int row, int col, int delta) {
-  if (bm.sparse) {
-    hashed_add(bm.rbase, bm.rmask, bm.rslot, row, col, delta, bm.overflow);
-    hashed_add(bm.cbase, bm.cmask, bm.cslot, col, row, delta, bm.overflow);
-    return;
-  }
-  atomicAdd(bm.M + (size_t)row * bm.ld + col, delta);
-  atomicAdd(bm.MT + (size_t)col * bm.ld + row, delta);
-  chunk_add(bm.CS, bm.nch, row, col, delta);
-  chunk_add(bm.CST, bm.nch, col, row, delta);
-}
 
 // Same for a dense cell owned by one thread (plain update of M/MT, atomic chunk sums, which
 // lanes share); hashed rows are always updated atomically (lanes share their slots).
@@ -203,54 +156,7 @@ __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, 
   const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const int n = *n_moved;
-  for (int i = wid; i < n; i += nw) {
-    const int v = moved_list[i];
-    const int r = bm.b[v], s = prop[v];
-    const int self = g.self[v];
-    int cr = 0, cs = 0;
-    const int o0 = g.out_ptr[v], o1 = g.out_ptr[v + 1];
-    for (int e = o0 + lane; e < o1; e += kWarp) {
-      const int u = __ldg(g.out_idx + e);
-      if (u == v) continue;
-      const int bo = bm.b[u], pu = prop[u];
-      const int bn = pu >= 0 ? pu : bo;
-      cell_add(bm, r, bo, -1);
-      cell_add(bm, s, bn, 1);
-      const int ba = (pu >= 0 && u < v) ? pu : bo;
-      cr += (ba == r);
-      cs += (ba == s);
-    }
-    const int i0 = g.in_ptr[v], i1 = g.in_ptr[v + 1];
-    for (int e = i0 + lane; e < i1; e += kWarp) {
-      const int u = __ldg(g.in_idx + e);
-      const int bo = bm.b[u], pu = prop[u];
-      if (pu < 0) {
-        cell_add(bm, bo, r, -1);
-        cell_add(bm, bo, s, 1);
-      }
-      const int ba = (pu >= 0 && u < v) ? pu : bo;
-      cr += (ba == r);
-      cs += (ba == s);
-    }
-    cr = warp_sum_int(cr);
-    cs = warp_sum_int(cs);
-    if (lane == 0) {
-      if (self) {
-        cell_add(bm, r, r, -1);
-        cell_add(bm, s, s, 1);
-      }
-      const int k_out = o1 - o0, k_in_self = (i1 - i0) + self;
-      atomicAdd(bm.d_out + r, -k_out);
-      atomicAdd(bm.d_out + s, k_out);
-      atomicAdd(bm.d_in + r, -k_in_self);
-      atomicAdd(bm.d_in + s, k_in_self);
-      qr[v] = -(cr + self);
-      qs[v] = cs + self;
-      const unsigned long long key = ((unsigned long long)gen << 32) | (unsigned)v;
-      atomicMax(last + r, key);
-      atomicMax(last + s, key);
-    }
-  }
+  for (int i = wid; i < n; i += nw) apply_moved_vertex(g, bm, moved_list[i], prop, qr, qs, last, gen, lane);
 }
 
 // d[r], d[s] from the last mover of each block, then the new assignment; clears the other
@@ -259,15 +165,8 @@ __global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n
                                const int* qr, const int* qs, const unsigned long long* last, unsigned gen) {
   const int n = *n_moved;
   if (blockIdx.x == 0 && threadIdx.x == 0) *next_n_moved = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int v = moved_list[i];
-    const int r = bm.b[v], s = prop[v];
-    const unsigned long long key = ((unsigned long long)gen << 32) | (unsigned)v;
-    if (last[r] == key) bm.d[r] = bm.d_out[r] + bm.d_in[r] - bm_get(bm, r, r) - qr[v];
-    if (last[s] == key) bm.d[s] = bm.d_out[s] + bm.d_in[s] - bm_get(bm, s, s) - qs[v];
-    bm.b[v] = s;
-    prop[v] = -1;
-  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    finish_moved_vertex(bm, moved_list[i], prop, qr, qs, last, gen);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -1,0 +1,143 @@
+// Per-element steps of the finetune apply and of entropy::mdl, shared by the single-graph
+// kernels (sbp_kernels.cu) and the batched persistent kernel (sbp_batched.cu) so both run the
+// same arithmetic in the same order.
+#pragma once
+#include "sbp_device.cuh"
+
+namespace sbpb {
+
+// Sum over the CTA's threads (deterministic: warp butterflies, then warps in order); the total
+// is returned to thread 0.
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+  __syncthreads();
+  return t;
+}
+
+// M[row,col] += delta with the transpose kept in step: dense cells and both chunk sums, or the
+// two hashed rows (atomic).
+__device__ __forceinline__ void cell_add(const BlockView& bm, int row, int col, int delta) {
+  if (bm.sparse) {
+    hashed_add(bm.rbase, bm.rmask, bm.rslot, row, col, delta, bm.overflow);
+    hashed_add(bm.cbase, bm.cmask, bm.cslot, col, row, delta, bm.overflow);
+    return;
+  }
+  atomicAdd(bm.M + (size_t)row * bm.ld + col, delta);
+  atomicAdd(bm.MT + (size_t)col * bm.ld + row, delta);
+  chunk_add(bm.CS, bm.nch, row, col, delta);
+  chunk_add(bm.CST, bm.nch, col, row, delta);
+}
+
+// Apply of one accepted move v: r -> prop[v] (Blockmodel::move_vertex, src/blockmodel/
+// blockmodel.cpp:344-360, for a batch of simultaneous moves): M, MT and the chunk sums by edge,
+// d_out / d_in, the quirk terms qr/qs of d[r], d[s] (the neighbours that are counted in the
+// reference's sequential apply) and the batch's last mover of r and s.  One warp per vertex.
+__device__ __forceinline__ void apply_moved_vertex(const GraphView& g, const BlockView& bm, int v, const int* prop,
+                                                   int* qr, int* qs, unsigned long long* last, unsigned gen,
+                                                   int lane) {
+  const int r = bm.b[v], s = prop[v];
+  const int self = g.self[v];
+  int cr = 0, cs = 0;
+  const int o0 = g.out_ptr[v], o1 = g.out_ptr[v + 1];
+  for (int e = o0 + lane; e < o1; e += kWarp) {
+    const int u = __ldg(g.out_idx + e);
+    if (u == v) continue;
+    const int bo = bm.b[u], pu = prop[u];
+    const int bn = pu >= 0 ? pu : bo;
+    cell_add(bm, r, bo, -1);
+    cell_add(bm, s, bn, 1);
+    const int ba = (pu >= 0 && u < v) ? pu : bo;
+    cr += (ba == r);
+    cs += (ba == s);
+  }
+  const int i0 = g.in_ptr[v], i1 = g.in_ptr[v + 1];
+  for (int e = i0 + lane; e < i1; e += kWarp) {
+    const int u = __ldg(g.in_idx + e);
+    const int bo = bm.b[u], pu = prop[u];
+    if (pu < 0) {
+      cell_add(bm, bo, r, -1);
+      cell_add(bm, bo, s, 1);
+    }
+    const int ba = (pu >= 0 && u < v) ? pu : bo;
+    cr += (ba == r);
+    cs += (ba == s);
+  }
+  cr = warp_sum_int(cr);
+  cs = warp_sum_int(cs);
+  if (lane == 0) {
+    if (self) {
+      cell_add(bm, r, r, -1);
+      cell_add(bm, s, s, 1);
+    }
+    const int k_out = o1 - o0, k_in_self = (i1 - i0) + self;
+    atomicAdd(bm.d_out + r, -k_out);
+    atomicAdd(bm.d_out + s, k_out);
+    atomicAdd(bm.d_in + r, -k_in_self);
+    atomicAdd(bm.d_in + s, k_in_self);
+    qr[v] = -(cr + self);
+    qs[v] = cs + self;
+    const unsigned long long key = ((unsigned long long)gen << 32) | (unsigned)v;
+    atomicMax(last + r, key);
+    atomicMax(last + s, key);
+  }
+}
+
+// d[r], d[s] from the last mover of each block, then the new assignment of v.
+__device__ __forceinline__ void finish_moved_vertex(const BlockView& bm, int v, int* prop, const int* qr,
+                                                    const int* qs, const unsigned long long* last, unsigned gen) {
+  const int r = bm.b[v], s = prop[v];
+  const unsigned long long key = ((unsigned long long)gen << 32) | (unsigned)v;
+  if (last[r] == key) bm.d[r] = bm.d_out[r] + bm.d_in[r] - bm_get(bm, r, r) - qr[v];
+  if (last[s] == key) bm.d[s] = bm.d_out[s] + bm.d_in[s] - bm_get(bm, s, s) - qs[v];
+  bm.b[v] = s;
+  prop[v] = -1;
+}
+
+// MDL: L = sum_cells g(M) - sum g(d_out) - sum g(d_in); mdl = E h(B^2/E) + V log B - L.
+// Deterministic two-pass reduction: partial cta of ncta CTAs of 256 threads (elements in
+// grid-stride order), then the partials summed in a fixed order.
+__device__ __forceinline__ double mdl_cells_part(const BlockView& bm, int cta, int ncta, double* red) {
+  double acc = 0.0;
+  const long long BB = (long long)bm.B * bm.B;
+  const long long stride = (long long)ncta * blockDim.x;
+  for (long long i = (long long)cta * blockDim.x + threadIdx.x; i < BB; i += stride) {
+    const int row = (int)(i / bm.B), col = (int)(i - (long long)row * bm.B);
+    const int m = bm.M[(size_t)row * bm.ld + col];
+    if (m > 0) acc += xlogx((double)m);
+  }
+  for (long long x = (long long)cta * blockDim.x + threadIdx.x; x < bm.B; x += stride)
+    acc -= xlogx((double)bm.d_out[x]) + xlogx((double)bm.d_in[x]);
+  return block_sum(acc, red);
+}
+
+// Edge form: sum_cells M log M = sum over edges of log M[b_src, b_dst].
+__device__ __forceinline__ double mdl_edges_part(const GraphView& g, const BlockView& bm, const int* out_src, int cta,
+                                                 int ncta, double* red) {
+  double acc = 0.0;
+  const long long stride = (long long)ncta * blockDim.x;
+  for (long long e = (long long)cta * blockDim.x + threadIdx.x; e < g.E; e += stride) {
+    const int bv = bm.b[__ldg(out_src + e)], bu = bm.b[__ldg(g.out_idx + e)];
+    acc += log((double)bm_get(bm, bv, bu));
+  }
+  for (long long x = (long long)cta * blockDim.x + threadIdx.x; x < bm.B; x += stride)
+    acc -= xlogx((double)bm.d_out[x]) + xlogx((double)bm.d_in[x]);
+  return block_sum(acc, red);
+}
+
+__device__ __forceinline__ double mdl_final_value(const double* partial, int n, int V, long long E, int B,
+                                                  double* red) {
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+  const double L = block_sum(acc, red);
+  const double x = pow((double)B, 2) / (double)E;
+  const double h = ((1 + x) * log(1 + x)) - (x * log(x));
+  return ((double)E * h) + ((double)V * log((double)B)) - L;
+}
+
+}  // namespace sbpb

@@ -33,7 +33,8 @@ EXPORTED = [
     "sbp_mlp_create", "sbp_mlp_destroy", "sbp_mlp_get_params", "sbp_mlp_set_params", "sbp_mlp_forward",
     "sbp_mlp_gradients", "sbp_mlp_train", "sbp_dataset_create", "sbp_dataset_destroy", "sbp_dataset_size",
     "sbp_dataset_append", "sbp_dataset_read", "sbp_vertex_features", "sbp_learned_evaluate", "sbp_learned_q",
-    "sbp_collect_moves", "sbp_finetune_learned", "sbp_partition_learned", "sbp_mdl_device_noalloc",
+    "sbp_collect_moves", "sbp_finetune_learned", "sbp_partition_learned", "sbp_partition_batched",
+    "sbp_batched_reset_tuning", "sbp_mdl_device_noalloc",
 ]
 
 MLP_FEATURES, MLP_OUTPUTS, MLP_SLOTS, MLP_ESCAPE, MLP_PARAMS = 64, 16, 14, 14, 26896
@@ -94,6 +95,13 @@ class TrainStats(ctypes.Structure):
 class LearnedOptions(ctypes.Structure):
     _fields_ = [("epsilon", ctypes.c_float), ("fallback_acceptance", ctypes.c_float), ("stop_rule", ctypes.c_int32),
                 ("_pad", ctypes.c_int32)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("rounds", ctypes.c_int32), ("batched_finetunes", ctypes.c_int32),
+                ("fallback_finetunes", ctypes.c_int32), ("sweep_launches", ctypes.c_int32), ("chunk", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32), ("tuned", ctypes.c_int32), ("candidates", ctypes.c_int32),
+                ("candidate_ms", ctypes.c_double * 8), ("sweep_seconds", ctypes.c_double), ("seconds", ctypes.c_double)]
 
 
 class Trace(ctypes.Structure):
@@ -171,6 +179,9 @@ def load(path=LIB_PATH):
                                        ctypes.POINTER(LearnedOptions), ctypes.POINTER(Trace), ctypes.POINTER(Stats)]
     L.sbp_partition_learned.argtypes = [vp, ctypes.POINTER(Options), vp, ctypes.POINTER(LearnedOptions), _i32p,
                                         ctypes.POINTER(Stats)]
+    L.sbp_partition_batched.argtypes = [ctypes.c_int32, ctypes.POINTER(vp), ctypes.POINTER(Options),
+                                        ctypes.POINTER(_i32p), ctypes.POINTER(Stats), ctypes.POINTER(BatchInfo)]
+    L.sbp_batched_reset_tuning.argtypes = []
     _lib = L
     return L
 
@@ -571,3 +582,32 @@ class learned:
         _check(_lib.sbp_partition_learned(graph.h, ctypes.byref(opt), mlp.h if mlp is not None else None,
                                           ctypes.byref(lo), _p(out), ctypes.byref(st)))
         return out, st.as_dict()
+
+
+# ------------------------------------------------------------------------------------------
+# Batched partitioning (no counterpart in the reference)
+# ------------------------------------------------------------------------------------------
+class batched:
+    @staticmethod
+    def stochastic_block_partition(graphs, algorithm="async_gibbs", batches=10, approximate=True,
+                                   asynciterations=2**31 - 1, seed=0):
+        """Partition every graph (each exactly as sbp.stochastic_block_partition would) with the
+        finetunes of all graphs in one persistent launch per sweep.  Returns (assignments, stats,
+        info)."""
+        load()
+        algo = ALGORITHMS[algorithm] if isinstance(algorithm, str) else int(algorithm)
+        opt = Options(algo, int(batches), int(bool(approximate)), int(asynciterations), int(seed))
+        n = len(graphs)
+        outs = [np.zeros(g.V, np.int32) for g in graphs]
+        hs = (ctypes.c_void_p * n)(*[g.h.value if isinstance(g.h, ctypes.c_void_p) else g.h for g in graphs])
+        ps = (_i32p * n)(*[_p(o) for o in outs])
+        st = (Stats * n)()
+        info = BatchInfo()
+        _check(_lib.sbp_partition_batched(n, hs, ctypes.byref(opt), ps, st, ctypes.byref(info)))
+        inf = {k: getattr(info, k) for k, _ in info._fields_}
+        inf["candidate_ms"] = list(info.candidate_ms)[:info.candidates]
+        return outs, [x.as_dict() for x in st], inf
+
+    @staticmethod
+    def reset_tuning():
+        _check(load().sbp_batched_reset_tuning())

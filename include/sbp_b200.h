@@ -304,6 +304,35 @@ SbpStatus sbp_finetune_learned(SbpBlockmodel *bm, const SbpGraph *g, int32_t alg
 SbpStatus sbp_partition_learned(const SbpGraph *g, const SbpOptions *opt, const SbpMlp *mlp,
                                 const SbpLearnedOptions *lopt, int32_t *out_assignment, SbpStats *stats);
 
+/* ------------------------------------------------------------------------------------------
+ * Batched partitioning (no counterpart in the reference, which partitions one graph per run):
+ * n graphs of uneven sizes, each partitioned exactly as by sbp_partition (same options, same
+ * result), with the asynchronous-Gibbs finetune of all graphs in one persistent kernel launch
+ * per sweep (per-graph work queues, replayed as a CUDA graph) and work-item shapes chosen by
+ * an autotuner that times candidates on the first sweeps of a workload.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct {
+    int32_t rounds;             /* lockstep rounds (merge + finetune of every unfinished graph) */
+    int32_t batched_finetunes;  /* finetune calls run by the persistent kernel */
+    int32_t fallback_finetunes; /* finetune calls run by the single-graph path (row-hashed storage,
+                                   Metropolis-Hastings or hybrid rounds, very large degrees) */
+    int32_t sweep_launches;     /* persistent-kernel launches (one per sweep of a round) */
+    int32_t chunk;              /* light vertices per evaluation work item (autotuned) */
+    int32_t ctas_per_sm;        /* persistent CTAs per SM (autotuned) */
+    int32_t tuned;              /* 1: this call ran the autotuner; 0: it used an earlier choice */
+    int32_t candidates;         /* candidates timed */
+    double candidate_ms[8];     /* their sweep times, per graph swept */
+    double sweep_seconds;       /* device time of the persistent sweep launches */
+    double seconds;             /* device-clock time of the whole call */
+} SbpBatchInfo;
+
+/* graphs[n] -> out_assignments[i][V_i]; stats[i] per graph (optional; total_seconds is the
+ * batch's time); info optional.  The graphs must not be used by another call meanwhile. */
+SbpStatus sbp_partition_batched(int32_t n, const SbpGraph *const *graphs, const SbpOptions *opt,
+                                int32_t *const *out_assignments, SbpStats *stats, SbpBatchInfo *info);
+/* Forget the autotuner's choices (the next batched call tunes again). */
+SbpStatus sbp_batched_reset_tuning(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,90 @@
+"""GPU tests of the batched partitioner: every graph of a batch gets exactly the partition that
+sbp_partition gives it alone (assignment, block count, MDL and counters), whatever shapes the
+autotuner picks, including rounds that fall back to the single-graph finetune."""
+import numpy as np
+import pytest
+
+from conftest import random_graph
+
+pytestmark = pytest.mark.gpu
+
+
+def uneven_graphs(seed, sizes):
+    out = []
+    for i, V in enumerate(sizes):
+        K = int(round(1.2 * V ** 0.35))
+        out.append(random_graph(V, K, seed + i, kmin=6, kmax=60, w=0.55 + 0.05 * (i % 7), alpha=3.0))
+    return out
+
+
+def with_hub(V, s, d, hub=0, extra=400, seed=0):
+    """Add in-edges to one vertex so that it is evaluated on the heavy path."""
+    rng = np.random.default_rng(seed)
+    src = rng.choice(np.arange(1, V), size=min(extra, V - 1), replace=False).astype(np.int32)
+    return V, np.concatenate([s, src]), np.concatenate([d, np.full(len(src), hub, np.int32)])
+
+
+def single(S, g, seed):
+    return S.sbp.stochastic_block_partition(g, algorithm="async_gibbs", batches=10, seed=seed)
+
+
+def assert_same(out_b, st_b, out_s, st_s):
+    assert np.array_equal(out_b, out_s)
+    for k in ("num_blocks", "mdl", "sweeps", "visits", "accepted", "proposals_moved", "outer_iterations"):
+        assert st_b[k] == st_s[k], k
+
+
+def test_batched_equals_single_partitions(S):
+    specs = uneven_graphs(100, [300, 1700, 800, 2500, 450, 1200])
+    graphs = []
+    for i, (V, s, d, _) in enumerate(specs):
+        if i == 3:
+            V, s, d = with_hub(V, s, d, seed=i)
+        graphs.append(S.Graph(V, s, d))
+    S.batched.reset_tuning()
+    outs, stats, info = S.batched.stochastic_block_partition(graphs, batches=10, seed=5)
+    assert info["tuned"] == 1 and info["candidates"] >= 1
+    assert info["batched_finetunes"] > 0 and info["sweep_launches"] > 0
+    for g, out, st in zip(graphs, outs, stats):
+        out_s, st_s = single(S, g, 5)
+        assert_same(out, st, out_s, st_s)
+    # the tuned shape is reused, and the answer does not change
+    outs2, stats2, info2 = S.batched.stochastic_block_partition(graphs, batches=10, seed=5)
+    assert info2["tuned"] == 0
+    for a, b in zip(outs, outs2):
+        assert np.array_equal(a, b)
+
+
+def test_batched_fallback_rounds_are_identical(S):
+    """Small dense limit: the first rounds use row-hashed storage and the single-graph finetune."""
+    specs = uneven_graphs(200, [900, 400, 1500])
+    graphs = [S.Graph(V, s, d) for V, s, d, _ in specs]
+    S.set_option("dense_max_blocks", 64)
+    try:
+        outs, stats, info = S.batched.stochastic_block_partition(graphs, batches=8, seed=11)
+        assert info["fallback_finetunes"] > 0 and info["batched_finetunes"] > 0
+        for g, out, st in zip(graphs, outs, stats):
+            out_s, st_s = S.sbp.stochastic_block_partition(g, algorithm="async_gibbs", batches=8, seed=11)
+            assert_same(out, st, out_s, st_s)
+    finally:
+        S.set_option("dense_max_blocks", 16384)
+
+
+def test_batched_other_algorithms_fall_back(S):
+    specs = uneven_graphs(300, [400, 700])
+    graphs = [S.Graph(V, s, d) for V, s, d, _ in specs]
+    outs, stats, info = S.batched.stochastic_block_partition(graphs, algorithm="hybrid_mcmc", batches=5, seed=3)
+    assert info["batched_finetunes"] == 0 and info["fallback_finetunes"] > 0
+    for g, out, st in zip(graphs, outs, stats):
+        out_s, st_s = S.sbp.stochastic_block_partition(g, algorithm="hybrid_mcmc", batches=5, seed=3)
+        assert_same(out, st, out_s, st_s)
+
+
+def test_batched_single_graph_and_errors(S):
+    V, s, d, _ = random_graph(600, 5, 9)
+    g = S.Graph(V, s, d)
+    outs, stats, _ = S.batched.stochastic_block_partition([g], seed=2)
+    out_s, st_s = single(S, g, 2)
+    assert_same(outs[0], stats[0], out_s, st_s)
+    with pytest.raises(S.SbpError):
+        S.batched.stochastic_block_partition([g], batches=0)
