@@ -46,6 +46,7 @@ def args_parse():
     ap.add_argument("--algorithm", default="async_gibbs")
     ap.add_argument("--batches", type=int, default=10)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain comparison")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched 64-graph comparison")
     return ap.parse_args()
 
 
@@ -191,6 +192,30 @@ def learned_vs_plain(S, O, dcsbm, np):
             **runs, "time_ratio_plain_over_learned": p["seconds"] / l["seconds"],
             "mdl_gap_learned_vs_plain": (l["mdl"] - p["mdl"]) / p["mdl"],
             "target": "learned reaches the plain final MDL within 0.5 % in at least 2x less wall time"}
+
+
+def batched_vs_sequential(S, dcsbm, np):
+    """64 directed DC-SBM graphs of uneven size (V log-uniform in 1k-50k, blocks round(1.2 V^0.35),
+    gamma 2.5 on [10,100], within-block fraction uniform in 0.5-0.9, seeds 3..66): one batched
+    call (persistent sweep launches, autotuned shapes; the first call tunes, the second is
+    timed) against the same 64 partitions one after another.  Device clock."""
+    specs = [dcsbm.generate(**dcsbm.batched_config(i)) for i in range(64)]
+    graphs = [S.Graph(V, s, d) for V, s, d, _ in specs]
+    S.batched.stochastic_block_partition(graphs, batches=10, seed=1)
+    outs, stats, info = S.batched.stochastic_block_partition(graphs, batches=10, seed=1)
+    seq = [S.sbp.stochastic_block_partition(g, batches=10, seed=1) for g in graphs]
+    seq_s = sum(st["total_seconds"] for _, st in seq)
+    identical = sum(int(np.array_equal(o, so) and st["mdl"] == sst["mdl"])
+                    for o, st, (so, sst) in zip(outs, stats, seq))
+    visits = sum(st["visits"] for st in stats)
+    return {"workload": "64 directed DC-SBM graphs, V log-uniform in [1000, 50000], seeds 3-66",
+            "vertices": int(sum(g.V for g in graphs)), "edges": int(sum(g.E for g in graphs)),
+            "batched_seconds": info["seconds"], "sweep_kernel_seconds": info["sweep_seconds"],
+            "sequential_seconds": seq_s, "speedup": seq_s / info["seconds"],
+            "visits_per_s_batched": visits / info["seconds"], "identical_partitions": identical,
+            "sweep_launches": info["sweep_launches"], "batched_finetunes": info["batched_finetunes"],
+            "fallback_finetunes": info["fallback_finetunes"],
+            "autotuned": {"chunk": info["chunk"], "ctas_per_sm": info["ctas_per_sm"]}}
 
 
 def main():
@@ -368,6 +393,8 @@ def main():
             line["cpu_baseline"] = base
         if world == 1 and not a.no_learned:
             line["learned_vs_plain"] = learned_vs_plain(S, O, dcsbm, np)
+        if world == 1 and not a.no_batched:
+            line["batched"] = batched_vs_sequential(S, dcsbm, np)
         print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
