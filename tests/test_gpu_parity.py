@@ -248,3 +248,25 @@ def test_hashed_rows_grow_and_stay_exact(S, O):
         assert total > 0, "the test no longer drives the rows past their capacity"
     finally:
         S.set_option("dense_max_blocks", 16384)
+
+
+def _reference_runs():
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "reference_runs.json")) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("run", _reference_runs(), ids=lambda r: f"cfg{r['config']}-{r['algorithm']}")
+def test_end_to_end_against_recorded_reference_runs(S, O, run):
+    """Unseeded end-to-end criterion: the engine's final MDL within 0.5 % and its NMI against
+    the planted blocks within 0.01 of a run of the reference itself (built from its sources;
+    recorded by tests/golden/make_reference_runs.py)."""
+    import dcsbm
+    V, s, d, truth = dcsbm.config_graph(run["config"])
+    g = S.Graph(V, s, d)
+    assert g.E == run["E"]
+    out, st = S.sbp.stochastic_block_partition(g, algorithm=run["algorithm"], batches=run["batches"],
+                                               approximate=run["approximate"], seed=17)
+    assert abs(st["mdl"] - run["mdl"]) <= 0.005 * run["mdl"]
+    assert abs(O.nmi(out, truth) - run["nmi"]) <= 0.01
