@@ -219,7 +219,7 @@ void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, in
     }
     k_gibbs_eval<<<grid, kLightWarps * 32, smem, c.stream>>>(g.view(), bm.view(), plan.order.p + plan.light_begin[bt],
                                                             nl, rng, sweep, bm.prop.p, bm.moved.p, n_cur,
-                                                            c.counters, g.light_cap, c.status);
+                                                            c.counters, g.light_cap, c.status, nullptr, 0);
     SBP_CHECK_LAUNCH();
     if (g_prof.on) {
       SBP_CUDA(cudaEventRecord(e1, c.stream));
@@ -234,7 +234,7 @@ void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, in
     set_smem_limit((const void*)k_gibbs_eval, std::max(smem, (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps));
     k_gibbs_eval<<<grid_for(nh, 1, 64 * c.num_sms), 32, smem, c.stream>>>(
         g.view(), bm.view(), plan.order.p + plan.heavy_begin[bt], nh, rng, sweep, bm.prop.p, bm.moved.p, n_cur,
-        c.counters, g.heavy_cap, c.status);
+        c.counters, g.heavy_cap, c.status, nullptr, 0);
     SBP_CHECK_LAUNCH();
   }
   gibbs_apply(bm, g, nl + nh);
@@ -248,7 +248,7 @@ void gibbs_apply(SbpBlockmodel& bm, const SbpGraph& g, int batch) {
   const unsigned gen = ++bm.gen;
   const int gw = grid_for((long long)batch * 32, 256, 64 * c.num_sms);
   k_apply_edges<<<gw, 256, 0, c.stream>>>(g.view(), bm.view(), bm.moved.p, n_cur, bm.prop.p, bm.qr.p, bm.qs.p,
-                                          bm.last.p, gen);
+                                          bm.last.p, gen, nullptr, 0);
   SBP_CHECK_LAUNCH();
   if (bm.sparse) {
     int ovf = 0;
@@ -269,10 +269,101 @@ void gibbs_apply(SbpBlockmodel& bm, const SbpGraph& g, int batch) {
     }
   }
   k_apply_finish<<<grid_for(batch, 256, 64 * c.num_sms), 256, 0, c.stream>>>(
-      bm.view(), bm.moved.p, n_cur, n_next, bm.prop.p, bm.qr.p, bm.qs.p, bm.last.p, gen);
+      bm.view(), bm.moved.p, n_cur, n_next, bm.prop.p, bm.qr.p, bm.qs.p, bm.last.p, gen, nullptr, 0);
   SBP_CHECK_LAUNCH();
 }
 
+
+// Asynchronous-Gibbs sweeps of one finetune call as ONE CUDA graph launch: a conditional while
+// node whose body is a sweep (every batch's evaluation, apply and degree step, the MDL, then
+// k_sweep_control, which applies the early stop on the GPU and sets the loop condition).
+// Same kernels, same order and the same early-stop arithmetic as the host loop, so the chain
+// and the sweep count are the host loop's.  Returns the sweeps run.
+static DevBuf<SweepCtl> g_ctl;
+
+static int gibbs_sweeps_graph(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, RngParams rng,
+                              int max_sweeps, bool bracket, double initial_entropy) {
+  Context& c = Context::get();
+  const int nb = (int)plan.light_n.size();
+  g_ctl.reserve(1);
+  SweepCtl h;
+  std::memset(&h, 0, sizeof h);
+  h.sweep = 0;
+  h.gen0 = bm.gen;
+  h.nbatches = nb;
+  h.count = 0;
+  h.max_sweeps = max_sweeps;
+  h.bracket = bracket ? 1 : 0;
+  h.n_moved = bm.n_moved.p;
+  h.initial = initial_entropy;
+  SBP_CUDA(SBP_COPY_ASYNC(g_ctl.p, &h, sizeof h, cudaMemcpyHostToDevice, c.stream));
+  const size_t smem_light = (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps;
+  const size_t smem_heavy = (size_t)table_ints(g.heavy_cap) * sizeof(int);
+  set_smem_limit((const void*)k_gibbs_eval, std::max(smem_light, smem_heavy));
+  const bool cells = (long long)bm.B * bm.B <= 4LL * g.E;
+  const int mdl_grid = c.npartial;
+
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  struct Guard {
+    cudaGraph_t* g;
+    cudaGraphExec_t* e;
+    ~Guard() {
+      if (*e) cudaGraphExecDestroy(*e);
+      if (*g) cudaGraphDestroy(*g);
+    }
+  } guard{&graph, &exec};
+  SBP_CUDA(cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle loop;
+  SBP_CUDA(cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault));
+  // cudaGraphNodeParams holds a union of non-trivial members: build it in zeroed storage
+  alignas(cudaGraphNodeParams) unsigned char cp_storage[sizeof(cudaGraphNodeParams)] = {};
+  cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_storage);
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = loop;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  SBP_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  SBP_CUDA(cudaStreamBeginCaptureToGraph(c.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  int launches = 0;
+  for (int bt = 0; bt < nb; ++bt) {
+    const int nl = plan.light_n[bt], nh = plan.heavy_n[bt];
+    if (nl > 0) {
+      k_gibbs_eval<<<grid_for(nl, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem_light, c.stream>>>(
+          g.view(), bm.view(), plan.order.p + plan.light_begin[bt], nl, rng, 0, bm.prop.p, bm.moved.p, nullptr,
+          c.counters, g.light_cap, c.status, g_ctl.p, bt);
+      ++launches;
+    }
+    if (nh > 0) {
+      k_gibbs_eval<<<grid_for(nh, 1, 64 * c.num_sms), 32, smem_heavy, c.stream>>>(
+          g.view(), bm.view(), plan.order.p + plan.heavy_begin[bt], nh, rng, 0, bm.prop.p, bm.moved.p, nullptr,
+          c.counters, g.heavy_cap, c.status, g_ctl.p, bt);
+      ++launches;
+    }
+    const int batch = nl + nh;
+    k_apply_edges<<<grid_for((long long)batch * 32, 256, 64 * c.num_sms), 256, 0, c.stream>>>(
+        g.view(), bm.view(), bm.moved.p, nullptr, bm.prop.p, bm.qr.p, bm.qs.p, bm.last.p, 0u, g_ctl.p, bt);
+    k_apply_finish<<<grid_for(batch, 256, 64 * c.num_sms), 256, 0, c.stream>>>(
+        bm.view(), bm.moved.p, nullptr, nullptr, bm.prop.p, bm.qr.p, bm.qs.p, bm.last.p, 0u, g_ctl.p, bt);
+    launches += 2;
+  }
+  if (cells) k_mdl_cells<<<mdl_grid, 256, 0, c.stream>>>(bm.view(), c.partial);
+  else k_mdl_edges<<<mdl_grid, 256, 0, c.stream>>>(g.view(), bm.view(), g.out_src.p, c.partial);
+  k_mdl_final<<<1, 256, 0, c.stream>>>(c.partial, mdl_grid, g.V, g.E, bm.B, c.scalar);
+  k_sweep_control<<<1, 32, 0, c.stream>>>(g_ctl.p, c.scalar, loop);
+  launches += 3;
+  const cudaError_t ce = cudaStreamEndCapture(c.stream, &body);
+  SBP_CUDA(ce);
+  SBP_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+  SBP_CUDA(cudaGraphLaunch(exec, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(&h, g_ctl.p, sizeof h, cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  g_launches += (long long)launches * h.count;
+  bm.gen += (unsigned)(nb * h.count);
+  return h.count;
+}
 
 // finetune::{metropolis_hastings, asynchronous_gibbs, hybrid_mcmc}.
 void finetune(SbpBlockmodel& bm, SbpGraph& g, int algo, const SbpFinetuneOptions& opt, const SbpReplay* replay,
@@ -304,6 +395,10 @@ void finetune(SbpBlockmodel& bm, SbpGraph& g, int algo, const SbpFinetuneOptions
   long long mh_visits = 0, mh_moved = 0, mh_acc = 0;
   const BatchPlan* plan = nullptr;
   if (algo != SBP_METROPOLIS_HASTINGS) plan = &g.plan(algo, opt.batches);
+  if (algo == SBP_ASYNC_GIBBS && g_graph_sweeps && !bm.sparse && !g_prof.on && !plan->light_n.empty()) {
+    st.sweeps = gibbs_sweeps_graph(bm, g, *plan, rng, max_sweeps, bracket, initial_entropy);
+    c.check_status();
+  } else
   for (int it = 0; it < max_sweeps; ++it) {
     if (algo == SBP_METROPOLIS_HASTINGS) {
       const MhResult r = mh_pass(bm, g, g.identity.p, g.V, g.max_k, rng, it);
@@ -782,6 +877,9 @@ SbpStatus sbp_set_option(const char* name, int64_t value) {
   if (n == "dense_max_blocks") {
     SBP_REQUIRE(value >= 1 && value <= (1 << 30), "dense_max_blocks out of range");
     g_dense_max_blocks = (int)value;
+  } else if (n == "graph_sweeps") {
+    SBP_REQUIRE(value == 0 || value == 1, "graph_sweeps must be 0 or 1");
+    g_graph_sweeps = (int)value;
   } else {
     throw Error(SBP_ERR_INVALID_ARGUMENT, "unknown option: " + n);
   }

@@ -3,6 +3,7 @@
 // sbp_learned.cu: the learned proposal).  Not part of the public C ABI.
 #pragma once
 #include <functional>
+#include <map>
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -57,23 +58,75 @@ inline cudaError_t count_copy(cudaError_t e, size_t bytes, cudaMemcpyKind kind) 
 #define SBP_COPY_ASYNC(dst, src, bytes, kind, stream) \
   count_copy(cudaMemcpyAsync(dst, src, bytes, kind, stream), bytes, kind)
 
+// Released device buffers are kept for reuse instead of being freed: cudaFree synchronizes
+// the whole device, and every partition round releases and reallocates its blockmodel's
+// buffers.  A reused buffer is handed out only after the engine's stream has drained, so no
+// queued kernel still reads it.  At most kDeviceCacheBytes stay cached.
+cudaStream_t engine_stream();
+
+struct DeviceCache {
+  static constexpr size_t kDeviceCacheBytes = 32ull << 30;
+  std::multimap<size_t, void*> blocks;   // bytes -> buffer
+  size_t cached = 0;
+  static DeviceCache& get() {
+    static DeviceCache* c = new DeviceCache();   // never destroyed: buffers live until exit
+    return *c;
+  }
+  void* take(size_t bytes, size_t* got) {
+    auto it = blocks.lower_bound(bytes);
+    if (it != blocks.end() && it->first <= bytes + bytes / 4 + (1u << 20)) {
+      void* p = it->second;
+      *got = it->first;
+      cached -= it->first;
+      blocks.erase(it);
+      SBP_CUDA(cudaStreamSynchronize(engine_stream()));
+      return p;
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaErrorMemoryAllocation && !blocks.empty()) {   // give the cache back and retry
+      cudaGetLastError();
+      SBP_CUDA(cudaStreamSynchronize(engine_stream()));
+      for (auto& kv : blocks) cudaFree(kv.second);
+      blocks.clear();
+      cached = 0;
+      e = cudaMalloc(&p, bytes);
+    }
+    if (e == cudaErrorMemoryAllocation) throw Error(SBP_ERR_OUT_OF_MEMORY, "cudaMalloc: out of device memory");
+    SBP_CUDA(e);
+    *got = bytes;
+    return p;
+  }
+  void give(void* p, size_t bytes) {
+    if (cached + bytes > kDeviceCacheBytes) {
+      cudaFree(p);
+      return;
+    }
+    blocks.emplace(bytes, p);
+    cached += bytes;
+  }
+};
+
 template <class T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  size_t bytes = 0;   // size of the underlying allocation
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) DeviceCache::get().give(p, bytes);
     p = nullptr;
     n = 0;
+    bytes = 0;
   }
   void reserve(size_t count) {   // grow-only, contents not preserved
     if (count <= n && p) return;
     release();
-    SBP_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    const size_t want = std::max<size_t>(count, 1) * sizeof(T);
+    p = static_cast<T*>(DeviceCache::get().take(want, &bytes));
     n = std::max<size_t>(count, 1);
   }
 };
@@ -134,6 +187,8 @@ struct Context {
   }
 };
 
+inline cudaStream_t engine_stream() { return Context::get().stream; }
+
 // Optional timing of the vertex-evaluation kernel: CUDA events around every light-vertex
 // evaluation launch on the launching stream, resolved when the profile is read.
 struct EvalProfiler {
@@ -188,6 +243,9 @@ constexpr int kSmemRebuildMaxB = 100;
 
 // Blocks above which the block matrix is row-hashed instead of dense (sbp_set_option).
 inline int g_dense_max_blocks = 16384;
+// 1: an asynchronous-Gibbs finetune on dense storage runs as one CUDA graph launch with the
+// sweep loop decided on the GPU; 0: one host-driven launch sequence per sweep (sbp_set_option).
+inline int g_graph_sweeps = 1;
 inline long long g_overflow_rebuilds = 0;   // rebuilds forced by a full hashed row
 
 }  // namespace sbpb

@@ -97,8 +97,12 @@ __global__ void k_mdl_final(const double* partial, int n, int V, long long E, in
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256, 2) k_gibbs_eval(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng,
                              int sweep, int* prop, int* moved_list, int* n_moved, unsigned long long* counters,
-                             int cap, int* status) {
+                             int cap, int* status, const SweepCtl* ctl, int batch) {
   extern __shared__ int smem[];
+  if (ctl) {
+    sweep = ctl->sweep;
+    n_moved = ctl->n_moved + ((ctl->gen0 + (unsigned)batch) & 1u);
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wpb = blockDim.x >> 5;
   WarpTable t = carve_table(smem, cap, warp);
@@ -151,7 +155,11 @@ __device__ __forceinline__ void cell_add_owned(const BlockView& bm, int row, int
 // delta of each move as seen at its turn in vertex order, which Blockmodel::move_vertex folds
 // into d[r], d[s] (blockmodel.cpp:348-359); last[x] keeps (batch generation, last mover of x).
 __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, const int* n_moved, const int* prop,
-                              int* qr, int* qs, unsigned long long* last, unsigned gen) {
+                              int* qr, int* qs, unsigned long long* last, unsigned gen, const SweepCtl* ctl, int batch) {
+  if (ctl) {
+    gen = ctl->gen0 + (unsigned)batch + 1u;
+    n_moved = ctl->n_moved + ((gen - 1u) & 1u);
+  }
   const int lane = threadIdx.x & 31;
   const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -162,11 +170,42 @@ __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, 
 // d[r], d[s] from the last mover of each block, then the new assignment; clears the other
 // moved-count slot for the next batch.
 __global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved, int* prop,
-                               const int* qr, const int* qs, const unsigned long long* last, unsigned gen) {
+                               const int* qr, const int* qs, const unsigned long long* last, unsigned gen,
+                               const SweepCtl* ctl, int batch) {
+  if (ctl) {
+    gen = ctl->gen0 + (unsigned)batch + 1u;
+    n_moved = ctl->n_moved + ((gen - 1u) & 1u);
+    next_n_moved = ctl->n_moved + (gen & 1u);
+  }
   const int n = *n_moved;
   if (blockIdx.x == 0 && threadIdx.x == 0) *next_n_moved = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     finish_moved_vertex(bm, moved_list[i], prop, qr, qs, last, gen);
+}
+
+// End of one sweep of a graph-run finetune: record delta = MDL - first MDL (the asynchronous-
+// Gibbs rule, src/finetune.cpp:40,74) and apply finetune::early_stop (src/finetune.cpp:144-162)
+// in the host's arithmetic; the loop continues while it does not stop.
+__global__ void k_sweep_control(SweepCtl* ctl, const double* mdl, cudaGraphConditionalHandle loop) {
+  if (threadIdx.x || blockIdx.x) return;
+  const int it = ctl->count;
+  ctl->deltas[it] = *mdl - ctl->initial;
+  ctl->count = it + 1;
+  bool stop;
+  if (ctl->deltas[it] == 0.0) {
+    stop = true;
+  } else if (it < 3) {
+    stop = false;
+  } else {
+    double average = ctl->deltas[it] + ctl->deltas[it - 1] + ctl->deltas[it - 2];
+    average /= -3.0;
+    const double threshold = ctl->bracket ? 1e-4 * ctl->initial : 5e-4 * ctl->initial;
+    stop = average < threshold;
+  }
+  if (ctl->count >= ctl->max_sweeps) stop = true;
+  ctl->sweep = it + 1;
+  ctl->gen0 += (unsigned)ctl->nbatches;
+  cudaGraphSetConditional(loop, stop ? 0u : 1u);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -7,6 +7,21 @@ namespace sbpb {
 constexpr int kProposalsPerBlock = 10;   // block_merge::NUM_AGG_PROPOSALS_PER_BLOCK (include/block_merge.hpp:24)
 constexpr int kMaxIterations = 100;      // finetune::MAX_NUM_ITERATIONS (include/finetune.hpp:56)
 
+// Device-side state of an asynchronous-Gibbs finetune run as one CUDA graph: the loop over
+// sweeps and its early stop are decided on the GPU (k_sweep_control).  Kernels given a
+// control block read the sweep index and the batch generation from it.
+struct SweepCtl {
+  int sweep;               // index of the sweep being run
+  unsigned gen0;           // batch generation before the sweep
+  int nbatches;
+  int count;               // sweeps finished
+  int max_sweeps;
+  int bracket;
+  int* n_moved;            // the blockmodel's two moved-count slots
+  double initial;          // the call's first MDL, as stored (float) by the reference
+  double deltas[kMaxIterations];
+};
+
 struct Csr {
   const int* ptr;
   const int* idx;
@@ -21,11 +36,13 @@ __global__ void k_mdl_edges(GraphView g, BlockView bm, const int* __restrict__ o
 __global__ void k_mdl_final(const double* partial, int n, int V, long long E, int B, double* out);
 __global__ void __launch_bounds__(256, 2) k_gibbs_eval(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng,
                              int sweep, int* prop, int* moved_list, int* n_moved, unsigned long long* counters,
-                             int cap, int* status);
+                             int cap, int* status, const SweepCtl* ctl, int batch);
 __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, const int* n_moved, const int* prop,
-                              int* qr, int* qs, unsigned long long* last, unsigned gen);
+                              int* qr, int* qs, unsigned long long* last, unsigned gen, const SweepCtl* ctl, int batch);
 __global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved, int* prop,
-                               const int* qr, const int* qs, const unsigned long long* last, unsigned gen);
+                               const int* qr, const int* qs, const unsigned long long* last, unsigned gen,
+                               const SweepCtl* ctl, int batch);
+__global__ void k_sweep_control(SweepCtl* ctl, const double* mdl, cudaGraphConditionalHandle loop);
 __global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, int n, int start, RngParams rng,
                      int sweep, int cap, double* out, int* status);
 __global__ void k_move_vertex(GraphView g, BlockView bm, int v, int s, int cap, int* status);

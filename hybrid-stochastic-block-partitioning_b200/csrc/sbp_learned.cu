@@ -1039,7 +1039,7 @@ SbpStatus sbp_collect_moves(SbpBlockmodel* bm, const SbpGraph* cg, SbpDataset* d
         set_smem_limit((const void*)k_gibbs_eval, smem);
         k_gibbs_eval<<<grid_for(nl, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem, c.stream>>>(
             g.view(), bm->view(), plan.order.p + plan.light_begin[bt], nl, rng, it, bm->prop.p, bm->moved.p, n_cur,
-            c.counters, g.light_cap, c.status);
+            c.counters, g.light_cap, c.status, nullptr, 0);
         SBP_CHECK_LAUNCH();
       }
       if (nh > 0) {
@@ -1048,7 +1048,7 @@ SbpStatus sbp_collect_moves(SbpBlockmodel* bm, const SbpGraph* cg, SbpDataset* d
                        std::max(smem, (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps));
         k_gibbs_eval<<<grid_for(nh, 1, 64 * c.num_sms), 32, smem, c.stream>>>(
             g.view(), bm->view(), plan.order.p + plan.heavy_begin[bt], nh, rng, it, bm->prop.p, bm->moved.p, n_cur,
-            c.counters, g.heavy_cap, c.status);
+            c.counters, g.heavy_cap, c.status, nullptr, 0);
         SBP_CHECK_LAUNCH();
       }
       const int batch = nl + nh;

@@ -111,7 +111,9 @@ int32_t sbp_device_count(void);
 /* Engine options (no reference counterpart).  "dense_max_blocks": blockmodels with more blocks
  * than this keep their block matrix as row-hashed regions (a sparse device-resident matrix with
  * integer counts updated by atomics) instead of dense B x B arrays; default 16384.  Applies to
- * blockmodels whose block count is set after the call. */
+ * blockmodels whose block count is set after the call.  "graph_sweeps" (default 1): an
+ * asynchronous-Gibbs finetune on dense storage runs as one CUDA graph launch whose sweep loop and
+ * early stop are decided on the GPU; 0 drives every sweep from the host (same results). */
 SbpStatus sbp_set_option(const char *name, int64_t value);
 
 /* The CUDA stream every call of this library runs on (cudaStream_t), for interop and timing.

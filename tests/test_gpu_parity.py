@@ -270,3 +270,31 @@ def test_end_to_end_against_recorded_reference_runs(S, O, run):
                                                approximate=run["approximate"], seed=17)
     assert abs(st["mdl"] - run["mdl"]) <= 0.005 * run["mdl"]
     assert abs(O.nmi(out, truth) - run["nmi"]) <= 0.01
+
+
+@pytest.mark.parametrize("batches,seed", [(10, 3), (3, 4), (7, 5)])   # odd batch counts flip the moved-slot parity
+def test_graph_run_sweeps_equal_host_driven_sweeps(S, O, batches, seed):
+    """An asynchronous-Gibbs finetune as one CUDA graph launch (loop and early stop on the GPU)
+    gives the host-driven loop's chain, sweep count and counters, and the oracle's."""
+    V, s, d, _ = random_graph(1500, 8, 90 + seed)
+    a = random_assignment(V, 40, seed)
+    g = S.Graph(V, s, d)
+    res = []
+    for mode in (1, 0):
+        S.set_option("graph_sweeps", mode)
+        try:
+            bm = S.Blockmodel(g, 40, a)
+            st = S.finetune.asynchronous_gibbs(bm, batches=batches, seed=seed, call=1)
+            res.append((bm, st))
+        finally:
+            S.set_option("graph_sweeps", 1)
+    (b1, s1), (b0, s0) = res
+    assert np.array_equal(b1.block_assignment(), b0.block_assignment())
+    assert np.array_equal(b1.blockmatrix(), b0.blockmatrix())
+    assert np.array_equal(b1.degrees_all()[2], b0.degrees_all()[2])
+    for k in ("sweeps", "visits", "accepted", "proposals_moved", "mdl"):
+        assert s1[k] == s0[k], k
+    obm = O.Blockmodel(O.Graph(V, s, d), 40, a)
+    ost = obm.finetune(1, batches=batches, seed=seed, call=1)
+    assert_same_state(b1, obm)
+    assert s1["sweeps"] == ost["sweeps"]
