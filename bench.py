@@ -381,7 +381,7 @@ def main():
                     "h2d_bytes_per_step": int((pe1["h2d_bytes"] - pe0["h2d_bytes"]) / max(1, a.steps)),
                     "d2h_bytes_per_step": int((pe1["d2h_bytes"] - pe0["d2h_bytes"]) / max(1, a.steps)),
                     "ms_per_step": e2e_ms / max(1, a.steps)},
-            "roofline": {"bound": "hbm", "kernel": "k_gibbs_eval", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": "k_gibbs_eval_dense / _hashed", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
                          "avg_launch_us": avg_ms * 1e3, "launches_profiled": int(pr["eval_launches"]),
                          "bytes_per_launch": pr["eval_bytes"] / max(1, pr["eval_launches"])},

@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(kBThreads, 2)
             const uint4 x =
                 draw_record(gr.rng, (uint32_t)v, (uint32_t)gr.sweep, 0u, (long long)gr.sweep * gr.g.V + v, status);
             int r, k_out, k_in;
-            const EvalResult res = evaluate_vertex(gr.g, gr.bm, v, x, t, lane, status, &r, &k_out, &k_in);
+            const EvalResult res = evaluate_vertex<Store::kDense>(gr.g, gr.bm, v, x, t, lane, status, &r, &k_out, &k_in);
             c_visit++;
             if (res.s != r) c_moved++;
             if (res.accepted) {
@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(kBThreads, 2)
             const uint4 x =
                 draw_record(gr.rng, (uint32_t)v, (uint32_t)gr.sweep, 0u, (long long)gr.sweep * gr.g.V + v, status);
             int r, k_out, k_in;
-            const EvalResult res = evaluate_vertex(gr.g, gr.bm, v, x, big, lane, status, &r, &k_out, &k_in);
+            const EvalResult res = evaluate_vertex<Store::kDense>(gr.g, gr.bm, v, x, big, lane, status, &r, &k_out, &k_in);
             if (lane == 0) {
               atomicAdd(gr.counters + 0, 1ull);
               if (res.s != r) atomicAdd(gr.counters + 1, 1ull);

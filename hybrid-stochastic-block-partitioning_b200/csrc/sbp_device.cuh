@@ -204,11 +204,21 @@ __device__ __forceinline__ void hashed_add(const long long* base, const int* mas
 }
 
 // M[row, col] and MT[row, col] = M[col, row] in either representation.
+// Storage of the block matrix as a compile-time choice (kAny: decided by bm.sparse at run time).
+// Kernels instantiated for one storage carry no code for the other.
+enum class Store { kAny, kDense, kHashed };
+
+template <Store S = Store::kAny>
 __device__ __forceinline__ int bm_get(const BlockView& bm, int row, int col) {
-  return bm.sparse ? hashed_get(bm.rbase, bm.rmask, bm.rslot, row, col) : bm.M[(size_t)row * bm.ld + col];
+  if constexpr (S == Store::kDense) return bm.M[(size_t)row * bm.ld + col];
+  else if constexpr (S == Store::kHashed) return hashed_get(bm.rbase, bm.rmask, bm.rslot, row, col);
+  else return bm.sparse ? hashed_get(bm.rbase, bm.rmask, bm.rslot, row, col) : bm.M[(size_t)row * bm.ld + col];
 }
+template <Store S = Store::kAny>
 __device__ __forceinline__ int bm_getT(const BlockView& bm, int row, int col) {
-  return bm.sparse ? hashed_get(bm.cbase, bm.cmask, bm.cslot, row, col) : bm.MT[(size_t)row * bm.ld + col];
+  if constexpr (S == Store::kDense) return bm.MT[(size_t)row * bm.ld + col];
+  else if constexpr (S == Store::kHashed) return hashed_get(bm.cbase, bm.cmask, bm.cslot, row, col);
+  else return bm.sparse ? hashed_get(bm.cbase, bm.cmask, bm.cslot, row, col) : bm.MT[(size_t)row * bm.ld + col];
 }
 
 // Walk of a hashed row in ascending column order: bisection over the column space for the
@@ -487,6 +497,7 @@ __device__ __forceinline__ int gather_neighbour_blocks(const GraphView& g, const
 // over the distinct neighbour blocks gives the Hastings sums and the changed cells; the corner
 // cells, degree terms and the net-zero double count are spread over lanes.  Every lane
 // returns the same values.
+template <Store ST = Store::kAny>
 __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView& bm, int r, int s, int k_out,
                                              int k_in, int self, const WarpTable& t, int lane, double* H) {
   __syncwarp();
@@ -496,8 +507,8 @@ __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView
   const int d_rs = -mc.co_s + mc.ci_r;
   const int d_sr = mc.co_r - mc.ci_s;
   const int d_ss = mc.co_s + mc.ci_s + self;
-  const int M_rr = bm_get(bm, r, r), M_rs = bm_get(bm, r, s);
-  const int M_sr = bm_get(bm, s, r), M_ss = bm_get(bm, s, s);
+  const int M_rr = bm_get<ST>(bm, r, r), M_rs = bm_get<ST>(bm, r, s);
+  const int M_sr = bm_get<ST>(bm, s, r), M_ss = bm_get<ST>(bm, s, s);
   const int dout_r = bm.d_out[r], dout_s = bm.d_out[s], din_r = bm.d_in[r], din_s = bm.d_in[s];
   const int kin_self = k_in + self;
 
@@ -508,7 +519,7 @@ __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView
     const int h = t.list[i];
     const int u = t.keys[h];
     const int co = t.cout[h], ci = t.cin[h];
-    const int M_su = bm_get(bm, s, u), M_us = bm_getT(bm, s, u), M_ru = bm_get(bm, r, u), M_ur = bm_getT(bm, r, u);
+    const int M_su = bm_get<ST>(bm, s, u), M_us = bm_getT<ST>(bm, s, u), M_ru = bm_get<ST>(bm, r, u), M_ur = bm_getT<ST>(bm, r, u);
     const int du = bm.d[u];
     const bool is_r = (u == r), is_s = (u == s), corner = is_r || is_s;
     const double c = (double)(co + ci + (is_r ? self : 0));
@@ -560,6 +571,7 @@ __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView
 //     gathered elements, so its block comes from the same pass;
 //  2. the multinomial walk over M[t,:] + M[:,t] picks s;
 //  3. move_delta gives delta-MDL and the Hastings correction.
+template <Store ST = Store::kAny>
 __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const BlockView& bm, int v, uint4 x,
                                                       const WarpTable& t, int lane, int* status, int* r_out,
                                                       int* k_out_out, int* k_in_out) {
@@ -585,14 +597,17 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
     const int dot = bm.d_out[tblk];
     const long long total = (long long)dot + (long long)bm.d_in[tblk];
     const long long target = scale32(x.y, total);
-    if (bm.sparse) {
+    const bool hashed = ST == Store::kHashed || (ST == Store::kAny && bm.sparse);
+    if (ST != Store::kDense && hashed) {
       if (target < dot) s = warp_select_hashed(bm.rbase, bm.rmask, bm.rslot, tblk, bm.B, target, lane);
       else s = warp_select_hashed(bm.cbase, bm.cmask, bm.cslot, tblk, bm.B, target - dot, lane);
-    } else if (target < dot) {
+    } else if (ST != Store::kHashed && target < dot) {
       s = warp_select_chunked(bm.M + (size_t)tblk * bm.ld, bm.CS + (size_t)tblk * bm.nch, bm.nch, target, lane);
-    } else {
+    } else if (ST != Store::kHashed) {
       s = warp_select_chunked(bm.MT + (size_t)tblk * bm.ld, bm.CST + (size_t)tblk * bm.nch, bm.nch, target - dot,
                               lane);
+    } else {
+      s = -1;
     }
     if (s < 0) {
       if (lane == 0) atomicOr(status, kErrScan);
@@ -602,7 +617,7 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
   res.s = s;
   if (s == r) return res;
   double Hp;
-  const double dS = move_delta(g, bm, r, s, k_out, k_in, self, t, lane, &Hp);
+  const double dS = move_delta<ST>(g, bm, r, s, k_out, k_in, self, t, lane, &Hp);
   const double H = (k == 0) ? 1.0 : Hp;
   double ap = exp(-3.0 * dS) * H;
   ap = ap >= 1.0 ? 1.0 : ap;

@@ -207,9 +207,10 @@ void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, in
   Context& c = Context::get();
   const int nl = plan.light_n[bt], nh = plan.heavy_n[bt];
   int* n_cur = bm.n_moved.p + (bm.gen & 1);
+  const GibbsEvalKernel k_eval = gibbs_eval_kernel(bm.sparse);
   if (nl > 0) {
     const size_t smem = (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps;
-    set_smem_limit((const void*)k_gibbs_eval, smem);
+    set_smem_limit((const void*)k_eval, smem);
     const int grid = grid_for(nl, kLightWarps, 64 * c.num_sms);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (g_prof.on) {
@@ -217,7 +218,7 @@ void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, in
       e1 = g_prof.get();
       SBP_CUDA(cudaEventRecord(e0, c.stream));
     }
-    k_gibbs_eval<<<grid, kLightWarps * 32, smem, c.stream>>>(g.view(), bm.view(), plan.order.p + plan.light_begin[bt],
+    k_eval<<<grid, kLightWarps * 32, smem, c.stream>>>(g.view(), bm.view(), plan.order.p + plan.light_begin[bt],
                                                             nl, rng, sweep, bm.prop.p, bm.moved.p, n_cur,
                                                             c.counters, g.light_cap, c.status, nullptr, 0);
     SBP_CHECK_LAUNCH();
@@ -231,8 +232,8 @@ void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, in
   }
   if (nh > 0) {
     const size_t smem = (size_t)table_ints(g.heavy_cap) * sizeof(int);
-    set_smem_limit((const void*)k_gibbs_eval, std::max(smem, (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps));
-    k_gibbs_eval<<<grid_for(nh, 1, 64 * c.num_sms), 32, smem, c.stream>>>(
+    set_smem_limit((const void*)k_eval, std::max(smem, (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps));
+    k_eval<<<grid_for(nh, 1, 64 * c.num_sms), 32, smem, c.stream>>>(
         g.view(), bm.view(), plan.order.p + plan.heavy_begin[bt], nh, rng, sweep, bm.prop.p, bm.moved.p, n_cur,
         c.counters, g.heavy_cap, c.status, nullptr, 0);
     SBP_CHECK_LAUNCH();
@@ -299,7 +300,8 @@ static int gibbs_sweeps_graph(SbpBlockmodel& bm, const SbpGraph& g, const BatchP
   SBP_CUDA(SBP_COPY_ASYNC(g_ctl.p, &h, sizeof h, cudaMemcpyHostToDevice, c.stream));
   const size_t smem_light = (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps;
   const size_t smem_heavy = (size_t)table_ints(g.heavy_cap) * sizeof(int);
-  set_smem_limit((const void*)k_gibbs_eval, std::max(smem_light, smem_heavy));
+  const GibbsEvalKernel k_eval = k_gibbs_eval_dense;   // the graph runs dense storage only
+  set_smem_limit((const void*)k_eval, std::max(smem_light, smem_heavy));
   const bool cells = (long long)bm.B * bm.B <= 4LL * g.E;
   const int mdl_grid = c.npartial;
 
@@ -331,13 +333,13 @@ static int gibbs_sweeps_graph(SbpBlockmodel& bm, const SbpGraph& g, const BatchP
   for (int bt = 0; bt < nb; ++bt) {
     const int nl = plan.light_n[bt], nh = plan.heavy_n[bt];
     if (nl > 0) {
-      k_gibbs_eval<<<grid_for(nl, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem_light, c.stream>>>(
+      k_eval<<<grid_for(nl, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem_light, c.stream>>>(
           g.view(), bm.view(), plan.order.p + plan.light_begin[bt], nl, rng, 0, bm.prop.p, bm.moved.p, nullptr,
           c.counters, g.light_cap, c.status, g_ctl.p, bt);
       ++launches;
     }
     if (nh > 0) {
-      k_gibbs_eval<<<grid_for(nh, 1, 64 * c.num_sms), 32, smem_heavy, c.stream>>>(
+      k_eval<<<grid_for(nh, 1, 64 * c.num_sms), 32, smem_heavy, c.stream>>>(
           g.view(), bm.view(), plan.order.p + plan.heavy_begin[bt], nh, rng, 0, bm.prop.p, bm.moved.p, nullptr,
           c.counters, g.heavy_cap, c.status, g_ctl.p, bt);
       ++launches;

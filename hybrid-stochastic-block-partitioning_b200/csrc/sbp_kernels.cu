@@ -3,7 +3,7 @@
 // Kernel map (reference function each one stands in for):
 //   k_rebuild_*        Blockmodel::initialize_edge_counts     src/blockmodel/blockmodel.cpp:187-255
 //   k_mdl_*            entropy::mdl / log_posterior_probability src/entropy.cpp:584-589, blockmodel.cpp:267-285
-//   k_gibbs_eval       asynchronous_gibbs evaluation half     src/finetune.cpp:49-57, 531-545
+//   k_gibbs_eval_*     asynchronous_gibbs evaluation half     src/finetune.cpp:49-57, 531-545
 //   k_apply_*          asynchronous_gibbs apply half          src/finetune.cpp:58-71 + Blockmodel::move_vertex
 //   k_mh               metropolis_hastings sweep              src/finetune.cpp:412-444, 446-501
 //   k_row_nnz/fill     ISparseMatrix row/column views for the merge phase
@@ -95,9 +95,11 @@ __global__ void k_mdl_final(const double* partial, int n, int V, long long E, in
 // Asynchronous Gibbs: evaluate a list of vertices against the frozen state.  Accepted moves
 // go to prop[v] and the moved list; counters: [0] visits [1] proposals_moved [2] accepted.
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 2) k_gibbs_eval(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng,
-                             int sweep, int* prop, int* moved_list, int* n_moved, unsigned long long* counters,
-                             int cap, int* status, const SweepCtl* ctl, int batch) {
+template <Store ST>
+__device__ __forceinline__ void gibbs_eval_body(GraphView g, BlockView bm, const int* __restrict__ verts, int n,
+                                                RngParams rng, int sweep, int* prop, int* moved_list, int* n_moved,
+                                                unsigned long long* counters, int cap, int* status,
+                                                const SweepCtl* ctl, int batch) {
   extern __shared__ int smem[];
   if (ctl) {
     sweep = ctl->sweep;
@@ -112,7 +114,7 @@ __global__ void __launch_bounds__(256, 2) k_gibbs_eval(GraphView g, BlockView bm
     const int v = verts[i];
     const uint4 x = draw_record(rng, (uint32_t)v, (uint32_t)sweep, 0u, (long long)sweep * g.V + v, status);
     int r, k_out, k_in;
-    const EvalResult res = evaluate_vertex(g, bm, v, x, t, lane, status, &r, &k_out, &k_in);
+    const EvalResult res = evaluate_vertex<ST>(g, bm, v, x, t, lane, status, &r, &k_out, &k_in);
     c_visit++;
     if (res.s != r) c_moved++;
     if (res.accepted) {
@@ -129,6 +131,21 @@ __global__ void __launch_bounds__(256, 2) k_gibbs_eval(GraphView g, BlockView bm
     atomicAdd(counters + 1, c_moved);
     atomicAdd(counters + 2, c_acc);
   }
+}
+
+__global__ void __launch_bounds__(256, 2)
+    k_gibbs_eval_dense(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
+                       int* prop, int* moved_list, int* n_moved, unsigned long long* counters, int cap, int* status,
+                       const SweepCtl* ctl, int batch) {
+  gibbs_eval_body<Store::kDense>(g, bm, verts, n, rng, sweep, prop, moved_list, n_moved, counters, cap, status, ctl,
+                                 batch);
+}
+__global__ void __launch_bounds__(256, 2)
+    k_gibbs_eval_hashed(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
+                        int* prop, int* moved_list, int* n_moved, unsigned long long* counters, int cap, int* status,
+                        const SweepCtl* ctl, int batch) {
+  gibbs_eval_body<Store::kHashed>(g, bm, verts, n, rng, sweep, prop, moved_list, n_moved, counters, cap, status, ctl,
+                                  batch);
 }
 
 

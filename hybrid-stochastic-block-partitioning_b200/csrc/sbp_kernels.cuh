@@ -34,9 +34,18 @@ __global__ void k_rebuild_degrees(BlockView bm);
 __global__ void k_mdl_cells(BlockView bm, double* partial);
 __global__ void k_mdl_edges(GraphView g, BlockView bm, const int* __restrict__ out_src, double* partial);
 __global__ void k_mdl_final(const double* partial, int n, int V, long long E, int B, double* out);
-__global__ void __launch_bounds__(256, 2) k_gibbs_eval(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng,
-                             int sweep, int* prop, int* moved_list, int* n_moved, unsigned long long* counters,
-                             int cap, int* status, const SweepCtl* ctl, int batch);
+// Asynchronous-Gibbs evaluation compiled for one storage of the block matrix.
+__global__ void __launch_bounds__(256, 2)
+    k_gibbs_eval_dense(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
+                       int* prop, int* moved_list, int* n_moved, unsigned long long* counters, int cap, int* status,
+                       const SweepCtl* ctl, int batch);
+__global__ void __launch_bounds__(256, 2)
+    k_gibbs_eval_hashed(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
+                        int* prop, int* moved_list, int* n_moved, unsigned long long* counters, int cap, int* status,
+                        const SweepCtl* ctl, int batch);
+using GibbsEvalKernel = void (*)(GraphView, BlockView, const int* __restrict__, int, RngParams, int, int*, int*, int*,
+                                 unsigned long long*, int, int*, const SweepCtl*, int);
+inline GibbsEvalKernel gibbs_eval_kernel(bool hashed) { return hashed ? k_gibbs_eval_hashed : k_gibbs_eval_dense; }
 __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, const int* n_moved, const int* prop,
                               int* qr, int* qs, unsigned long long* last, unsigned gen, const SweepCtl* ctl, int batch);
 __global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved, int* prop,

@@ -1034,19 +1034,20 @@ SbpStatus sbp_collect_moves(SbpBlockmodel* bm, const SbpGraph* cg, SbpDataset* d
       // plain evaluation (gibbs_batch without its apply), record, then apply
       const int nl = plan.light_n[bt], nh = plan.heavy_n[bt];
       int* n_cur = bm->n_moved.p + (bm->gen & 1);
+      const GibbsEvalKernel k_eval = gibbs_eval_kernel(bm->sparse);
       if (nl > 0) {
         const size_t smem = (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps;
-        set_smem_limit((const void*)k_gibbs_eval, smem);
-        k_gibbs_eval<<<grid_for(nl, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem, c.stream>>>(
+        set_smem_limit((const void*)k_eval, smem);
+        k_eval<<<grid_for(nl, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem, c.stream>>>(
             g.view(), bm->view(), plan.order.p + plan.light_begin[bt], nl, rng, it, bm->prop.p, bm->moved.p, n_cur,
             c.counters, g.light_cap, c.status, nullptr, 0);
         SBP_CHECK_LAUNCH();
       }
       if (nh > 0) {
         const size_t smem = (size_t)table_ints(g.heavy_cap) * sizeof(int);
-        set_smem_limit((const void*)k_gibbs_eval,
+        set_smem_limit((const void*)k_eval,
                        std::max(smem, (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps));
-        k_gibbs_eval<<<grid_for(nh, 1, 64 * c.num_sms), 32, smem, c.stream>>>(
+        k_eval<<<grid_for(nh, 1, 64 * c.num_sms), 32, smem, c.stream>>>(
             g.view(), bm->view(), plan.order.p + plan.heavy_begin[bt], nh, rng, it, bm->prop.p, bm->moved.p, n_cur,
             c.counters, g.heavy_cap, c.status, nullptr, 0);
         SBP_CHECK_LAUNCH();
