@@ -49,7 +49,8 @@ static void rebuild_hashed_side(SbpBlockmodel& bm, long long E, unsigned long lo
     SBP_CHECK_LAUNCH();
   }
   exclusive_scan_u32(g_sort.rowcnt.p, g_sort.rowptr.p, B, g_sort.partial.p, c.num_sms, c.stream);
-  k_row_caps<<<grid_for(B, 256, 8 * c.num_sms), 256, 0, c.stream>>>(g_sort.rowcnt.p, B, g_sort.caps.p, mask.p);
+  k_row_caps<<<grid_for(B, 256, 8 * c.num_sms), 256, 0, c.stream>>>(g_sort.rowcnt.p, B, (unsigned)g_hashed_row_factor,
+                                                                   g_sort.caps.p, mask.p);
   exclusive_scan_u32(g_sort.caps.p, base.p, B, g_sort.partial.p, c.num_sms, c.stream);
   SBP_CHECK_LAUNCH();
   long long lastbase = 0;
@@ -879,6 +880,9 @@ SbpStatus sbp_set_option(const char* name, int64_t value) {
   if (n == "dense_max_blocks") {
     SBP_REQUIRE(value >= 1 && value <= (1 << 30), "dense_max_blocks out of range");
     g_dense_max_blocks = (int)value;
+  } else if (n == "hashed_row_factor") {
+    SBP_REQUIRE(value >= 2 && value <= 64, "hashed_row_factor must be in [2, 64]");
+    g_hashed_row_factor = (int)value;
   } else if (n == "graph_sweeps") {
     SBP_REQUIRE(value == 0 || value == 1, "graph_sweeps must be 0 or 1");
     g_graph_sweeps = (int)value;

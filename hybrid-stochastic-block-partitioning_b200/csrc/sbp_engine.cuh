@@ -242,7 +242,9 @@ constexpr size_t kSmemBudget = 200 * 1024;
 constexpr int kSmemRebuildMaxB = 100;
 
 // Blocks above which the block matrix is row-hashed instead of dense (sbp_set_option).
-inline int g_dense_max_blocks = 16384;
+inline int g_dense_max_blocks = 65536;
+// Hashed row capacity = power of two >= factor * (cells after a rebuild) + 4 * factor.
+inline int g_hashed_row_factor = 4;
 // 1: an asynchronous-Gibbs finetune on dense storage runs as one CUDA graph launch with the
 // sweep loop decided on the GPU; 0: one host-driven launch sequence per sweep (sbp_set_option).
 inline int g_graph_sweeps = 1;
@@ -400,6 +402,16 @@ struct SbpBlockmodel {
     Context& c = Context::get();
     B = nb;
     sparse = B > g_dense_max_blocks;
+    if (!sparse && B > 4096) {   // dense only while it takes at most 40 % of the free device memory
+      const double dense_bytes = 2.0 * (double)B * (double)(((B + kChunk - 1) / kChunk) * kChunk) * sizeof(int);
+      size_t free_b = 0, total_b = 0;
+      if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        const size_t have = M.n * sizeof(int) * 2;   // a buffer this blockmodel already holds counts as free
+        if (dense_bytes > 0.4 * (double)(free_b + have)) sparse = true;
+      } else {
+        cudaGetLastError();
+      }
+    }
     ld = ((B + kChunk - 1) / kChunk) * kChunk;
     nch = (B + kChunk - 1) / kChunk;
     if (sparse) {

@@ -69,7 +69,7 @@ __global__ void k_relabel(int* b, int V, const int* map);
 __global__ void k_edge_keys(GraphView g, const int* __restrict__ b, const int* __restrict__ out_src, int B,
                             unsigned long long* keys, unsigned long long* keysT);
 __global__ void k_unique_rows(const unsigned long long* __restrict__ ukeys, long long n, int B, unsigned* rowcnt);
-__global__ void k_row_caps(const unsigned* __restrict__ rowcnt, int B, unsigned* cap, int* mask);
+__global__ void k_row_caps(const unsigned* __restrict__ rowcnt, int B, unsigned factor, unsigned* cap, int* mask);
 __global__ void k_fill_empty(int2* slot, long long n);
 __global__ void k_fill_rows(const long long* __restrict__ rowptr, const unsigned long long* __restrict__ ukeys,
                             const long long* __restrict__ heads, long long nu, long long nedges, int B,

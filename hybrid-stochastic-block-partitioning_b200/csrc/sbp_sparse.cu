@@ -22,10 +22,11 @@ __global__ void k_unique_rows(const unsigned long long* __restrict__ ukeys, long
     atomicAdd(rowcnt + (ukeys[j] / (unsigned long long)B), 1u);
 }
 
-// Row capacity: a power of two with at least half free after the rebuild (room to grow).
-__global__ void k_row_caps(const unsigned* __restrict__ rowcnt, int B, unsigned* cap, int* mask) {
+// Row capacity: a power of two with at least three quarters free after the rebuild (room to
+// grow: at large B most moves add cells, and a full row forces a rebuild).
+__global__ void k_row_caps(const unsigned* __restrict__ rowcnt, int B, unsigned factor, unsigned* cap, int* mask) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < B; r += gridDim.x * blockDim.x) {
-    unsigned want = 2u * rowcnt[r] + 8u, c = 8u;
+    unsigned want = factor * rowcnt[r] + 4u * factor, c = 8u;
     while (c < want) c <<= 1;
     cap[r] = c;
     mask[r] = (int)c - 1;

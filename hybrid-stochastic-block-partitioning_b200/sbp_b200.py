@@ -208,7 +208,7 @@ def device_count():
 
 
 def set_option(name, value):
-    """Engine option, e.g. set_option("dense_max_blocks", 16384)."""
+    """Engine option, e.g. set_option("dense_max_blocks", 65536) (include/sbp_b200.h lists them)."""
     _check(load().sbp_set_option(name.encode(), int(value)))
 
 

@@ -67,7 +67,7 @@ def test_batched_fallback_rounds_are_identical(S):
             out_s, st_s = S.sbp.stochastic_block_partition(g, algorithm="async_gibbs", batches=8, seed=11)
             assert_same(out, st, out_s, st_s)
     finally:
-        S.set_option("dense_max_blocks", 16384)
+        S.set_option("dense_max_blocks", 65536)
 
 
 def test_batched_other_algorithms_fall_back(S):

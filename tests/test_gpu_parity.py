@@ -16,9 +16,9 @@ RTOL_MDL = 1e-9
 @pytest.fixture(params=["dense", "hashed"])
 def storage(request, S):
     """Run the test with dense B x B counts and again with the row-hashed block matrix."""
-    S.set_option("dense_max_blocks", 16384 if request.param == "dense" else 1)
+    S.set_option("dense_max_blocks", 65536 if request.param == "dense" else 1)
     yield request.param
-    S.set_option("dense_max_blocks", 16384)
+    S.set_option("dense_max_blocks", 65536)
 
 
 def pair(S, O, V, s, d, B, a):
@@ -234,6 +234,7 @@ def test_hashed_rows_grow_and_stay_exact(S, O):
     """Finetune from many tiny blocks on the row-hashed matrix: rows fill up as blocks grow,
     the storage is rebuilt with more room, and the chain stays bit-exact with the oracle."""
     S.set_option("dense_max_blocks", 1)
+    S.set_option("hashed_row_factor", 2)   # tight rows: overflows are frequent
     try:
         V, s, d, _ = random_graph(2000, 8, 61, kmin=6, kmax=60, w=0.8)
         a = random_assignment(V, 900, 61)
@@ -247,7 +248,8 @@ def test_hashed_rows_grow_and_stay_exact(S, O):
             total += st["overflow_rebuilds"]
         assert total > 0, "the test no longer drives the rows past their capacity"
     finally:
-        S.set_option("dense_max_blocks", 16384)
+        S.set_option("dense_max_blocks", 65536)
+        S.set_option("hashed_row_factor", 4)
 
 
 def _reference_runs():
