@@ -141,6 +141,20 @@ def reference_baseline(V, src, dst, truth, budget_s):
     return cpu_baseline_port(V, src, dst, truth, budget_s)
 
 
+def reduce_over_ranks(ms, count, device):
+    """Whole-job figures of a replica run: the slowest rank's time (max) and every rank's
+    units (sum).  One rank: unchanged."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(ms), float(count)
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(count)], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(c.item())
+
+
 def learned_vs_plain(S, O, dcsbm, np):
     """Time to final MDL, learned vs plain proposal, on the 200,000-vertex / 71-block DC-SBM.
 
@@ -312,15 +326,7 @@ def main():
     prof1 = S.profile_read()
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms, float(visits)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        tm = t[:1].clone()
-        torch.distributed.all_reduce(tm, op=torch.distributed.ReduceOp.MAX)
-        tv = t[1:].clone()
-        torch.distributed.all_reduce(tv, op=torch.distributed.ReduceOp.SUM)
-        ms_max, visits_all = float(tm.item()), float(tv.item())
-    else:
-        ms_max, visits_all = ms, float(visits)
+    ms_max, visits_all = reduce_over_ranks(ms, visits, "cuda")
     value = visits_all / (ms_max / 1e3)
 
     # end to end through the C ABI from host buffers (graph upload + partition + read back)
@@ -341,14 +347,7 @@ def main():
     e3.record(ext)
     barrier()
     pe1 = S.profile_read()
-    e2e_ms = e2.elapsed_time(e3)
-    if world > 1:
-        tt = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
-        tv = torch.tensor([float(ev)], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(tv, op=torch.distributed.ReduceOp.SUM)
-        ev = float(tv.item())
+    e2e_ms, ev = reduce_over_ranks(e2e_ms, ev, "cuda")
     e2e_value = ev / (e2e_ms / 1e3)
 
     # roofline of the vertex-evaluation kernel: one profiled partition, CUDA events per launch

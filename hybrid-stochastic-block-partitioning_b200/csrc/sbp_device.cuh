@@ -431,6 +431,7 @@ __device__ __forceinline__ void build_table(const GraphView& g, const BlockView&
 }
 
 struct EvalResult {
+  int t;          // block of the proposal's neighbour (-1: no neighbour, uniform proposal)
   int s;          // proposed block
   int accepted;   // 1 if accepted (s != r)
   double dS;      // delta MDL (0 when s == r)
@@ -589,6 +590,7 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
   res.H = 1.0;
   const int idx = k > 0 ? (int)scale32(x.x, k) : -1;
   const int tblk = gather_neighbour_blocks(g, bm, v, r, o0, k_out, i0, k, self, idx, t, lane, status);
+  res.t = k > 0 ? tblk : -1;
 
   int s;
   if (k == 0) {

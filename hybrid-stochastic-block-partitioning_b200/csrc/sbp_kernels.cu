@@ -236,9 +236,9 @@ __global__ void k_sweep_control(SweepCtl* ctl, const double* mdl, cudaGraphCondi
 __global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, int n, int start, RngParams rng,
                      int sweep, int cap, double* out, int* status) {
   extern __shared__ int smem[];
-  __shared__ int s_acc[32], s_moved[32];
+  __shared__ int s_acc[32], s_moved[32], s_r[32], s_s[32], s_t[32], s_commit[32];
   __shared__ double s_dS[32];
-  __shared__ int s_first, s_stop;
+  __shared__ int s_first, s_stop, s_upto;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int W = blockDim.x >> 5;
   WarpTable t = carve_table(smem, cap, warp);
@@ -267,17 +267,56 @@ __global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, i
       s_acc[warp] = (i < n) ? res.accepted : 0;
       s_moved[warp] = (i < n && res.s != r) ? 1 : 0;
       s_dS[warp] = res.dS;
+      s_r[warp] = r;
+      s_s[warp] = res.s;
+      s_t[warp] = res.t;
+      s_commit[warp] = 0;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
+      const int avail = min(W, n - pos);
       int first = -1;
-      for (int w = 0; w < W; ++w)
+      for (int w = 0; w < avail; ++w)
         if (s_acc[w]) { first = w; break; }
+      int upto = first >= 0 ? first + 1 : avail;
+      if (first >= 0) s_commit[first] = 1;
+      if (first >= 0 && !bm.sparse) {
+        // later vertices whose evaluation no commit of this round could have touched keep their
+        // result: a commit c changes cells in rows / columns r_c, s_c towards its neighbour
+        // blocks, and the degrees and d of r_c and s_c.  Vertex w read its neighbours' blocks
+        // (a neighbour that moved puts r_c among them), the row and column of its proposal's
+        // block t_w, cells towards r_w, s_w and its neighbour blocks, and their degrees.
+        int ncommit = 1;
+        int cw[32];
+        cw[0] = first;
+        for (int w = first + 1; w < avail; ++w) {
+          const WarpTable tw = carve_table(smem, cap, w);
+          bool indep = true;
+          for (int q = 0; q < ncommit && indep; ++q) {
+            const int c = cw[q];
+            const WarpTable tc = carve_table(smem, cap, c);
+            const int rc = s_r[c], sc = s_s[c];
+            const int rw = s_r[w], sw = s_s[w], tb = s_t[w];
+            if (rc == rw || rc == sw || rc == tb || sc == rw || sc == sw || sc == tb) indep = false;
+            else if (table_find(tw, rc) >= 0 || table_find(tw, sc) >= 0) indep = false;
+            else if ((tb >= 0 && table_find(tc, tb) >= 0) || table_find(tc, rw) >= 0 || table_find(tc, sw) >= 0)
+              indep = false;
+          }
+          if (!indep) break;
+          upto = w + 1;
+          if (s_acc[w]) {
+            s_commit[w] = 1;
+            cw[ncommit++] = w;
+          }
+        }
+      }
       s_first = first;
+      s_upto = upto;
     }
     __syncthreads();
     const int first = s_first;
-    if (first == warp) {
+    const int upto_round = s_upto;
+    if (s_commit[warp]) {
       // apply the move of v from r to s with the counts still in this warp's table; lanes own
       // distinct non-corner cells, lane 0 owns the four corner cells (r,r) (r,s) (s,r) (s,s)
       const int s = res.s;
@@ -327,15 +366,16 @@ __global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, i
       }
     }
     if (threadIdx.x == 0) {
-      const int upto = first >= 0 ? first + 1 : min(W, n - pos);
-      for (int w = 0; w < upto; ++w) moved += s_moved[w];
-      visits += upto;
-      if (first >= 0) {
-        accepted++;
-        sum_dS += s_dS[first];
+      for (int w = 0; w < upto_round; ++w) {
+        moved += s_moved[w];
+        if (s_commit[w]) {   // accepted moves in vertex order
+          accepted++;
+          sum_dS += s_dS[w];
+        }
       }
+      visits += upto_round;
     }
-    pos += first >= 0 ? first + 1 : W;
+    pos += upto_round;
     table_reset(t, lane);
     __syncthreads();
     if (s_stop) break;
