@@ -347,7 +347,7 @@ def main():
     e3.record(ext)
     barrier()
     pe1 = S.profile_read()
-    e2e_ms, ev = reduce_over_ranks(e2e_ms, ev, "cuda")
+    e2e_ms, ev = reduce_over_ranks(e2.elapsed_time(e3), ev, "cuda")
     e2e_value = ev / (e2e_ms / 1e3)
 
     # roofline of the vertex-evaluation kernel: one profiled partition, CUDA events per launch
