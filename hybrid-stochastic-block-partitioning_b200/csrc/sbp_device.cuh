@@ -88,6 +88,32 @@ __device__ __forceinline__ double dxlogx(double a, double b) {
   return (a - b) * log(sa) + b * log1p((sa - sb) / sb);
 }
 
+// g(a) - g(b) for integer counts a, b >= 0 as (a - b) log a + b log(a / b), from a table of
+// log(x) = hi + lo (lo carries the bits below hi's last place):
+//  - a close to b (128 |a - b| <= b): log(a / b) = 2 atanh(z), z = (a - b) / (a + b), by its
+//    Taylor series 2 (z + z^3/3 + z^5/5 + z^7/7), |z| <= 1/255, which keeps the relative
+//    accuracy that a difference of two table logs would lose;
+//  - otherwise log(a / b) = (hi_a - hi_b) + (lo_a - lo_b).
+// A zero side uses log 1 = 0, which leaves the other side's g term.  Counts beyond the table
+// go through dxlogx.
+constexpr int kLogTable = 1 << 20;
+__device__ __forceinline__ double dxlogx_int(const double2* __restrict__ logt, int a, int b) {
+  if (a < kLogTable && b < kLogTable) {
+    const int d = a - b;
+    const double2 la = __ldg(logt + (a > 0 ? a : 1));
+    double lab;
+    if (128LL * (d < 0 ? -(long long)d : (long long)d) <= (long long)b) {
+      const double z = (double)d / ((double)a + (double)b), w = z * z;
+      lab = 2.0 * z + 2.0 * z * w * (1.0 / 3.0 + w * (1.0 / 5.0 + w * (1.0 / 7.0)));
+    } else {
+      const double2 lb = __ldg(logt + (b > 0 ? b : 1));
+      lab = (la.x - lb.x) + (la.y - lb.y);
+    }
+    return (double)d * (la.x + la.y) + (double)b * lab;
+  }
+  return dxlogx((double)a, (double)b);
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
@@ -113,6 +139,7 @@ __device__ __forceinline__ long long warp_incl_scan(long long v, int lane) {
 struct GraphView {
   int V;
   long long E;
+  double log_E;           // log(max(E, 2)), the zero-snap scale of a delta-MDL
   const int* out_ptr;     // [V+1]
   const int* out_idx;     // out-neighbours incl. self loop, first-occurrence order
   const int* in_ptr;      // [V+1]
@@ -145,6 +172,7 @@ struct BlockView {
   int* d_out;             // [B]
   int* d_in;              // [B]
   int* d;                 // [B] block degrees as the reference maintains them
+  const double2* logt;    // [kLogTable] log(x) = hi + lo for integer x (entry 0 unused)
 };
 
 // Walk values row[0..n) ascending and return the first index whose running sum exceeds
@@ -493,11 +521,31 @@ __device__ __forceinline__ int gather_neighbour_blocks(const GraphView& g, const
   return tblk;
 }
 
+// Position of the n-th (0-based) set bit of m; requires n < popc(m).
+__device__ __forceinline__ int nth_set_bit(unsigned m, int n) {
+  int pos = 0;
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) {
+    const int c = __popc(m & ((1u << w) - 1u));
+    if (n >= c) {
+      n -= c;
+      m >>= w;
+      pos += w;
+    }
+  }
+  return pos;
+}
+
 // Delta-MDL of moving v from r to s (s != r) against the current state, with the gathered
-// table of v's neighbour blocks, and the reference's Hastings correction (*H).  One load round
-// over the distinct neighbour blocks gives the Hastings sums and the changed cells; the corner
-// cells, degree terms and the net-zero double count are spread over lanes.  Every lane
-// returns the same values.
+// table of v's neighbour blocks, and the reference's Hastings correction (*H).
+//  - One load round over the distinct neighbour blocks (lane i: table entries i, i+32, ...)
+//    gives the Hastings sums and the changed cells.
+//  - The FP64 terms are then spread over the warp one term per lane: the eight corner-cell
+//    and degree terms, and two cells per (neighbour block, direction) pair that changes:
+//    (r,u) and (s,u) for v's out-edges to u, (u,r) and (u,s) for its in-edges from u.
+//  - The double count of a present net-zero (r,s) / (s,r) Delta cell is added by the lanes
+//    that hold it, and only then.
+// Every lane returns the same values.
 template <Store ST = Store::kAny>
 __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView& bm, int r, int s, int k_out,
                                              int k_in, int self, const WarpTable& t, int lane, double* H) {
@@ -516,43 +564,81 @@ __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView
   double fwd = 0.0, bwd = 0.0, dS = 0.0;
   long long T = 0;   // integer scale of the changed cells and degrees (zero snap below)
   const int n = *t.nlist;
-  for (int i = lane; i < n; i += kWarp) {
-    const int h = t.list[i];
-    const int u = t.keys[h];
-    const int co = t.cout[h], ci = t.cin[h];
-    const int M_su = bm_get<ST>(bm, s, u), M_us = bm_getT<ST>(bm, s, u), M_ru = bm_get<ST>(bm, r, u), M_ur = bm_getT<ST>(bm, r, u);
-    const int du = bm.d[u];
-    const bool is_r = (u == r), is_s = (u == s), corner = is_r || is_s;
-    const double c = (double)(co + ci + (is_r ? self : 0));
-    fwd += c * (M_su + M_us + 1.0) / ((double)du + (double)B);
-    const double bw = is_r ? (double)(M_rr + d_rr) + (double)(M_rr + d_rr) + 1.0
-                    : is_s ? (double)(M_rs + d_rs) + (double)(M_sr + d_sr) + 1.0
-                           : (double)(M_ru - co) + (double)(M_ur - ci) + 1.0;
-    const int nd = is_r ? (dout_r - k_out) + (din_r - k_in) - (M_rr + d_rr)
-                 : is_s ? (dout_s + k_out) + (din_s + k_in) - (M_ss + d_ss) : du;
-    bwd += c * bw / ((double)nd + (double)B);
-    // changed non-corner cells (r,u) (s,u) (u,r) (u,s); corner cells are handled below
-    const int co_c = corner ? 0 : co, ci_c = corner ? 0 : ci;
-    dS += dxlogx(M_ru, M_ru - co_c) + dxlogx(M_su, M_su + co_c) + dxlogx(M_ur, M_ur - ci_c) +
-          dxlogx(M_us, M_us + ci_c);
-    T += (co_c ? 2LL * (M_ru + M_su) : 0LL) + (ci_c ? 2LL * (M_ur + M_us) : 0LL);
+  for (int base = 0; base < n; base += kWarp) {
+    const int i = base + lane;
+    int M_su = 0, M_us = 0, M_ru = 0, M_ur = 0, co_c = 0, ci_c = 0;
+    if (i < n) {
+      const int h = t.list[i];
+      const int u = t.keys[h];
+      const int co = t.cout[h], ci = t.cin[h];
+      M_su = bm_get<ST>(bm, s, u);
+      M_us = bm_getT<ST>(bm, s, u);
+      M_ru = bm_get<ST>(bm, r, u);
+      M_ur = bm_getT<ST>(bm, r, u);
+      const int du = bm.d[u];
+      const bool is_r = (u == r), is_s = (u == s), corner = is_r || is_s;
+      const double c = (double)(co + ci + (is_r ? self : 0));
+      fwd += c * (M_su + M_us + 1.0) / ((double)du + (double)B);
+      const double bw = is_r ? (double)(M_rr + d_rr) + (double)(M_rr + d_rr) + 1.0
+                      : is_s ? (double)(M_rs + d_rs) + (double)(M_sr + d_sr) + 1.0
+                             : (double)(M_ru - co) + (double)(M_ur - ci) + 1.0;
+      const int nd = is_r ? (dout_r - k_out) + (din_r - k_in) - (M_rr + d_rr)
+                   : is_s ? (dout_s + k_out) + (din_s + k_in) - (M_ss + d_ss) : du;
+      bwd += c * bw / ((double)nd + (double)B);
+      // changed non-corner cells (r,u) (s,u) (u,r) (u,s); corner cells are terms 0-3 below
+      co_c = corner ? 0 : co;
+      ci_c = corner ? 0 : ci;
+      T += (co_c ? 2LL * (M_ru + M_su) : 0LL) + (ci_c ? 2LL * (M_ur + M_us) : 0LL);
+    }
+    const unsigned m_out = __ballot_sync(kFull, co_c != 0), m_in = __ballot_sync(kFull, ci_c != 0);
+    const int n_out = __popc(m_out), n_terms_cells = 2 * (n_out + __popc(m_in));
+    const int extra = base == 0 ? 8 : 0;   // corner-cell and degree terms, once
+    const int n_terms = extra + n_terms_cells;
+    for (int q0 = 0; q0 < n_terms; q0 += kWarp) {
+      const int q = q0 + lane;
+      const int cell = q - extra;
+      const int pair = cell >> 1;
+      const bool is_cell = q >= extra && q < n_terms;
+      const bool out_pair = pair < n_out;
+      const int owner = !is_cell ? lane : out_pair ? nth_set_bit(m_out, pair) : nth_set_bit(m_in, pair - n_out);
+      const int x_ru = __shfl_sync(kFull, M_ru, owner), x_su = __shfl_sync(kFull, M_su, owner);
+      const int x_ur = __shfl_sync(kFull, M_ur, owner), x_us = __shfl_sync(kFull, M_us, owner);
+      const int x_co = __shfl_sync(kFull, co_c, owner), x_ci = __shfl_sync(kFull, ci_c, owner);
+      int a = 0, d = 0;
+      double sign = 1.0;
+      if (is_cell) {
+        const bool s_side = cell & 1;
+        a = out_pair ? (s_side ? x_su : x_ru) : (s_side ? x_us : x_ur);
+        const int m = out_pair ? x_co : x_ci;
+        d = s_side ? m : -m;
+      } else if (q < extra) {
+        // corner cells (r,r) (r,s) (s,r) (s,s), then the out- and in-degrees of r and s
+        a = q == 0 ? M_rr : q == 1 ? M_rs : q == 2 ? M_sr : q == 3 ? M_ss
+          : q == 4 ? dout_r : q == 5 ? dout_s : q == 6 ? din_r : din_s;
+        d = q == 0 ? d_rr : q == 1 ? d_rs : q == 2 ? d_sr : q == 3 ? d_ss
+          : q == 4 ? -k_out : q == 5 ? k_out : q == 6 ? -kin_self : kin_self;
+        sign = q < 4 ? 1.0 : -1.0;
+      }
+      if (d) dS += sign * dxlogx_int(bm.logt, a, a + d);
+    }
+  }
+  if (lane < 8) {
+    const int ca = lane == 0 ? M_rr : lane == 1 ? M_rs : lane == 2 ? M_sr : lane == 3 ? M_ss
+                 : lane == 4 ? dout_r : lane == 5 ? dout_s : lane == 6 ? din_r : din_s;
+    const int cd = lane == 0 ? d_rr : lane == 1 ? d_rs : lane == 2 ? d_sr : lane == 3 ? d_ss
+                 : lane == 4 ? -k_out : lane == 5 ? k_out : lane == 6 ? -kin_self : kin_self;
+    T += lane < 4 ? (cd ? 2LL * ca + cd : 0LL) : 2LL * ca;
   }
   {
-    // one corner-cell or degree term per lane (lanes 0-7), the double count of a present
-    // net-zero (r,s) / (s,r) Delta cell on lanes 8 and 9; selects, no divergent branches
-    const int ca = lane == 0 ? M_rr : lane == 1 ? M_rs : lane == 2 ? M_sr : lane == 3 ? M_ss
-                 : lane == 4 ? dout_r : lane == 5 ? dout_s : lane == 6 ? din_r : lane == 7 ? din_s : 0;
-    const int cd = lane == 0 ? d_rr : lane == 1 ? d_rs : lane == 2 ? d_sr : lane == 3 ? d_ss
-                 : lane == 4 ? -k_out : lane == 5 ? k_out : lane == 6 ? -kin_self : lane == 7 ? kin_self : 0;
-    const double sign = lane < 4 ? 1.0 : -1.0;
-    dS += sign * dxlogx((double)ca, (double)(ca + cd));
-    T += lane < 4 ? (cd ? 2LL * ca + cd : 0LL) : 2LL * ca;
+    // the double count of a present net-zero (r,s) / (s,r) Delta cell (lanes 8 and 9)
     const bool q_rs = (mc.co_s > 0 || mc.ci_r > 0) && d_rs == 0 && M_rs > 0;
     const bool q_sr = (mc.co_r > 0 || mc.ci_s > 0) && d_sr == 0 && M_sr > 0;
     const int qm = lane == 8 ? (q_rs ? M_rs : 0) : lane == 9 ? (q_sr ? M_sr : 0) : 0;
-    const double x1 = qm ? (lane == 8 ? (double)kin_self / (double)din_s : -(double)kin_self / (double)din_r) : 0.0;
-    const double x2 = qm ? (lane == 8 ? -(double)k_out / (double)dout_r : (double)k_out / (double)dout_s) : 0.0;
-    dS += (double)qm * (log1p(x1) + log1p(x2));
+    if (qm) {
+      const double x1 = lane == 8 ? (double)kin_self / (double)din_s : -(double)kin_self / (double)din_r;
+      const double x2 = lane == 8 ? -(double)k_out / (double)dout_r : (double)k_out / (double)dout_s;
+      dS += (double)qm * (log1p(x1) + log1p(x2));
+    }
   }
   fwd = warp_sum(fwd);
   bwd = warp_sum(bwd);
@@ -561,7 +647,7 @@ __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView
   for (int o = 16; o > 0; o >>= 1) T += __shfl_xor_sync(kFull, T, o);
   // A mathematically zero change reads as exactly 0 whatever the summation order: the
   // Metropolis-Hastings early stop tests `delta == 0.0` (src/finetune.cpp:147).
-  if (fabs(dS) <= 0x1p-40 * (double)T * log(g.E > 2 ? (double)g.E : 2.0)) dS = 0.0;
+  if (fabs(dS) <= 0x1p-40 * (double)T * g.log_E) dS = 0.0;
   *H = bwd / fwd;
   return dS;
 }

@@ -12,6 +12,7 @@
 #include <numeric>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -57,6 +58,19 @@ inline cudaError_t count_copy(cudaError_t e, size_t bytes, cudaMemcpyKind kind) 
 #define SBP_COPY(dst, src, bytes, kind) count_copy(cudaMemcpy(dst, src, bytes, kind), bytes, kind)
 #define SBP_COPY_ASYNC(dst, src, bytes, kind, stream) \
   count_copy(cudaMemcpyAsync(dst, src, bytes, kind, stream), bytes, kind)
+
+// Total memory of the current device, asked once.
+inline size_t device_memory_bytes() {
+  static size_t total = [] {
+    size_t f = 0, t = 0;
+    if (cudaMemGetInfo(&f, &t) != cudaSuccess) {
+      cudaGetLastError();
+      t = 0;
+    }
+    return t;
+  }();
+  return total;
+}
 
 // Released device buffers are kept for reuse instead of being freed: cudaFree synchronizes
 // the whole device, and every partition round releases and reallocates its blockmodel's
@@ -134,6 +148,29 @@ struct DevBuf {
 // ------------------------------------------------------------------------------------------
 // Process-wide context: one stream, the device status word, counters and readback buffers.
 // ------------------------------------------------------------------------------------------
+// log(x) for the integers 1 <= x < kLogTable as a pair of doubles (hi = log x rounded, lo = the
+// rest), from the host's long-double log (64-bit mantissa): the vertex-move delta-MDL takes
+// g(a) - g(b), g(x) = x log x, of integer counts from it (dxlogx_int in sbp_device.cuh).
+inline double2* make_log_table() {
+  std::vector<double2> h(kLogTable);
+  h[0] = make_double2(0.0, 0.0);
+  const int nt = 8;
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; ++t)
+    th.emplace_back([&h, t, nt] {
+      for (int x = 1 + t; x < kLogTable; x += nt) {
+        const long double l = logl((long double)x);
+        const double hi = (double)l;
+        h[x] = make_double2(hi, (double)(l - (long double)hi));
+      }
+    });
+  for (auto& t : th) t.join();
+  double2* d = nullptr;
+  SBP_CUDA(cudaMalloc(&d, sizeof(double2) * kLogTable));
+  SBP_CUDA(cudaMemcpy(d, h.data(), sizeof(double2) * kLogTable, cudaMemcpyHostToDevice));
+  return d;
+}
+
 struct Context {
   cudaStream_t stream = nullptr;
   int num_sms = 0;
@@ -142,6 +179,7 @@ struct Context {
   double* partial = nullptr;             // MDL partial sums
   double* scalar = nullptr;              // MDL result
   double* mh_out = nullptr;              // MH sweep outputs [4]
+  double2* logt = nullptr;               // [kLogTable] log(x) as hi + lo doubles (entry 0 unused)
   int npartial = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
@@ -167,6 +205,7 @@ struct Context {
       SBP_CUDA(cudaMemset(c->status, 0, 8 * sizeof(int)));
       SBP_CUDA(cudaEventCreate(&c->ev0));
       SBP_CUDA(cudaEventCreate(&c->ev1));
+      c->logt = make_log_table();
       ctx = c;
     }
     return *ctx;
@@ -280,6 +319,7 @@ struct SbpGraph {
     GraphView g;
     g.V = V;
     g.E = E;
+    g.log_E = std::log(E > 2 ? (double)E : 2.0);
     g.out_ptr = out_ptr.p;
     g.out_idx = out_idx.p;
     g.in_ptr = in_ptr.p;
@@ -379,6 +419,7 @@ struct SbpBlockmodel {
     v.d_out = d_out.p;
     v.d_in = d_in.p;
     v.d = d.p;
+    v.logt = Context::get().logt;
     return v;
   }
 
@@ -402,8 +443,11 @@ struct SbpBlockmodel {
     Context& c = Context::get();
     B = nb;
     sparse = B > g_dense_max_blocks;
-    if (!sparse && B > 4096) {   // dense only while it takes at most 40 % of the free device memory
-      const double dense_bytes = 2.0 * (double)B * (double)(((B + kChunk - 1) / kChunk) * kChunk) * sizeof(int);
+    const double dense_bytes = 2.0 * (double)B * (double)(((B + kChunk - 1) / kChunk) * kChunk) * sizeof(int);
+    // dense only while it takes at most 40 % of the free device memory; cudaMemGetInfo can
+    // stall the host for tens of milliseconds, so it is asked only for a matrix above 5 % of
+    // the device's memory
+    if (!sparse && dense_bytes > 0.05 * (double)device_memory_bytes()) {
       size_t free_b = 0, total_b = 0;
       if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
         const size_t have = M.n * sizeof(int) * 2;   // a buffer this blockmodel already holds counts as free
