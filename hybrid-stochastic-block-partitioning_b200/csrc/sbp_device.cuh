@@ -154,7 +154,8 @@ struct BlockView {
   int sparse;             // 0: dense M/MT below; 1: row-hashed regions (large B)
   // row-hashed storage: row r of M lives in rslot[rbase[r] .. rbase[r] + rmask[r]], slots
   // (col, count), col = -1 for an empty slot; MT likewise in cslot.  Keys are never removed
-  // (a count can drop to 0).  An insertion that finds its row full sets *overflow.
+  // (a count can drop to 0).  An insertion that finds its row full sets overflow[0] and the
+  // row's flag: overflow[1 + row] for a row of M, overflow[1 + B + row] for a row of MT.
   const long long* rbase;
   const int* rmask;
   int2* rslot;
@@ -211,7 +212,7 @@ __device__ __forceinline__ int hashed_get(const long long* base, const int* mask
 }
 
 __device__ __forceinline__ void hashed_add(const long long* base, const int* mask, int2* slot, int row, int col,
-                                           int delta, int* overflow) {
+                                           int delta, int* overflow, int* row_full) {
   const long long b0 = base[row];
   const int m = mask[row];
   unsigned h = slot_hash(col) & (unsigned)m;
@@ -229,6 +230,7 @@ __device__ __forceinline__ void hashed_add(const long long* base, const int* mas
     h = (h + 1) & (unsigned)m;
   }
   atomicOr(overflow, 1);
+  row_full[row] = 1;
 }
 
 // M[row, col] and MT[row, col] = M[col, row] in either representation.
@@ -249,34 +251,40 @@ __device__ __forceinline__ int bm_getT(const BlockView& bm, int row, int col) {
   else return bm.sparse ? hashed_get(bm.cbase, bm.cmask, bm.cslot, row, col) : bm.MT[(size_t)row * bm.ld + col];
 }
 
-// Walk of a hashed row in ascending column order: bisection over the column space for the
-// first column whose running count exceeds `target`.  Same result as the dense walks.
+// Walk of a hashed row in ascending column order: the first column whose running count
+// exceeds `target`, found digit by digit (4 bits of the column at a time, most significant
+// first).  Each pass sums the row's counts of the columns left in range into 16 bins (`bins`:
+// 16 ints of the warp's shared memory), scans the bins and keeps the one that holds the target.
+// Same result as the dense walks.
 __device__ __forceinline__ int warp_select_hashed(const long long* base, const int* mask, const int2* slot, int row,
-                                                  int B, long long target, int lane) {
+                                                  int B, long long target, int lane, int* bins) {
   const long long b0 = base[row];
   const int cap = mask[row] + 1;
-  int lo = 0, hi = B - 1;
-  while (lo < hi) {
-    const int mid = lo + ((hi - lo) >> 1);
-    long long cnt = 0;
+  int bits = 0;
+  while ((1 << bits) < B) ++bits;
+  int lo = 0;
+  for (int shift = ((bits + 3) / 4) * 4 - 4; shift >= 0; shift -= 4) {
+    if (lane < 16) bins[lane] = 0;
+    __syncwarp();
+    const long long span = 16LL << shift;
     for (int i = lane; i < cap; i += kWarp) {
       const int2 e = slot[b0 + i];
-      if (e.x >= 0 && e.x <= mid) cnt += e.y;
+      if (e.x >= lo && (long long)e.x < lo + span && e.y > 0) atomicAdd(&bins[(e.x - lo) >> shift], e.y);
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFull, cnt, o);
-    if (cnt > target) hi = mid;
-    else lo = mid + 1;
+    __syncwarp();
+    const long long v = lane < 16 ? (long long)bins[lane] : 0;
+    const long long incl = warp_incl_scan(v, lane);
+    const unsigned hit = __ballot_sync(kFull, lane < 16 && incl > target);
+    if (!hit) return -1;
+    const int sel = __ffs(hit) - 1;
+    target -= __shfl_sync(kFull, incl - v, sel);
+    lo += sel << shift;
+    __syncwarp();
   }
-  long long cnt = 0;
-  for (int i = lane; i < cap; i += kWarp) {
-    const int2 e = slot[b0 + i];
-    if (e.x >= 0 && e.x <= lo) cnt += e.y;
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFull, cnt, o);
-  return cnt > target ? lo : -1;
+  return lo;
 }
+
+__device__ __forceinline__ int select_in_chunk(int4 q, int chunk, long long target, int lane);
 
 // Two-level walk: find the chunk through the chunk sums, then the column inside the chunk
 // with one 16-byte load per lane.  Same result as warp_select_dense on the full row.
@@ -299,6 +307,12 @@ __device__ __forceinline__ int warp_select_chunked(const int* row, const int* cs
   }
   if (chunk < 0) return -1;
   const int4 q = *reinterpret_cast<const int4*>(row + chunk * kChunk + 4 * lane);
+  return select_in_chunk(q, chunk, target, lane);
+}
+
+// The column inside one chunk of kChunk counts (four per lane, q) at which the running sum
+// first exceeds target; -1 if the chunk is exhausted.
+__device__ __forceinline__ int select_in_chunk(int4 q, int chunk, long long target, int lane) {
   const long long lsum = (long long)q.x + q.y + q.z + q.w;
   const long long incl = warp_incl_scan(lsum, lane);
   const unsigned hit = __ballot_sync(kFull, incl > target);
@@ -311,6 +325,20 @@ __device__ __forceinline__ int warp_select_chunked(const int* row, const int* cs
   else if (t < (long long)qx + qy) k = 1;
   else if (t < (long long)qx + qy + qz) k = 2;
   return chunk * kChunk + 4 * src + k;
+}
+
+// The walk of warp_select_chunked for a row of at most 32 chunks whose chunk sums are already
+// loaded (lane c holds chunk c's sum, 0 beyond the row).
+__device__ __forceinline__ int select_chunk_then_column(const int* row, int csum_lane, long long target, int lane) {
+  const long long v = csum_lane;
+  const long long incl = warp_incl_scan(v, lane);
+  const long long tot = __shfl_sync(kFull, incl, 31);
+  if (target >= tot) return -1;
+  const unsigned hit = __ballot_sync(kFull, incl > target);
+  const int src = __ffs(hit) - 1;
+  target -= __shfl_sync(kFull, incl - v, src);
+  const int4 q = *reinterpret_cast<const int4*>(row + src * kChunk + 4 * lane);
+  return select_in_chunk(q, src, target, lane);
 }
 
 __device__ __forceinline__ void chunk_add(int* cs, int nch, int row, int col, int delta) {
@@ -521,6 +549,34 @@ __device__ __forceinline__ int gather_neighbour_blocks(const GraphView& g, const
   return tblk;
 }
 
+// Loads of move_delta that do not depend on the proposed block s: issued right after the
+// neighbour table is built, so that they overlap the multinomial walk that picks s.
+struct NbPrefetch {
+  int u, co, ci, M_ru, M_ur, du;   // this lane's first table entry (u = -1: none)
+  int M_rr, dout_r, din_r;
+};
+
+template <Store ST = Store::kAny>
+__device__ __forceinline__ void prefetch_nb(const BlockView& bm, int r, const WarpTable& t, int lane, NbPrefetch* p) {
+  __syncwarp();
+  const int n = *t.nlist;
+  p->u = -1;
+  p->co = p->ci = p->M_ru = p->M_ur = p->du = 0;
+  if (lane < n) {
+    const int h = t.list[lane];
+    const int u = t.keys[h];
+    p->u = u;
+    p->co = t.cout[h];
+    p->ci = t.cin[h];
+    p->M_ru = bm_get<ST>(bm, r, u);
+    p->M_ur = bm_getT<ST>(bm, r, u);
+    p->du = bm.d[u];
+  }
+  p->M_rr = bm_get<ST>(bm, r, r);
+  p->dout_r = bm.d_out[r];
+  p->din_r = bm.d_in[r];
+}
+
 // Position of the n-th (0-based) set bit of m; requires n < popc(m).
 __device__ __forceinline__ int nth_set_bit(unsigned m, int n) {
   int pos = 0;
@@ -548,7 +604,8 @@ __device__ __forceinline__ int nth_set_bit(unsigned m, int n) {
 // Every lane returns the same values.
 template <Store ST = Store::kAny>
 __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView& bm, int r, int s, int k_out,
-                                             int k_in, int self, const WarpTable& t, int lane, double* H) {
+                                             int k_in, int self, const WarpTable& t, int lane, double* H,
+                                             const NbPrefetch* pre = nullptr) {
   __syncwarp();
   const MoveCounts mc = corner_counts(t, r, s);
   const int B = bm.B;
@@ -556,9 +613,10 @@ __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView
   const int d_rs = -mc.co_s + mc.ci_r;
   const int d_sr = mc.co_r - mc.ci_s;
   const int d_ss = mc.co_s + mc.ci_s + self;
-  const int M_rr = bm_get<ST>(bm, r, r), M_rs = bm_get<ST>(bm, r, s);
+  const int M_rr = pre ? pre->M_rr : bm_get<ST>(bm, r, r), M_rs = bm_get<ST>(bm, r, s);
   const int M_sr = bm_get<ST>(bm, s, r), M_ss = bm_get<ST>(bm, s, s);
-  const int dout_r = bm.d_out[r], dout_s = bm.d_out[s], din_r = bm.d_in[r], din_s = bm.d_in[s];
+  const int dout_r = pre ? pre->dout_r : bm.d_out[r], dout_s = bm.d_out[s];
+  const int din_r = pre ? pre->din_r : bm.d_in[r], din_s = bm.d_in[s];
   const int kin_self = k_in + self;
 
   double fwd = 0.0, bwd = 0.0, dS = 0.0;
@@ -568,14 +626,25 @@ __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView
     const int i = base + lane;
     int M_su = 0, M_us = 0, M_ru = 0, M_ur = 0, co_c = 0, ci_c = 0;
     if (i < n) {
-      const int h = t.list[i];
-      const int u = t.keys[h];
-      const int co = t.cout[h], ci = t.cin[h];
+      int u, co, ci, du;
+      if (pre && base == 0) {
+        u = pre->u;
+        co = pre->co;
+        ci = pre->ci;
+        M_ru = pre->M_ru;
+        M_ur = pre->M_ur;
+        du = pre->du;
+      } else {
+        const int h = t.list[i];
+        u = t.keys[h];
+        co = t.cout[h];
+        ci = t.cin[h];
+        M_ru = bm_get<ST>(bm, r, u);
+        M_ur = bm_getT<ST>(bm, r, u);
+        du = bm.d[u];
+      }
       M_su = bm_get<ST>(bm, s, u);
       M_us = bm_getT<ST>(bm, s, u);
-      M_ru = bm_get<ST>(bm, r, u);
-      M_ur = bm_getT<ST>(bm, r, u);
-      const int du = bm.d[u];
       const bool is_r = (u == r), is_s = (u == s), corner = is_r || is_s;
       const double c = (double)(co + ci + (is_r ? self : 0));
       fwd += c * (M_su + M_us + 1.0) / ((double)du + (double)B);
@@ -678,22 +747,41 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
   const int tblk = gather_neighbour_blocks(g, bm, v, r, o0, k_out, i0, k, self, idx, t, lane, status);
   res.t = k > 0 ? tblk : -1;
 
+  NbPrefetch pre;
+  prefetch_nb<ST>(bm, r, t, lane, &pre);
+
   int s;
   if (k == 0) {
     s = random_block(r, bm.B, x.y);
   } else {
-    const int dot = bm.d_out[tblk];
-    const long long total = (long long)dot + (long long)bm.d_in[tblk];
-    const long long target = scale32(x.y, total);
     const bool hashed = ST == Store::kHashed || (ST == Store::kAny && bm.sparse);
     if (ST != Store::kDense && hashed) {
-      if (target < dot) s = warp_select_hashed(bm.rbase, bm.rmask, bm.rslot, tblk, bm.B, target, lane);
-      else s = warp_select_hashed(bm.cbase, bm.cmask, bm.cslot, tblk, bm.B, target - dot, lane);
-    } else if (ST != Store::kHashed && target < dot) {
-      s = warp_select_chunked(bm.M + (size_t)tblk * bm.ld, bm.CS + (size_t)tblk * bm.nch, bm.nch, target, lane);
+      const int dot = bm.d_out[tblk];
+      const long long target = scale32(x.y, (long long)dot + (long long)bm.d_in[tblk]);
+      int* bins = t.nlist + 16;   // spare ints after the table's list count
+      if (target < dot) s = warp_select_hashed(bm.rbase, bm.rmask, bm.rslot, tblk, bm.B, target, lane, bins);
+      else s = warp_select_hashed(bm.cbase, bm.cmask, bm.cslot, tblk, bm.B, target - dot, lane, bins);
     } else if (ST != Store::kHashed) {
-      s = warp_select_chunked(bm.MT + (size_t)tblk * bm.ld, bm.CST + (size_t)tblk * bm.nch, bm.nch, target - dot,
-                              lane);
+      // the degrees of t and, in the same round trip, row t of M and of MT (B <= kChunk: the
+      // whole rows, four counts per lane) or their chunk sums (up to 32 chunks); the walk then
+      // picks the row (target < d_out[t]) or the column
+      const int dot = bm.d_out[tblk], dit = bm.d_in[tblk];
+      const size_t ro = (size_t)tblk * bm.ld, co = (size_t)tblk * bm.nch;
+      int4 qa = make_int4(0, 0, 0, 0), qb = make_int4(0, 0, 0, 0);
+      int ca = 0, cb = 0;
+      if (bm.nch == 1) {
+        qa = *reinterpret_cast<const int4*>(bm.M + ro + 4 * lane);
+        qb = *reinterpret_cast<const int4*>(bm.MT + ro + 4 * lane);
+      } else if (lane < bm.nch) {
+        ca = bm.CS[co + lane];
+        cb = bm.CST[co + lane];
+      }
+      const long long target = scale32(x.y, (long long)dot + (long long)dit);
+      const bool in_row = target < dot;
+      const long long tg = in_row ? target : target - dot;
+      if (bm.nch == 1) s = select_in_chunk(in_row ? qa : qb, 0, tg, lane);
+      else if (bm.nch <= kWarp) s = select_chunk_then_column(in_row ? bm.M + ro : bm.MT + ro, in_row ? ca : cb, tg, lane);
+      else s = warp_select_chunked(in_row ? bm.M + ro : bm.MT + ro, in_row ? bm.CS + co : bm.CST + co, bm.nch, tg, lane);
     } else {
       s = -1;
     }
@@ -705,7 +793,7 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
   res.s = s;
   if (s == r) return res;
   double Hp;
-  const double dS = move_delta<ST>(g, bm, r, s, k_out, k_in, self, t, lane, &Hp);
+  const double dS = move_delta<ST>(g, bm, r, s, k_out, k_in, self, t, lane, &Hp, &pre);
   const double H = (k == 0) ? 1.0 : Hp;
   double ap = exp(-3.0 * dS) * H;
   ap = ap >= 1.0 ? 1.0 : ap;

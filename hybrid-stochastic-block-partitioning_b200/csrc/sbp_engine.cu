@@ -27,7 +27,7 @@ static int key_bits(int B) {
 // One orientation of the sparse rebuild: sort keys, unique them, size the rows, fill them.
 static void rebuild_hashed_side(SbpBlockmodel& bm, long long E, unsigned long long* keys, DevBuf<long long>& base,
                                 DevBuf<int>& mask, DevBuf<int2>& slot, DevBuf<int>& cptr, DevBuf<int>& cidx,
-                                DevBuf<int>& cval) {
+                                DevBuf<int>& cval, long long* top, long long* limit) {
   Context& c = Context::get();
   const int B = bm.B;
   long long nu = 0;
@@ -59,7 +59,10 @@ static void rebuild_hashed_side(SbpBlockmodel& bm, long long E, unsigned long lo
   SBP_CUDA(SBP_COPY_ASYNC(&lastcap, g_sort.caps.p + B - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream));
   c.sync();
   const long long total = lastbase + lastcap;
-  slot.reserve(total);
+  // half as many slots again stay free for rows that outgrow their region (regrow_hashed)
+  slot.reserve(total + total / 2 + 4096);
+  *top = total;
+  *limit = (long long)slot.n;
   cptr.reserve(B + 1);
   cidx.reserve(std::max(nu, 1LL));
   cval.reserve(std::max(nu, 1LL));
@@ -89,14 +92,16 @@ static void rebuild_sparse(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_
   g_sort.rowptr.reserve(B);
   SBP_CUDA(cudaMemsetAsync(bm.d_out.p, 0, B * sizeof(int), c.stream));
   SBP_CUDA(cudaMemsetAsync(bm.d_in.p, 0, B * sizeof(int), c.stream));
-  SBP_CUDA(cudaMemsetAsync(bm.overflow.p, 0, sizeof(int), c.stream));
+  SBP_CUDA(cudaMemsetAsync(bm.overflow.p, 0, (1 + 2 * (size_t)B) * sizeof(int), c.stream));
   k_block_degrees<<<grid_for(g.V, 256, 8 * c.num_sms), 256, 0, c.stream>>>(g.view(), bm.b.p, bm.d_out.p, bm.d_in.p);
   if (E > 0)
     k_edge_keys<<<grid_for(E, 256, 16 * c.num_sms), 256, 0, c.stream>>>(g.view(), bm.b.p, g.out_src.p, B,
                                                                        g_sort.keys.p, g_sort.keysT.p);
   SBP_CHECK_LAUNCH();
-  rebuild_hashed_side(bm, E, g_sort.keys.p, bm.rbase, bm.rmask, bm.rslot, bm.csr_rptr, bm.csr_ridx, bm.csr_rval);
-  rebuild_hashed_side(bm, E, g_sort.keysT.p, bm.cbase, bm.cmask, bm.cslot, bm.csr_cptr, bm.csr_cidx, bm.csr_cval);
+  rebuild_hashed_side(bm, E, g_sort.keys.p, bm.rbase, bm.rmask, bm.rslot, bm.csr_rptr, bm.csr_ridx, bm.csr_rval,
+                      &bm.rtop, &bm.rlimit);
+  rebuild_hashed_side(bm, E, g_sort.keysT.p, bm.cbase, bm.cmask, bm.cslot, bm.csr_cptr, bm.csr_cidx, bm.csr_cval,
+                      &bm.ctop, &bm.climit);
   if (recompute_d) {
     k_rebuild_degrees<<<grid_for(B, 256, 1 << 20), 256, 0, c.stream>>>(bm.view());
     SBP_CHECK_LAUNCH();
@@ -131,14 +136,62 @@ void rebuild(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_d) {
   SBP_CHECK_LAUNCH();
 }
 
+// A Gibbs apply ran out of room in some hashed rows (their flags are set): give each such row
+// a new region after the slots in use, sized from its block's degree (a row of M has at most
+// min(d_out, B) cells, a row of MT at most min(d_in, B)), and recount it from the edges and the
+// assignment, which already carries the batch's moves.  Rows that did not run out of room took
+// every update of the batch and stay as they are.  Costs one pass over the edges instead of a
+// full rebuild; returns false (and changes nothing) when the slot arrays have no room left.
+static DevBuf<int> g_regrow_list;
+static DevBuf<unsigned long long> g_regrow_ctr;   // [0, 1] slots taken per side, [2, 3] rows per side, [4] no room
+
+static bool regrow_hashed(SbpBlockmodel& bm, const SbpGraph& g) {
+  Context& c = Context::get();
+  const int B = bm.B;
+  g_regrow_list.reserve(2 * (size_t)B);
+  g_regrow_ctr.reserve(5);
+  SBP_CUDA(cudaMemsetAsync(g_regrow_ctr.p, 0, 5 * sizeof(unsigned long long), c.stream));
+  int* full_r = bm.overflow.p + 1;
+  int* full_c = bm.overflow.p + 1 + B;
+  const int grid = grid_for(B, 256, 16 * c.num_sms);
+  k_regrow_alloc<<<grid, 256, 0, c.stream>>>(full_r, bm.d_out.p, B, bm.rtop, bm.rlimit, g_regrow_ctr.p,
+                                             g_regrow_ctr.p + 2, bm.rbase.p, bm.rmask.p, g_regrow_list.p,
+                                             g_regrow_ctr.p + 4);
+  k_regrow_alloc<<<grid, 256, 0, c.stream>>>(full_c, bm.d_in.p, B, bm.ctop, bm.climit, g_regrow_ctr.p + 1,
+                                             g_regrow_ctr.p + 3, bm.cbase.p, bm.cmask.p, g_regrow_list.p + B,
+                                             g_regrow_ctr.p + 4);
+  SBP_CHECK_LAUNCH();
+  unsigned long long h[5];
+  SBP_CUDA(SBP_COPY_ASYNC(h, g_regrow_ctr.p, sizeof h, cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  if (h[4]) return false;
+  bm.rtop += (long long)h[0];
+  bm.ctop += (long long)h[1];
+  if (h[2]) k_regrow_clear<<<4 * c.num_sms, 256, 0, c.stream>>>(g_regrow_list.p, (int)h[2], bm.rbase.p, bm.rmask.p,
+                                                                 bm.rslot.p);
+  if (h[3]) k_regrow_clear<<<4 * c.num_sms, 256, 0, c.stream>>>(g_regrow_list.p + B, (int)h[3], bm.cbase.p,
+                                                                 bm.cmask.p, bm.cslot.p);
+  if (g.E > 0)
+    k_regrow_fill<<<grid_for(g.E, 256, 16 * c.num_sms), 256, 0, c.stream>>>(g.view(), bm.view(), g.out_src.p);
+  SBP_CHECK_LAUNCH();
+  SBP_CUDA(cudaMemsetAsync(bm.overflow.p, 0, (1 + 2 * (size_t)B) * sizeof(int), c.stream));
+  return true;
+}
+
+// After a sweep in which hashed rows were regrown: rebuild every row from the assignment
+// (keeping d), which drops the cells whose count went back to 0 and sizes each row for its
+// current cells again.  Regrowth alone keeps a batch going; without this the rows fill up with
+// dead cells, probe chains grow and nearly every batch overflows.
+void tidy_hashed(SbpBlockmodel& bm, const SbpGraph& g, long long overflows_before) {
+  if (bm.sparse && g_overflow_rebuilds > overflows_before) rebuild(bm, g, false);
+}
+
 // entropy::mdl (src/entropy.cpp:584-589).
 double mdl(SbpBlockmodel& bm, const SbpGraph& g) {
   Context& c = Context::get();
-  const int grid = c.npartial;
-  if (!bm.sparse && (long long)bm.B * bm.B <= 4LL * g.E) k_mdl_cells<<<grid, 256, 0, c.stream>>>(bm.view(), c.partial);
-  else k_mdl_edges<<<grid, 256, 0, c.stream>>>(g.view(), bm.view(), g.out_src.p, c.partial);
-  SBP_CHECK_LAUNCH();
-  k_mdl_final<<<1, 256, 0, c.stream>>>(c.partial, grid, g.V, g.E, bm.B, c.scalar);
+  const int cells = !bm.sparse && (long long)bm.B * bm.B <= 4LL * g.E;
+  k_mdl<<<c.npartial, 256, 0, c.stream>>>(g.view(), bm.view(), g.out_src.p, cells, c.partial, c.done, c.scalar,
+                                         nullptr, 0);
   SBP_CHECK_LAUNCH();
   double out = 0.0;
   SBP_CUDA(SBP_COPY_ASYNC(&out, c.scalar, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -262,7 +315,7 @@ void gibbs_apply(SbpBlockmodel& bm, const SbpGraph& g, int batch) {
       k_recover_assign<<<grid_for(batch, 256, 64 * c.num_sms), 256, 0, c.stream>>>(bm.b.p, bm.moved.p, n_cur,
                                                                                     bm.prop.p, bm.old_block.p);
       SBP_CHECK_LAUNCH();
-      rebuild(bm, g, false);
+      if (!regrow_hashed(bm, g)) rebuild(bm, g, false);
       ++g_overflow_rebuilds;
       k_recover_finish<<<grid_for(batch, 256, 64 * c.num_sms), 256, 0, c.stream>>>(
           bm.view(), bm.moved.p, n_cur, n_next, bm.prop.p, bm.old_block.p, bm.qr.p, bm.qs.p, bm.last.p, gen);
@@ -277,8 +330,8 @@ void gibbs_apply(SbpBlockmodel& bm, const SbpGraph& g, int batch) {
 
 
 // Asynchronous-Gibbs sweeps of one finetune call as ONE CUDA graph launch: a conditional while
-// node whose body is a sweep (every batch's evaluation, apply and degree step, the MDL, then
-// k_sweep_control, which applies the early stop on the GPU and sets the loop condition).
+// node whose body is a sweep (every batch's evaluation, apply and degree step, then the MDL,
+// whose last CTA applies the early stop on the GPU and sets the loop condition).
 // Same kernels, same order and the same early-stop arithmetic as the host loop, so the chain
 // and the sweep count are the host loop's.  Returns the sweeps run.
 static DevBuf<SweepCtl> g_ctl;
@@ -352,11 +405,9 @@ static int gibbs_sweeps_graph(SbpBlockmodel& bm, const SbpGraph& g, const BatchP
         bm.view(), bm.moved.p, nullptr, nullptr, bm.prop.p, bm.qr.p, bm.qs.p, bm.last.p, 0u, g_ctl.p, bt);
     launches += 2;
   }
-  if (cells) k_mdl_cells<<<mdl_grid, 256, 0, c.stream>>>(bm.view(), c.partial);
-  else k_mdl_edges<<<mdl_grid, 256, 0, c.stream>>>(g.view(), bm.view(), g.out_src.p, c.partial);
-  k_mdl_final<<<1, 256, 0, c.stream>>>(c.partial, mdl_grid, g.V, g.E, bm.B, c.scalar);
-  k_sweep_control<<<1, 32, 0, c.stream>>>(g_ctl.p, c.scalar, loop);
-  launches += 3;
+  k_mdl<<<mdl_grid, 256, 0, c.stream>>>(g.view(), bm.view(), g.out_src.p, cells ? 1 : 0, c.partial, c.done,
+                                       c.scalar, g_ctl.p, loop);
+  launches += 1;
   const cudaError_t ce = cudaStreamEndCapture(c.stream, &body);
   SBP_CUDA(ce);
   SBP_CUDA(cudaGraphInstantiate(&exec, graph, 0));
@@ -419,7 +470,9 @@ void finetune(SbpBlockmodel& bm, SbpGraph& g, int algo, const SbpFinetuneOptions
         mh_moved += r.moved;
         mh_acc += r.accepted;
       }
+      const long long ovf_sweep = g_overflow_rebuilds;
       for (size_t bt = 0; bt < plan->light_n.size(); ++bt) gibbs_batch(bm, g, *plan, (int)bt, rng, it);
+      tidy_hashed(bm, g, ovf_sweep);
       const double entropy = mdl(bm, g);
       deltas.push_back(entropy - initial_entropy);   // last_iteration_entropy is never updated
       st.sweeps++;

@@ -179,6 +179,7 @@ struct Context {
   double* partial = nullptr;             // MDL partial sums
   double* scalar = nullptr;              // MDL result
   double* mh_out = nullptr;              // MH sweep outputs [4]
+  unsigned* done = nullptr;              // CTAs finished in the current k_mdl launch (0 between launches)
   double2* logt = nullptr;               // [kLogTable] log(x) as hi + lo doubles (entry 0 unused)
   int npartial = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -202,7 +203,9 @@ struct Context {
       SBP_CUDA(cudaMalloc(&c->partial, c->npartial * sizeof(double)));
       SBP_CUDA(cudaMalloc(&c->scalar, sizeof(double)));
       SBP_CUDA(cudaMalloc(&c->mh_out, 16 * sizeof(double)));
+      SBP_CUDA(cudaMalloc(&c->done, sizeof(unsigned)));
       SBP_CUDA(cudaMemset(c->status, 0, 8 * sizeof(int)));
+      SBP_CUDA(cudaMemset(c->done, 0, sizeof(unsigned)));
       SBP_CUDA(cudaEventCreate(&c->ev0));
       SBP_CUDA(cudaEventCreate(&c->ev1));
       c->logt = make_log_table();
@@ -394,6 +397,8 @@ struct SbpBlockmodel {
   DevBuf<long long> rbase, cbase;
   DevBuf<int> rmask, cmask, overflow, old_block;
   DevBuf<int2> rslot, cslot;
+  long long rtop = 0, ctop = 0;       // slots in use (rows are regrown after them)
+  long long rlimit = 0, climit = 0;   // slots allocated
   DevBuf<int> csr_rptr, csr_ridx, csr_rval, csr_cptr, csr_cidx, csr_cval;   // sorted rows after a rebuild
   float overall_entropy = 3.40282347e+38f;
   int num_blocks_to_merge = 0;
@@ -463,6 +468,7 @@ struct SbpBlockmodel {
       cbase.reserve(B);
       rmask.reserve(B);
       cmask.reserve(B);
+      overflow.reserve(1 + 2 * (size_t)B);   // any-row flag, then one flag per row of M and of MT
     } else {
       const size_t cells = (size_t)B * (size_t)ld;
       M.reserve(cells);
@@ -561,6 +567,7 @@ double mdl(SbpBlockmodel& bm, const SbpGraph& g);
 bool early_stop(int iteration, bool bracket, double initial_entropy, const std::vector<double>& deltas);
 void set_smem_limit(const void* fn, size_t bytes);
 // Apply half of an asynchronous-Gibbs batch: the accepted moves in bm.moved / n_moved[gen & 1].
+void tidy_hashed(SbpBlockmodel& bm, const SbpGraph& g, long long overflows_before);
 void gibbs_apply(SbpBlockmodel& bm, const SbpGraph& g, int batch);
 // One asynchronous-Gibbs batch with the plain proposal (evaluation + apply).
 void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, int bt, RngParams rng, int sweep);

@@ -2,7 +2,7 @@
 //
 // Kernel map (reference function each one stands in for):
 //   k_rebuild_*        Blockmodel::initialize_edge_counts     src/blockmodel/blockmodel.cpp:187-255
-//   k_mdl_*            entropy::mdl / log_posterior_probability src/entropy.cpp:584-589, blockmodel.cpp:267-285
+//   k_mdl              entropy::mdl / log_posterior_probability src/entropy.cpp:584-589, blockmodel.cpp:267-285
 //   k_gibbs_eval_*     asynchronous_gibbs evaluation half     src/finetune.cpp:49-57, 531-545
 //   k_apply_*          asynchronous_gibbs apply half          src/finetune.cpp:58-71 + Blockmodel::move_vertex
 //   k_mh               metropolis_hastings sweep              src/finetune.cpp:412-444, 446-501
@@ -65,32 +65,6 @@ __global__ void k_rebuild_degrees(BlockView bm) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x < bm.B) bm.d[x] = bm.d_out[x] + bm.d_in[x] - bm_get(bm, x, x);
 }
-
-// ------------------------------------------------------------------------------------------
-// MDL: L = sum_cells g(M) - sum g(d_out) - sum g(d_in);
-// mdl = E h(B^2/E) + V log B - L.  Deterministic two-pass reduction.
-// ------------------------------------------------------------------------------------------
-
-__global__ void k_mdl_cells(BlockView bm, double* partial) {
-  __shared__ double red[32];
-  const double t = mdl_cells_part(bm, blockIdx.x, gridDim.x, red);
-  if (threadIdx.x == 0) partial[blockIdx.x] = t;
-}
-
-// Edge form: sum_cells M log M = sum over edges of log M[b_src, b_dst]; one thread per edge.
-__global__ void k_mdl_edges(GraphView g, BlockView bm, const int* __restrict__ out_src, double* partial) {
-  __shared__ double red[32];
-  const double t = mdl_edges_part(g, bm, out_src, blockIdx.x, gridDim.x, red);
-  if (threadIdx.x == 0) partial[blockIdx.x] = t;
-}
-
-// Sum of the partials in a fixed order (one CTA of 256 threads) and the MDL formula.
-__global__ void k_mdl_final(const double* partial, int n, int V, long long E, int B, double* out) {
-  __shared__ double red[32];
-  const double v = mdl_final_value(partial, n, V, E, B, red);
-  if (threadIdx.x == 0) *out = v;
-}
-
 // ------------------------------------------------------------------------------------------
 // Asynchronous Gibbs: evaluate a list of vertices against the frozen state.  Accepted moves
 // go to prop[v] and the moved list; counters: [0] visits [1] proposals_moved [2] accepted.
@@ -203,10 +177,9 @@ __global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n
 // End of one sweep of a graph-run finetune: record delta = MDL - first MDL (the asynchronous-
 // Gibbs rule, src/finetune.cpp:40,74) and apply finetune::early_stop (src/finetune.cpp:144-162)
 // in the host's arithmetic; the loop continues while it does not stop.
-__global__ void k_sweep_control(SweepCtl* ctl, const double* mdl, cudaGraphConditionalHandle loop) {
-  if (threadIdx.x || blockIdx.x) return;
+__device__ __forceinline__ void sweep_control(SweepCtl* ctl, double mdl, cudaGraphConditionalHandle loop) {
   const int it = ctl->count;
-  ctl->deltas[it] = *mdl - ctl->initial;
+  ctl->deltas[it] = mdl - ctl->initial;
   ctl->count = it + 1;
   bool stop;
   if (ctl->deltas[it] == 0.0) {
@@ -223,6 +196,32 @@ __global__ void k_sweep_control(SweepCtl* ctl, const double* mdl, cudaGraphCondi
   ctl->sweep = it + 1;
   ctl->gen0 += (unsigned)ctl->nbatches;
   cudaGraphSetConditional(loop, stop ? 0u : 1u);
+}
+
+// entropy::mdl (src/entropy.cpp:584-589) in one launch.  Every CTA writes its partial sum (cell
+// form when B*B <= 4E on dense storage, else the edge form); the CTA that finishes last (a
+// counter taken after a memory fence) sums the partials in a fixed order and applies the
+// formula.  With a graph-run sweep (ctl) it then records the sweep and sets the loop condition.
+__global__ void k_mdl(GraphView g, BlockView bm, const int* __restrict__ out_src, int cells, double* partial,
+                      unsigned* done, double* out, SweepCtl* ctl, cudaGraphConditionalHandle loop) {
+  __shared__ double red[32];
+  __shared__ int s_last;
+  const double t = cells ? mdl_cells_part(bm, blockIdx.x, gridDim.x, red)
+                         : mdl_edges_part(g, bm, out_src, blockIdx.x, gridDim.x, red);
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = t;
+    __threadfence();
+    s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const double v = mdl_final_value(partial, gridDim.x, g.V, g.E, bm.B, red);
+  if (threadIdx.x == 0) {
+    *out = v;
+    *done = 0u;
+    if (ctl) sweep_control(ctl, v, loop);
+  }
 }
 
 // ------------------------------------------------------------------------------------------

@@ -8,7 +8,7 @@ constexpr int kProposalsPerBlock = 10;   // block_merge::NUM_AGG_PROPOSALS_PER_B
 constexpr int kMaxIterations = 100;      // finetune::MAX_NUM_ITERATIONS (include/finetune.hpp:56)
 
 // Device-side state of an asynchronous-Gibbs finetune run as one CUDA graph: the loop over
-// sweeps and its early stop are decided on the GPU (k_sweep_control).  Kernels given a
+// sweeps and its early stop are decided on the GPU (k_mdl).  Kernels given a
 // control block read the sweep index and the batch generation from it.
 struct SweepCtl {
   int sweep;               // index of the sweep being run
@@ -31,9 +31,8 @@ struct Csr {
 __global__ void k_rebuild_global(GraphView g, BlockView bm);
 __global__ void k_rebuild_smem(GraphView g, BlockView bm);
 __global__ void k_rebuild_degrees(BlockView bm);
-__global__ void k_mdl_cells(BlockView bm, double* partial);
-__global__ void k_mdl_edges(GraphView g, BlockView bm, const int* __restrict__ out_src, double* partial);
-__global__ void k_mdl_final(const double* partial, int n, int V, long long E, int B, double* out);
+__global__ void k_mdl(GraphView g, BlockView bm, const int* __restrict__ out_src, int cells, double* partial,
+                      unsigned* done, double* out, SweepCtl* ctl, cudaGraphConditionalHandle loop);
 // Asynchronous-Gibbs evaluation compiled for one storage of the block matrix.
 __global__ void __launch_bounds__(256, 2)
     k_gibbs_eval_dense(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
@@ -51,7 +50,6 @@ __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, 
 __global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved, int* prop,
                                const int* qr, const int* qs, const unsigned long long* last, unsigned gen,
                                const SweepCtl* ctl, int batch);
-__global__ void k_sweep_control(SweepCtl* ctl, const double* mdl, cudaGraphConditionalHandle loop);
 __global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, int n, int start, RngParams rng,
                      int sweep, int cap, double* out, int* status);
 __global__ void k_move_vertex(GraphView g, BlockView bm, int v, int s, int cap, int* status);
@@ -77,6 +75,12 @@ __global__ void k_fill_rows(const long long* __restrict__ rowptr, const unsigned
                             int* csr_ptr, int* csr_idx, int* csr_val);
 __global__ void k_block_degrees(GraphView g, const int* __restrict__ b, int* d_out, int* d_in);
 __global__ void k_recover_assign(int* b, const int* moved, const int* n_moved, const int* prop, int* old_block);
+__global__ void k_regrow_alloc(const int* __restrict__ full, const int* __restrict__ deg, int B, long long top,
+                               long long limit, unsigned long long* used, unsigned long long* nrows, long long* base,
+                               int* mask, int* list, unsigned long long* no_room);
+__global__ void k_regrow_clear(const int* __restrict__ list, int n, const long long* __restrict__ base,
+                               const int* __restrict__ mask, int2* slot);
+__global__ void k_regrow_fill(GraphView g, BlockView bm, const int* __restrict__ out_src);
 __global__ void k_recover_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved,
                                  int* prop, const int* old_block, const int* qr, const int* qs,
                                  const unsigned long long* last, unsigned gen);
@@ -85,6 +89,6 @@ __global__ void k_hashed_to_dense(const long long* __restrict__ base, const int*
                                   const int2* __restrict__ slot, int B, int row0, int rows, int* dense);
 
 // Shared-memory ints per warp table of `cap` slots (keys, out counts, in counts, used list, count).
-inline int table_ints(int cap) { return 4 * cap + 32; }
+inline int table_ints(int cap) { return 4 * cap + 32; }   // keys, counts, list; count + 31 spare (16 walk bins)
 
 }  // namespace sbpb

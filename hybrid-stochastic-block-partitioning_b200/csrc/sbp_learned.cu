@@ -526,10 +526,12 @@ static void finetune_learned(SbpBlockmodel& bm, SbpGraph& g, int algorithm, cons
       mh_moved += r.moved;
       mh_acc += r.accepted;
     }
+    const long long ovf_sweep = g_overflow_rebuilds;
     for (size_t bt = 0; bt < plan.light_n.size(); ++bt) {
       if (learned) learned_batch(bm, g, plan, (int)bt, *m, lp, rng, it);
       else gibbs_batch(bm, g, plan, (int)bt, rng, it);
     }
+    tidy_hashed(bm, g, ovf_sweep);
     const double entropy = mdl(bm, g);
     deltas.push_back(stop_rule == 1 ? entropy - last_entropy : entropy - initial_entropy);
     last_entropy = entropy;
@@ -1030,6 +1032,7 @@ SbpStatus sbp_collect_moves(SbpBlockmodel* bm, const SbpGraph* cg, SbpDataset* d
   SBP_CUDA(cudaMemsetAsync(c.counters, 0, 8 * sizeof(unsigned long long), c.stream));
   const auto t0 = std::chrono::steady_clock::now();
   for (int it = 0; it < sweeps; ++it) {
+    const long long ovf_sweep = g_overflow_rebuilds;
     for (size_t bt = 0; bt < plan.light_n.size(); ++bt) {
       // plain evaluation (gibbs_batch without its apply), record, then apply
       const int nl = plan.light_n[bt], nh = plan.heavy_n[bt];
@@ -1057,6 +1060,7 @@ SbpStatus sbp_collect_moves(SbpBlockmodel* bm, const SbpGraph* cg, SbpDataset* d
                    d->X.p, d->target.p, d->nvalid.p, d->count.p, d->capacity, cap, c.status);
       gibbs_apply(*bm, g, batch);
     }
+    tidy_hashed(*bm, g, ovf_sweep);
     st.sweeps++;
     c.check_status();
   }

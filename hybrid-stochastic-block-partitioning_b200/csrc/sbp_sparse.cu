@@ -62,6 +62,53 @@ __global__ void k_fill_rows(const long long* __restrict__ rowptr, const unsigned
   }
 }
 
+// Regrowth of the hashed rows that ran out of room (one side: rows of M or of MT).  A flagged
+// row x gets a region of the power of two at least twice its old room and at least
+// 2 min(deg[x], B) + 16 slots, taken after the `top` slots in use; with no room left below
+// `limit` the step reports it and changes nothing for that row.
+__global__ void k_regrow_alloc(const int* __restrict__ full, const int* __restrict__ deg, int B, long long top,
+                               long long limit, unsigned long long* used, unsigned long long* nrows, long long* base,
+                               int* mask, int* list, unsigned long long* no_room) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < B; x += gridDim.x * blockDim.x) {
+    if (!full[x]) continue;
+    const long long need = 2LL * (long long)min(deg[x], B) + 16;
+    long long cap = 2LL * ((long long)mask[x] + 1);
+    while (cap < need) cap <<= 1;
+    const unsigned long long off = atomicAdd(used, (unsigned long long)cap);
+    if (cap > (1LL << 30) || top + (long long)off + cap > limit) {
+      atomicOr(no_room, 1ull);
+      continue;
+    }
+    base[x] = top + (long long)off;
+    mask[x] = (int)(cap - 1);
+    list[atomicAdd(nrows, 1ull)] = x;
+  }
+}
+
+// Empty slots in the new regions (one CTA per listed row).
+__global__ void k_regrow_clear(const int* __restrict__ list, int n, const long long* __restrict__ base,
+                               const int* __restrict__ mask, int2* slot) {
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int x = list[i];
+    const long long b0 = base[x];
+    const int cap = mask[x] + 1;
+    for (int j = threadIdx.x; j < cap; j += blockDim.x) slot[b0 + j] = make_int2(-1, 0);
+  }
+}
+
+// Recount the regrown rows: every edge (b_src, b_dst) adds one to row b_src of M when that row
+// is flagged and to row b_dst of MT when that one is (the new regions cannot run out of room).
+__global__ void k_regrow_fill(GraphView g, BlockView bm, const int* __restrict__ out_src) {
+  const int* full_r = bm.overflow + 1;
+  const int* full_c = bm.overflow + 1 + bm.B;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < g.E; e += stride) {
+    const int bs = bm.b[__ldg(out_src + e)], bd = bm.b[__ldg(g.out_idx + e)];
+    if (full_r[bs]) hashed_add(bm.rbase, bm.rmask, bm.rslot, bs, bd, 1, bm.overflow, bm.overflow + 1);
+    if (full_c[bd]) hashed_add(bm.cbase, bm.cmask, bm.cslot, bd, bs, 1, bm.overflow, bm.overflow + 1 + bm.B);
+  }
+}
+
 // Block degrees from the vertices (out-degree; in-degree with the self loop).
 __global__ void k_block_degrees(GraphView g, const int* __restrict__ b, int* d_out, int* d_in) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < g.V; v += gridDim.x * blockDim.x) {

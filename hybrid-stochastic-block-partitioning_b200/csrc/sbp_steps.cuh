@@ -24,8 +24,8 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 // two hashed rows (atomic).
 __device__ __forceinline__ void cell_add(const BlockView& bm, int row, int col, int delta) {
   if (bm.sparse) {
-    hashed_add(bm.rbase, bm.rmask, bm.rslot, row, col, delta, bm.overflow);
-    hashed_add(bm.cbase, bm.cmask, bm.cslot, col, row, delta, bm.overflow);
+    hashed_add(bm.rbase, bm.rmask, bm.rslot, row, col, delta, bm.overflow, bm.overflow + 1);
+    hashed_add(bm.cbase, bm.cmask, bm.cslot, col, row, delta, bm.overflow, bm.overflow + 1 + bm.B);
     return;
   }
   atomicAdd(bm.M + (size_t)row * bm.ld + col, delta);
@@ -37,7 +37,8 @@ __device__ __forceinline__ void cell_add(const BlockView& bm, int row, int col, 
 // Apply of one accepted move v: r -> prop[v] (Blockmodel::move_vertex, src/blockmodel/
 // blockmodel.cpp:344-360, for a batch of simultaneous moves): M, MT and the chunk sums by edge,
 // d_out / d_in, the quirk terms qr/qs of d[r], d[s] (the neighbours that are counted in the
-// reference's sequential apply) and the batch's last mover of r and s.  One warp per vertex.
+// reference's sequential apply) and the batch's last mover of r and s.  One warp per vertex;
+// lanes whose edges change the same cell add their count with one atomic.
 __device__ __forceinline__ void apply_moved_vertex(const GraphView& g, const BlockView& bm, int v, const int* prop,
                                                    int* qr, int* qs, unsigned long long* last, unsigned gen,
                                                    int lane) {
@@ -45,28 +46,51 @@ __device__ __forceinline__ void apply_moved_vertex(const GraphView& g, const Blo
   const int self = g.self[v];
   int cr = 0, cs = 0;
   const int o0 = g.out_ptr[v], o1 = g.out_ptr[v + 1];
-  for (int e = o0 + lane; e < o1; e += kWarp) {
-    const int u = __ldg(g.out_idx + e);
-    if (u == v) continue;
-    const int bo = bm.b[u], pu = prop[u];
-    const int bn = pu >= 0 ? pu : bo;
-    cell_add(bm, r, bo, -1);
-    cell_add(bm, s, bn, 1);
-    const int ba = (pu >= 0 && u < v) ? pu : bo;
-    cr += (ba == r);
-    cs += (ba == s);
-  }
   const int i0 = g.in_ptr[v], i1 = g.in_ptr[v + 1];
-  for (int e = i0 + lane; e < i1; e += kWarp) {
-    const int u = __ldg(g.in_idx + e);
-    const int bo = bm.b[u], pu = prop[u];
-    if (pu < 0) {
-      cell_add(bm, bo, r, -1);
-      cell_add(bm, bo, s, 1);
+  const int k_out = o1 - o0, k = k_out + (i1 - i0);
+  // One pass over the virtual neighbour list (out-edges, then in-edges), two elements per lane
+  // in flight.  Out-edge v -> u (not the self loop): (r, b_u) -= 1 and (s, b'_u) += 1, b'_u the
+  // block u moves to in this batch.  In-edge u -> v of a u that stays: (b_u, r) -= 1 and
+  // (b_u, s) += 1 (a moving u's own out-edge covers the cell otherwise).
+  for (int base = 0; base < k; base += 2 * kWarp) {
+    int u[2], bo[2], pu[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int j = base + h * kWarp + lane;
+      u[h] = j < k ? (j < k_out ? __ldg(g.out_idx + o0 + j) : __ldg(g.in_idx + i0 + (j - k_out))) : -1;
     }
-    const int ba = (pu >= 0 && u < v) ? pu : bo;
-    cr += (ba == r);
-    cs += (ba == s);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      bo[h] = u[h] >= 0 ? bm.b[u[h]] : -1;
+      pu[h] = u[h] >= 0 ? prop[u[h]] : -1;
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int j = base + h * kWarp + lane;
+      const bool out_edge = j < k_out;
+      int ko = -1, kn = -1, ks = -1;
+      if (u[h] >= 0 && !(out_edge && u[h] == v)) {
+        if (out_edge) {
+          ko = bo[h];
+          kn = pu[h] >= 0 ? pu[h] : bo[h];
+        } else if (pu[h] < 0) {
+          ks = bo[h];
+        }
+        const int ba = (pu[h] >= 0 && u[h] < v) ? pu[h] : bo[h];
+        cr += (ba == r);
+        cs += (ba == s);
+      }
+      const unsigned po = __match_any_sync(kFull, ko);
+      if (ko >= 0 && (__ffs(po) - 1) == lane) cell_add(bm, r, ko, -__popc(po));
+      const unsigned pn = __match_any_sync(kFull, kn);
+      if (kn >= 0 && (__ffs(pn) - 1) == lane) cell_add(bm, s, kn, __popc(pn));
+      const unsigned pb = __match_any_sync(kFull, ks);
+      if (ks >= 0 && (__ffs(pb) - 1) == lane) {
+        const int c = __popc(pb);
+        cell_add(bm, ks, r, -c);
+        cell_add(bm, ks, s, c);
+      }
+    }
   }
   cr = warp_sum_int(cr);
   cs = warp_sum_int(cs);
@@ -75,7 +99,7 @@ __device__ __forceinline__ void apply_moved_vertex(const GraphView& g, const Blo
       cell_add(bm, r, r, -1);
       cell_add(bm, s, s, 1);
     }
-    const int k_out = o1 - o0, k_in_self = (i1 - i0) + self;
+    const int k_in_self = (i1 - i0) + self;
     atomicAdd(bm.d_out + r, -k_out);
     atomicAdd(bm.d_out + s, k_out);
     atomicAdd(bm.d_in + r, -k_in_self);
@@ -133,7 +157,7 @@ __device__ __forceinline__ double mdl_edges_part(const GraphView& g, const Block
 __device__ __forceinline__ double mdl_final_value(const double* partial, int n, int V, long long E, int B,
                                                   double* red) {
   double acc = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += __ldcg(partial + i);
   const double L = block_sum(acc, red);
   const double x = pow((double)B, 2) / (double)E;
   const double h = ((1 + x) * log(1 + x)) - (x * log(x));
