@@ -252,9 +252,9 @@ __device__ __forceinline__ int bm_getT(const BlockView& bm, int row, int col) {
 }
 
 // Walk of a hashed row in ascending column order: the first column whose running count
-// exceeds `target`, found digit by digit (4 bits of the column at a time, most significant
-// first).  Each pass sums the row's counts of the columns left in range into 16 bins (`bins`:
-// 16 ints of the warp's shared memory), scans the bins and keeps the one that holds the target.
+// exceeds `target`, found digit by digit (5 bits of the column at a time, most significant
+// first).  Each pass sums the row's counts of the columns left in range into 32 bins (`bins`:
+// 32 ints of the warp's shared memory), scans the bins and keeps the one that holds the target.
 // Same result as the dense walks.
 __device__ __forceinline__ int warp_select_hashed(const long long* base, const int* mask, const int2* slot, int row,
                                                   int B, long long target, int lane, int* bins) {
@@ -263,18 +263,18 @@ __device__ __forceinline__ int warp_select_hashed(const long long* base, const i
   int bits = 0;
   while ((1 << bits) < B) ++bits;
   int lo = 0;
-  for (int shift = ((bits + 3) / 4) * 4 - 4; shift >= 0; shift -= 4) {
-    if (lane < 16) bins[lane] = 0;
+  for (int shift = ((bits + 4) / 5) * 5 - 5; shift >= 0; shift -= 5) {
+    bins[lane] = 0;
     __syncwarp();
-    const long long span = 16LL << shift;
+    const long long span = 32LL << shift;
     for (int i = lane; i < cap; i += kWarp) {
       const int2 e = slot[b0 + i];
       if (e.x >= lo && (long long)e.x < lo + span && e.y > 0) atomicAdd(&bins[(e.x - lo) >> shift], e.y);
     }
     __syncwarp();
-    const long long v = lane < 16 ? (long long)bins[lane] : 0;
+    const long long v = bins[lane];
     const long long incl = warp_incl_scan(v, lane);
-    const unsigned hit = __ballot_sync(kFull, lane < 16 && incl > target);
+    const unsigned hit = __ballot_sync(kFull, incl > target);
     if (!hit) return -1;
     const int sel = __ffs(hit) - 1;
     target -= __shfl_sync(kFull, incl - v, sel);
@@ -423,7 +423,7 @@ __device__ __forceinline__ void table_add(const WarpTable& t, int key, bool vali
 
 // Per-warp table of `cap` slots carved from a CTA's dynamic shared memory (table_ints(cap) ints per warp).
 __device__ __forceinline__ WarpTable carve_table(int* base, int cap, int warp) {
-  int* p = base + (size_t)warp * (4 * cap + 32);
+  int* p = base + (size_t)warp * (4 * cap + 64);
   WarpTable t;
   t.keys = p;
   t.cout = p + cap;
@@ -758,7 +758,7 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
     if (ST != Store::kDense && hashed) {
       const int dot = bm.d_out[tblk];
       const long long target = scale32(x.y, (long long)dot + (long long)bm.d_in[tblk]);
-      int* bins = t.nlist + 16;   // spare ints after the table's list count
+      int* bins = t.nlist + 32;   // the 32 ints after the table's list count
       if (target < dot) s = warp_select_hashed(bm.rbase, bm.rmask, bm.rslot, tblk, bm.B, target, lane, bins);
       else s = warp_select_hashed(bm.cbase, bm.cmask, bm.cslot, tblk, bm.B, target - dot, lane, bins);
     } else if (ST != Store::kHashed) {

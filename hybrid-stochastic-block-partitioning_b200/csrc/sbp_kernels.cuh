@@ -89,6 +89,6 @@ __global__ void k_hashed_to_dense(const long long* __restrict__ base, const int*
                                   const int2* __restrict__ slot, int B, int row0, int rows, int* dense);
 
 // Shared-memory ints per warp table of `cap` slots (keys, out counts, in counts, used list, count).
-inline int table_ints(int cap) { return 4 * cap + 32; }   // keys, counts, list; count + 31 spare (16 walk bins)
+inline int table_ints(int cap) { return 4 * cap + 64; }   // keys, counts, list; count, 31 spare, 32 walk bins
 
 }  // namespace sbpb

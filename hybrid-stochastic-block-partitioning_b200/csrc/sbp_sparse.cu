@@ -22,11 +22,14 @@ __global__ void k_unique_rows(const unsigned long long* __restrict__ ukeys, long
     atomicAdd(rowcnt + (ukeys[j] / (unsigned long long)B), 1u);
 }
 
-// Row capacity: a power of two with at least three quarters free after the rebuild (room to
-// grow: at large B most moves add cells, and a full row forces a rebuild).
+// Row capacity: a power of two of at least factor * cells + 4 factor slots (room to grow: at
+// large B most moves add cells, and a full row has to be regrown).  Rows of more than 128
+// cells get at most factor 2: the hashed walk reads a row's whole region, and for long rows
+// that costs more than the occasional regrowth.
 __global__ void k_row_caps(const unsigned* __restrict__ rowcnt, int B, unsigned factor, unsigned* cap, int* mask) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < B; r += gridDim.x * blockDim.x) {
-    unsigned want = factor * rowcnt[r] + 4u * factor, c = 8u;
+    const unsigned f = rowcnt[r] > 128u && factor > 2u ? 2u : factor;
+    unsigned want = f * rowcnt[r] + 4u * f, c = 8u;
     while (c < want) c <<= 1;
     cap[r] = c;
     mask[r] = (int)c - 1;

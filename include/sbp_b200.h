@@ -113,8 +113,9 @@ int32_t sbp_device_count(void);
  * integer counts updated by atomics) instead of dense B x B arrays; default 65536 (dense storage
  * is faster wherever it fits; it also falls back to row-hashed when the dense matrix would take
  * more than 40 % of the free device memory).  Applies to blockmodels whose block count is set
- * after the call.  "hashed_row_factor" (default 4): a rebuilt hashed row gets room for
- * factor x its cells (larger: fewer rebuilds when rows fill up).  "graph_sweeps" (default 1): an
+ * after the call.  "hashed_row_factor" (default 4, range 2-64): a rebuilt hashed row gets room
+ * for factor x its cells, at most 2 x for rows of more than 128 cells (larger: rows fill up and
+ * are regrown less often; smaller: less memory and a cheaper walk of the row).  "graph_sweeps" (default 1): an
  * asynchronous-Gibbs finetune on dense storage runs as one CUDA graph launch whose sweep loop and
  * early stop are decided on the GPU; 0 drives every sweep from the host (same results). */
 SbpStatus sbp_set_option(const char *name, int64_t value);
