@@ -47,6 +47,10 @@ def args_parse():
     ap.add_argument("--batches", type=int, default=10)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain comparison")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched 64-graph comparison")
+    ap.add_argument("--host-sweeps", action="store_true",
+                    help="drive every finetune sweep from the host (same kernels and results) instead of one CUDA "
+                         "graph per finetune call; for kernel profilers, which do not profile the kernel nodes of a "
+                         "graph with conditional nodes")
     return ap.parse_args()
 
 
@@ -248,7 +252,8 @@ def main():
     config = {"workload": WORKLOAD if a.config == 2 else f"config {a.config}", "V": V, "edges_raw": int(len(src)),
               "blocks_planted": int(truth.max()) + 1, "algorithm": a.algorithm, "batches": a.batches,
               "merge": "approximate", "step": "one full stochastic_block_partition (B = V -> final B)",
-              "l2": "256 MB buffer written before every timed step (L2 flush)", "parallelism": f"replicas x{world}"}
+              "l2": "256 MB buffer written before every timed step (L2 flush)", "parallelism": f"replicas x{world}",
+              "sweep_driver": "host loop" if a.host_sweeps else "one CUDA graph per finetune call"}
 
     if a.impl == "reference":
         if rank != 0:
@@ -284,6 +289,8 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     import sbp_b200 as S
     S.load()
+    if a.host_sweeps:
+        S.set_option("graph_sweeps", 0)
     ext = torch.cuda.ExternalStream(S.stream_handle())
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
