@@ -951,57 +951,95 @@ SbpStatus sbp_graph_create(int32_t V, int64_t n, const int32_t* src, const int32
   *out = nullptr;
   SBP_REQUIRE(V > 0, "num_vertices must be positive");
   SBP_REQUIRE(n >= 0 && (n == 0 || (src && dst)), "edge arrays are NULL");
+  SBP_REQUIRE(n < 2000000000LL, "more than 2e9 edges are not supported");
   Context& c = Context::get();
-  for (int64_t i = 0; i < n; ++i)
-    SBP_REQUIRE(src[i] >= 0 && src[i] < V && dst[i] >= 0 && dst[i] < V, "edge endpoint out of range");
-  // utils::insert_nodup: keep the first occurrence of each (src, dst)
-  uint64_t cap = 16;
-  while (cap < (uint64_t)(2 * n + 16)) cap <<= 1;
-  std::vector<uint64_t> table(cap, ~0ull);
-  std::vector<int> ks, kd;
-  ks.reserve(n);
-  kd.reserve(n);
-  int shift = 64;
-  for (uint64_t x = cap; x > 1; x >>= 1) --shift;
-  for (int64_t i = 0; i < n; ++i) {
-    const uint64_t key = (uint64_t)(uint32_t)src[i] * (uint64_t)V + (uint64_t)(uint32_t)dst[i];
-    uint64_t h = (key * 0x9E3779B97F4A7C15ull) >> shift;
-    bool dup = false;
-    while (table[h] != ~0ull) {
-      if (table[h] == key) {
-        dup = true;
-        break;
-      }
-      h = (h + 1) & (cap - 1);
-    }
-    if (dup) continue;
-    table[h] = key;
-    ks.push_back(src[i]);
-    kd.push_back(dst[i]);
-  }
-  std::vector<uint64_t>().swap(table);
   auto g = std::make_unique<SbpGraph>();
   g->V = V;
-  g->E = (long long)ks.size();
-  const size_t m = ks.size();
-  std::vector<int> op(V + 1, 0), ip(V + 1, 0), oi(m), ii(m);
-  std::vector<unsigned char> self(V, 0);
-  for (size_t i = 0; i < m; ++i) {
-    op[ks[i] + 1]++;
-    if (ks[i] == kd[i]) self[ks[i]] = 1;
-    else ip[kd[i] + 1]++;
+  // Device ingest (sbp_ingest.cu): first occurrence of each (src, dst) pair, adjacency lists in
+  // input order, self loops on the out side only.
+  DevBuf<int> d_src, d_dst, first, bad;
+  DevBuf<unsigned long long> table, okeys, ikeys, tmp, partial, ctr;
+  DevBuf<unsigned> ocnt, icnt, hist;
+  DevBuf<long long> optr, iptr;
+  g->self.reserve(V);
+  ocnt.reserve((size_t)V + 1);
+  icnt.reserve((size_t)V + 1);
+  SBP_CUDA(cudaMemsetAsync(g->self.p, 0, V, c.stream));
+  SBP_CUDA(cudaMemsetAsync(ocnt.p, 0, ((size_t)V + 1) * sizeof(unsigned), c.stream));
+  SBP_CUDA(cudaMemsetAsync(icnt.p, 0, ((size_t)V + 1) * sizeof(unsigned), c.stream));
+  int ib = 1;
+  while ((1LL << ib) < n) ++ib;
+  int vb = 1;
+  while ((1LL << vb) < V) ++vb;
+  long long m = 0, mi = 0;
+  if (n > 0) {
+    d_src.reserve(n);
+    d_dst.reserve(n);
+    SBP_CUDA(SBP_COPY_ASYNC(d_src.p, src, n * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    SBP_CUDA(SBP_COPY_ASYNC(d_dst.p, dst, n * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    int tbits = 4;
+    while ((1LL << tbits) < 2 * n + 16) ++tbits;
+    const long long cap = 1LL << tbits;
+    table.reserve(cap);
+    first.reserve(cap);
+    bad.reserve(1);
+    ctr.reserve(2);
+    okeys.reserve(n);
+    ikeys.reserve(n);
+    SBP_CUDA(cudaMemsetAsync(table.p, 0xff, cap * sizeof(unsigned long long), c.stream));
+    SBP_CUDA(cudaMemsetAsync(first.p, 0x7f, cap * sizeof(int), c.stream));
+    SBP_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), c.stream));
+    SBP_CUDA(cudaMemsetAsync(ctr.p, 0, 2 * sizeof(unsigned long long), c.stream));
+    const int grid = grid_for(n, 256, 16 * c.num_sms);
+    k_ingest_first<<<grid, 256, 0, c.stream>>>(d_src.p, d_dst.p, n, V, table.p, first.p, tbits, bad.p);
+    k_ingest_keep<<<grid, 256, 0, c.stream>>>(d_src.p, d_dst.p, n, V, table.p, first.p, tbits, ib, okeys.p, ikeys.p,
+                                              ctr.p, ocnt.p, icnt.p, g->self.p);
+    SBP_CHECK_LAUNCH();
+    unsigned long long cnt[2] = {0, 0};
+    int any_bad = 0;
+    SBP_CUDA(SBP_COPY_ASYNC(cnt, ctr.p, sizeof cnt, cudaMemcpyDeviceToHost, c.stream));
+    SBP_CUDA(SBP_COPY_ASYNC(&any_bad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    if (any_bad) throw Error(SBP_ERR_INVALID_ARGUMENT, "edge endpoint out of range");
+    m = (long long)cnt[0];
+    mi = (long long)cnt[1];
   }
-  for (int v = 0; v < V; ++v) {
-    op[v + 1] += op[v];
-    ip[v + 1] += ip[v];
+  g->E = m;
+  partial.reserve(scan_partial_capacity(c.num_sms));
+  g->out_idx.reserve(m);
+  g->out_src.reserve(m);
+  g->in_idx.reserve(mi);
+  if (m > 0) {
+    tmp.reserve(m);
+    hist.reserve(radix_hist_capacity(m, c.num_sms));
+    unsigned long long* sorted = nullptr;
+    radix_sort_u64(okeys.p, tmp.p, m, vb + ib, hist.p, partial.p, c.num_sms, c.stream, &sorted);
+    k_ingest_fill<<<grid_for(m, 256, 16 * c.num_sms), 256, 0, c.stream>>>(sorted, m, ib, d_dst.p, g->out_idx.p,
+                                                                        g->out_src.p);
+    SBP_CHECK_LAUNCH();
   }
-  {
-    std::vector<int> fo(op.begin(), op.end() - 1), fi(ip.begin(), ip.end() - 1);
-    for (size_t i = 0; i < m; ++i) {
-      oi[fo[ks[i]]++] = kd[i];
-      if (ks[i] != kd[i]) ii[fi[kd[i]]++] = ks[i];
-    }
+  if (mi > 0) {
+    unsigned long long* sorted = nullptr;
+    radix_sort_u64(ikeys.p, tmp.p, mi, vb + ib, hist.p, partial.p, c.num_sms, c.stream, &sorted);
+    k_ingest_fill<<<grid_for(mi, 256, 16 * c.num_sms), 256, 0, c.stream>>>(sorted, mi, ib, d_src.p, g->in_idx.p,
+                                                                         nullptr);
+    SBP_CHECK_LAUNCH();
   }
+  optr.reserve((size_t)V + 1);
+  iptr.reserve((size_t)V + 1);
+  g->out_ptr.reserve((size_t)V + 1);
+  g->in_ptr.reserve((size_t)V + 1);
+  exclusive_scan_u32(ocnt.p, optr.p, (long long)V + 1, partial.p, c.num_sms, c.stream);
+  k_ingest_ptr<<<grid_for((long long)V + 1, 256, 8 * c.num_sms), 256, 0, c.stream>>>(optr.p, g->out_ptr.p,
+                                                                                    (long long)V + 1);
+  exclusive_scan_u32(icnt.p, iptr.p, (long long)V + 1, partial.p, c.num_sms, c.stream);
+  k_ingest_ptr<<<grid_for((long long)V + 1, 256, 8 * c.num_sms), 256, 0, c.stream>>>(iptr.p, g->in_ptr.p,
+                                                                                    (long long)V + 1);
+  SBP_CHECK_LAUNCH();
+  std::vector<int> op((size_t)V + 1), ip((size_t)V + 1);
+  SBP_CUDA(SBP_COPY_ASYNC(op.data(), g->out_ptr.p, ((size_t)V + 1) * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(ip.data(), g->in_ptr.p, ((size_t)V + 1) * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
   g->h_k.resize(V);
   for (int v = 0; v < V; ++v) {
     g->h_k[v] = (op[v + 1] - op[v]) + (ip[v + 1] - ip[v]);
@@ -1014,39 +1052,26 @@ SbpStatus sbp_graph_create(int32_t V, int64_t n, const int32_t* src, const int32
     if (V <= kMaxCap) g->heavy_cap = kMaxCap;   // distinct neighbour blocks <= B <= V
     else throw Error(SBP_ERR_UNSUPPORTED, "vertex degree above 4096 is not supported");
   }
-  // Graph::sort_vertices: degree = out + in - self, descending; ties by vertex id
-  std::vector<int> ord(V);
-  std::iota(ord.begin(), ord.end(), 0);
-  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return g->h_k[a] > g->h_k[b]; });
-  for (int i = 0; i < V; ++i) {
-    if ((double)i < 0.15 * (double)V) g->high.push_back(ord[i]);
-    else g->low.push_back(ord[i]);
+  // Graph::sort_vertices: degree = out + in - self, descending; ties by vertex id (a counting
+  // sort by degree, vertices in ascending order inside each degree)
+  {
+    std::vector<int> start((size_t)g->max_k + 2, 0), ord(V);
+    for (int v = 0; v < V; ++v) start[(size_t)(g->max_k - g->h_k[v]) + 1]++;
+    for (int k = 0; k <= g->max_k; ++k) start[k + 1] += start[k];
+    for (int v = 0; v < V; ++v) ord[start[g->max_k - g->h_k[v]]++] = v;
+    for (int i = 0; i < V; ++i) {
+      if ((double)i < 0.15 * (double)V) g->high.push_back(ord[i]);
+      else g->low.push_back(ord[i]);
+    }
   }
-  g->out_ptr.reserve(V + 1);
-  g->in_ptr.reserve(V + 1);
-  g->out_idx.reserve(m);
-  g->out_src.reserve(m);
-  g->in_idx.reserve(m);
-  g->self.reserve(V);
   g->identity.reserve(V);
   g->high_dev.reserve(g->high.size());
-  SBP_CUDA(SBP_COPY(g->out_ptr.p, op.data(), (V + 1) * sizeof(int), cudaMemcpyHostToDevice));
-  SBP_CUDA(SBP_COPY(g->in_ptr.p, ip.data(), (V + 1) * sizeof(int), cudaMemcpyHostToDevice));
-  if (m) {
-    std::vector<int> osrc(m);
-    for (int v = 0; v < V; ++v)
-      for (int e = op[v]; e < op[v + 1]; ++e) osrc[e] = v;
-    SBP_CUDA(SBP_COPY(g->out_src.p, osrc.data(), m * sizeof(int), cudaMemcpyHostToDevice));
-    SBP_CUDA(SBP_COPY(g->out_idx.p, oi.data(), m * sizeof(int), cudaMemcpyHostToDevice));
-    if (ip[V]) SBP_CUDA(SBP_COPY(g->in_idx.p, ii.data(), ip[V] * sizeof(int), cudaMemcpyHostToDevice));
-  }
-  SBP_CUDA(SBP_COPY(g->self.p, self.data(), V, cudaMemcpyHostToDevice));
-  std::vector<int> ident(V);
-  std::iota(ident.begin(), ident.end(), 0);
-  SBP_CUDA(SBP_COPY(g->identity.p, ident.data(), V * sizeof(int), cudaMemcpyHostToDevice));
+  k_iota<<<grid_for(V, 256, 8 * c.num_sms), 256, 0, c.stream>>>(g->identity.p, V);
+  SBP_CHECK_LAUNCH();
   if (!g->high.empty())
-    SBP_CUDA(SBP_COPY(g->high_dev.p, g->high.data(), g->high.size() * sizeof(int), cudaMemcpyHostToDevice));
-  (void)c;
+    SBP_CUDA(SBP_COPY_ASYNC(g->high_dev.p, g->high.data(), g->high.size() * sizeof(int), cudaMemcpyHostToDevice,
+                            c.stream));
+  c.sync();
   *out = g.release();
   SBP_API_END
 }

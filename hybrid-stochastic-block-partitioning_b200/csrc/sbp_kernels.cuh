@@ -81,6 +81,17 @@ __global__ void k_regrow_alloc(const int* __restrict__ full, const int* __restri
 __global__ void k_regrow_clear(const int* __restrict__ list, int n, const long long* __restrict__ base,
                                const int* __restrict__ mask, int2* slot);
 __global__ void k_regrow_fill(GraphView g, BlockView bm, const int* __restrict__ out_src);
+// sbp_ingest.cu
+__global__ void k_ingest_first(const int* __restrict__ src, const int* __restrict__ dst, long long n, int V,
+                               unsigned long long* keys, int* first, int tbits, int* bad);
+__global__ void k_ingest_keep(const int* __restrict__ src, const int* __restrict__ dst, long long n, int V,
+                              const unsigned long long* __restrict__ keys, const int* __restrict__ first, int tbits,
+                              int ib, unsigned long long* out_keys, unsigned long long* in_keys,
+                              unsigned long long* ctr, unsigned* out_cnt, unsigned* in_cnt, unsigned char* self);
+__global__ void k_ingest_fill(const unsigned long long* __restrict__ sorted, long long m, int ib,
+                              const int* __restrict__ other, int* idx, int* srcs);
+__global__ void k_ingest_ptr(const long long* __restrict__ in, int* out, long long n);
+__global__ void k_iota(int* out, int n);
 __global__ void k_recover_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved,
                                  int* prop, const int* old_block, const int* qr, const int* qs,
                                  const unsigned long long* last, unsigned gen);
