@@ -90,7 +90,7 @@ __device__ __forceinline__ double dxlogx(double a, double b) {
 
 // g(a) - g(b) for integer counts a, b >= 0 as (a - b) log a + b log(a / b), from a table of
 // log(x) = hi + lo (lo carries the bits below hi's last place):
-//  - a close to b (128 |a - b| <= b): log(a / b) = 2 atanh(z), z = (a - b) / (a + b), by its
+//  - a close to b (128 |a - b| <= b, b > 0): log(a / b) = 2 atanh(z), z = (a - b) / (a + b), by its
 //    Taylor series 2 (z + z^3/3 + z^5/5 + z^7/7), |z| <= 1/255, which keeps the relative
 //    accuracy that a difference of two table logs would lose;
 //  - otherwise log(a / b) = (hi_a - hi_b) + (lo_a - lo_b).
@@ -102,7 +102,7 @@ __device__ __forceinline__ double dxlogx_int(const double2* __restrict__ logt, i
     const int d = a - b;
     const double2 la = __ldg(logt + (a > 0 ? a : 1));
     double lab;
-    if (128LL * (d < 0 ? -(long long)d : (long long)d) <= (long long)b) {
+    if (b > 0 && 128LL * (d < 0 ? -(long long)d : (long long)d) <= (long long)b) {
       const double z = (double)d / ((double)a + (double)b), w = z * z;
       lab = 2.0 * z + 2.0 * z * w * (1.0 / 3.0 + w * (1.0 / 5.0 + w * (1.0 / 7.0)));
     } else {
