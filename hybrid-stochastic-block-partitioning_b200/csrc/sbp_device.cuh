@@ -49,7 +49,13 @@ struct RngParams {
   const uint4* replay;      // optional host-supplied stream (device copy)
   long long replay_records;
   uint32_t call;
+  int moves = 0;            // 1: replay records are proposals (s, 0, u_hi, u_lo), not random words
 };
+
+// The accept uniform of a proposal record: the bits of a double in [0, 1).
+__device__ __forceinline__ double record_uniform(uint4 x) {
+  return __hiloint2double((int)x.z, (int)x.w);
+}
 
 // Record for (a, b, tag); replay records are indexed by `slot`.
 __device__ __forceinline__ uint4 draw_record(const RngParams& p, uint32_t a, uint32_t b, uint32_t tag,
@@ -727,10 +733,13 @@ __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView
 //     gathered elements, so its block comes from the same pass;
 //  2. the multinomial walk over M[t,:] + M[:,t] picks s;
 //  3. move_delta gives delta-MDL and the Hastings correction.
+//
+// `given`: x is a proposal record (s, 0, u_hi, u_lo) of a replayed stream: the proposal is x.x
+// and the accept uniform the double of (x.z, x.w); steps 1 (without the neighbour pick) and 3.
 template <Store ST = Store::kAny>
 __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const BlockView& bm, int v, uint4 x,
                                                       const WarpTable& t, int lane, int* status, int* r_out,
-                                                      int* k_out_out, int* k_in_out) {
+                                                      int* k_out_out, int* k_in_out, bool given = false) {
   EvalResult res;
   const int r = bm.b[v];
   const int o0 = g.out_ptr[v], o1 = g.out_ptr[v + 1];
@@ -743,15 +752,21 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
   res.accepted = 0;
   res.dS = 0.0;
   res.H = 1.0;
-  const int idx = k > 0 ? (int)scale32(x.x, k) : -1;
+  const int idx = (k > 0 && !given) ? (int)scale32(x.x, k) : -1;
   const int tblk = gather_neighbour_blocks(g, bm, v, r, o0, k_out, i0, k, self, idx, t, lane, status);
-  res.t = k > 0 ? tblk : -1;
+  res.t = (k > 0 && !given) ? tblk : -1;
 
   NbPrefetch pre;
   prefetch_nb<ST>(bm, r, t, lane, &pre);
 
   int s;
-  if (k == 0) {
+  if (given) {
+    s = (int)x.x;
+    if (s < 0 || s >= bm.B) {   // a visit the stream has no proposal for
+      if (lane == 0) atomicOr(status, kErrReplay);
+      s = r;
+    }
+  } else if (k == 0) {
     s = random_block(r, bm.B, x.y);
   } else {
     const bool hashed = ST == Store::kHashed || (ST == Store::kAny && bm.sparse);
@@ -799,7 +814,7 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
   ap = ap >= 1.0 ? 1.0 : ap;
   res.dS = dS;
   res.H = H;
-  res.accepted = (u53(x.z, x.w) <= ap) ? 1 : 0;
+  res.accepted = ((given ? record_uniform(x) : u53(x.z, x.w)) <= ap) ? 1 : 0;
   return res;
 }
 

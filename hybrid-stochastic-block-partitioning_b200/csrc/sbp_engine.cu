@@ -9,6 +9,13 @@
 
 namespace sbpb {
 
+static thread_local char g_last_error[512];
+
+void set_last_error(const char* msg) {
+  std::snprintf(g_last_error, sizeof g_last_error, "%s", msg ? msg : "");
+}
+const char* last_error() { return g_last_error; }
+
 // Scratch of the sparse rebuild (grow-only, shared by all blockmodels).
 struct SortScratch {
   DevBuf<unsigned long long> keys, keysT, tmp, ukeys, partial;
@@ -421,7 +428,7 @@ static int gibbs_sweeps_graph(SbpBlockmodel& bm, const SbpGraph& g, const BatchP
 
 // finetune::{metropolis_hastings, asynchronous_gibbs, hybrid_mcmc}.
 void finetune(SbpBlockmodel& bm, SbpGraph& g, int algo, const SbpFinetuneOptions& opt, const SbpReplay* replay,
-              SbpStats& st) {
+              SbpStats& st, const SbpMoveReplay* moves) {
   Context& c = Context::get();
   std::memset(&st, 0, sizeof st);
   st.num_blocks = bm.B;
@@ -434,11 +441,13 @@ void finetune(SbpBlockmodel& bm, SbpGraph& g, int algo, const SbpFinetuneOptions
   SBP_CUDA(cudaEventRecord(c.ev0, c.stream));
   ReplayDev rp;
   rp.upload(replay);
+  rp.upload_moves(moves);
   RngParams rng;
   rng.seed = opt.seed;
   rng.replay = rp.records ? rp.buf.p : nullptr;
   rng.replay_records = rp.records;
   rng.call = opt.call;
+  rng.moves = rp.moves;
   const int max_sweeps = (opt.max_sweeps <= 0 || opt.max_sweeps > kMaxIterations) ? kMaxIterations : opt.max_sweeps;
   const bool bracket = opt.bracket_established != 0;
   SBP_CUDA(cudaMemsetAsync(c.counters, 0, 8 * sizeof(unsigned long long), c.stream));
@@ -626,7 +635,7 @@ static void carry_out_advanced(int B, int to_merge, const std::vector<int>& rptr
 }
 
 void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& opt, const SbpReplay* replay,
-                  int* best_out, double* dS_out, SbpStats& st) {
+                  int* best_out, double* dS_out, SbpStats& st, const SbpMoveReplay* moves) {
   Context& c = Context::get();
   const int B = bm.B;
   if (B < 2) throw Error(SBP_ERR_INVALID_ARGUMENT, "block merge needs at least two blocks");
@@ -634,6 +643,7 @@ void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& opt, co
   MergeScratch ms;
   ReplayDev rp;
   rp.upload(replay);
+  rp.upload_moves(moves);
   int nnz[2] = {0, 0};
   Csr rows, cols;
   if (bm.sparse) {
@@ -672,6 +682,7 @@ void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& opt, co
   rng.replay = rp.records ? rp.buf.p : nullptr;
   rng.replay_records = rp.records;
   rng.call = opt.call;
+  rng.moves = rp.moves;
   ms.best_s.reserve(B);
   ms.best_dS.reserve(B);
   SBP_CUDA(cudaMemsetAsync(c.counters, 0, 8 * sizeof(unsigned long long), c.stream));
@@ -795,12 +806,13 @@ int partition_merge(PartitionState& ps, SbpGraph& g, const SbpOptions& opt, SbpF
   mo.approximate = opt.approximate;
   mo.call = ps.call;
   mo.seed = opt.seed;
-  merge_blocks(ps.bm, g, mo, nullptr, nullptr, nullptr, ps.st);
+  merge_blocks(ps.bm, g, mo, nullptr, nullptr, nullptr, ps.st, ps.take_replay());
+  if (ps.replays) ps.block_counts.push_back(ps.bm.B);
   int algo = opt.algorithm;
   if (algo == SBP_ASYNC_GIBBS && !(ps.iteration < (float)opt.asynciterations)) algo = SBP_METROPOLIS_HASTINGS;
   fo->batches = opt.batches;
   fo->bracket_established = !ps.t.s[2].empty;
-  fo->max_sweeps = 0;
+  fo->max_sweeps = ps.max_sweeps;
   fo->call = ps.call;
   fo->seed = opt.seed;
   return algo;
@@ -830,21 +842,32 @@ void partition_finish_round(PartitionState& ps, SbpGraph& g, const SbpStats& fs,
   ps.bm.num_blocks_to_merge = to_merge;
 }
 
-void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st, const FinetuneStep* step) {
+void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st, const FinetuneStep* step,
+               PartitionReplay* replay) {
   Context& c = Context::get();
   cudaEvent_t t0, t1;
   SBP_CUDA(cudaEventCreate(&t0));
   SBP_CUDA(cudaEventCreate(&t1));
   SBP_CUDA(cudaEventRecord(t0, c.stream));
   PartitionState ps;
+  if (replay) {
+    ps.replays = replay->calls;
+    ps.nreplays = replay->num_calls;
+    ps.max_sweeps = replay->max_sweeps;
+  }
   partition_begin(ps, g);
   while (!ps.done) {
     SbpFinetuneOptions fo;
     const int algo = partition_merge(ps, g, opt, &fo);
     SbpStats fs;
     if (step) (*step)(ps.bm, g, algo, fo, fs);
-    else finetune(ps.bm, g, algo, fo, nullptr, fs);
+    else finetune(ps.bm, g, algo, fo, nullptr, fs, ps.take_replay());
+    if (ps.replays) ps.block_counts.push_back(ps.bm.B);
     partition_finish_round(ps, g, fs, out);
+  }
+  if (replay) {
+    replay->calls_made = ps.next_replay;
+    replay->block_counts = ps.block_counts;
   }
   st = ps.st;
   SBP_CUDA(cudaEventRecord(t1, c.stream));
@@ -866,15 +889,15 @@ void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st, const
   return SBP_OK;                                           \
   }                                                        \
   catch (const Error& e) {                                 \
-    g_last_error = e.what();                               \
+    set_last_error(e.what());                               \
     return e.code;                                         \
   }                                                        \
   catch (const std::bad_alloc&) {                          \
-    g_last_error = "host allocation failed";               \
+    set_last_error("host allocation failed");               \
     return SBP_ERR_OUT_OF_MEMORY;                          \
   }                                                        \
   catch (const std::exception& e) {                        \
-    g_last_error = e.what();                               \
+    set_last_error(e.what());                               \
     return SBP_ERR_CUDA;                                   \
   }
 
@@ -883,7 +906,7 @@ void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st, const
 
 extern "C" {
 
-const char* sbp_last_error(void) { return g_last_error.c_str(); }
+const char* sbp_last_error(void) { return sbpb::last_error(); }
 
 int32_t sbp_device_count(void) {
   int n = 0;
@@ -1250,6 +1273,51 @@ SbpStatus sbp_get_degrees(const SbpBlockmodel* bm, int32_t* d_out, int32_t* d_in
   SBP_API_END
 }
 
+SbpStatus sbp_set_degrees(SbpBlockmodel* bm, const int32_t* d) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(bm && d, "NULL argument");
+  Context& c = Context::get();
+  SBP_CUDA(SBP_COPY_ASYNC(bm->d.p, d, bm->B * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  c.sync();
+  SBP_API_END
+}
+
+SbpStatus sbp_mdl_of_cells(int32_t num_blocks, int64_t nnz, const int32_t* rows, const int32_t* cols,
+                           const int32_t* counts, const int32_t* d_out, const int32_t* d_in, int32_t num_vertices,
+                           int64_t num_edges, double* out) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(out && d_out && d_in && num_blocks > 0 && nnz >= 0 && num_vertices > 0 && num_edges > 0,
+              "bad argument");
+  SBP_REQUIRE(nnz == 0 || (rows && cols && counts), "NULL cell arrays");
+  for (int64_t i = 0; i < nnz; ++i) {
+    SBP_REQUIRE(rows[i] >= 0 && rows[i] < num_blocks && cols[i] >= 0 && cols[i] < num_blocks, "cell out of range");
+    SBP_REQUIRE(counts[i] > 0 && d_out[rows[i]] > 0 && d_in[cols[i]] > 0,
+                "a nonzero cell needs positive counts and degrees (the reference exits on a zero degree)");
+  }
+  Context& c = Context::get();
+  DevBuf<int> dr, dc, dv, ddo, ddi;
+  const size_t n = (size_t)std::max<int64_t>(nnz, 1);
+  dr.reserve(n);
+  dc.reserve(n);
+  dv.reserve(n);
+  ddo.reserve(num_blocks);
+  ddi.reserve(num_blocks);
+  if (nnz > 0) {
+    SBP_CUDA(SBP_COPY_ASYNC(dr.p, rows, nnz * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    SBP_CUDA(SBP_COPY_ASYNC(dc.p, cols, nnz * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    SBP_CUDA(SBP_COPY_ASYNC(dv.p, counts, nnz * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  }
+  SBP_CUDA(SBP_COPY_ASYNC(ddo.p, d_out, num_blocks * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(ddi.p, d_in, num_blocks * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+  k_mdl_cells_list<<<c.npartial, 256, 0, c.stream>>>(dr.p, dc.p, dv.p, nnz, ddo.p, ddi.p, c.partial);
+  k_mdl_cells_list_final<<<1, 256, 0, c.stream>>>(c.partial, c.npartial, num_vertices, num_edges, num_blocks,
+                                                  c.scalar);
+  SBP_CHECK_LAUNCH();
+  SBP_CUDA(SBP_COPY_ASYNC(out, c.scalar, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  SBP_API_END
+}
+
 SbpStatus sbp_mdl(const SbpBlockmodel* bm, const SbpGraph* g, double* out) {
   SBP_API_BEGIN
   SBP_REQUIRE(bm && g && out && bm->V == g->V, "bad argument");
@@ -1343,6 +1411,52 @@ SbpStatus sbp_merge_blocks(SbpBlockmodel* bm, const SbpGraph* g, const SbpMergeO
   SbpStats st;
   std::memset(&st, 0, sizeof st);
   merge_blocks(*bm, const_cast<SbpGraph&>(*g), *opt, replay, best_merge, delta_mdl, st);
+  if (stats) *stats = st;
+  SBP_API_END
+}
+
+SbpStatus sbp_finetune_replayed(SbpBlockmodel* bm, const SbpGraph* g, int32_t algorithm, const SbpFinetuneOptions* opt,
+                                const SbpMoveReplay* replay, SbpStats* stats) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(bm && g && opt && bm->V == g->V, "bad argument");
+  SBP_REQUIRE(replay && replay->proposal && replay->uniform && replay->records > 0,
+              "a finetune replay needs proposals and uniforms");
+  SbpStats st;
+  finetune(*bm, const_cast<SbpGraph&>(*g), algorithm, *opt, nullptr, st, replay);
+  if (stats) *stats = st;
+  SBP_API_END
+}
+
+SbpStatus sbp_merge_blocks_replayed(SbpBlockmodel* bm, const SbpGraph* g, const SbpMergeOptions* opt,
+                                    const SbpMoveReplay* replay, int32_t* best_merge, double* delta_mdl,
+                                    SbpStats* stats) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(bm && g && opt && bm->V == g->V, "bad argument");
+  SBP_REQUIRE(replay && replay->proposal && replay->records > 0, "a merge replay needs proposals");
+  SbpStats st;
+  std::memset(&st, 0, sizeof st);
+  merge_blocks(*bm, const_cast<SbpGraph&>(*g), *opt, nullptr, best_merge, delta_mdl, st, replay);
+  if (stats) *stats = st;
+  SBP_API_END
+}
+
+SbpStatus sbp_partition_replayed(const SbpGraph* g, const SbpOptions* opt, int32_t max_sweeps, int32_t num_calls,
+                                 const SbpMoveReplay* calls, int32_t* out_assignment, int32_t* block_counts,
+                                 int32_t* calls_made, SbpStats* stats) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(g && opt && out_assignment && calls && num_calls > 0, "NULL argument");
+  SBP_REQUIRE(opt->algorithm >= 0 && opt->algorithm <= 2, "unknown algorithm");
+  SBP_REQUIRE(opt->batches >= 1, "batches must be >= 1");
+  for (int k = 0; k < num_calls; ++k) SBP_REQUIRE(calls[k].proposal && calls[k].records > 0, "empty call stream");
+  PartitionReplay rp;
+  rp.calls = calls;
+  rp.num_calls = num_calls;
+  rp.max_sweeps = max_sweeps;
+  SbpStats st;
+  partition(const_cast<SbpGraph&>(*g), *opt, out_assignment, st, nullptr, &rp);
+  if (calls_made) *calls_made = rp.calls_made;
+  if (block_counts)
+    for (size_t k = 0; k < rp.block_counts.size() && k < (size_t)num_calls; ++k) block_counts[k] = rp.block_counts[k];
   if (stats) *stats = st;
   SBP_API_END
 }

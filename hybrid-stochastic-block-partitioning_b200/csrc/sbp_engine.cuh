@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/sbp_b200.h"
+#include "sbp_error.h"
 #include "sbp_kernels.cuh"
 #include "sbp_sort.cuh"
 
@@ -30,7 +31,6 @@ struct Error : std::runtime_error {
   Error(SbpStatus c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
-inline thread_local std::string g_last_error;
 
 #define SBP_CUDA(x)                                                                                     \
   do {                                                                                                  \
@@ -221,7 +221,8 @@ struct Context {
     sync();
     if (st) {
       SBP_CUDA(cudaMemsetAsync(status, 0, sizeof(int), stream));
-      if (st & kErrReplay) throw Error(SBP_ERR_REPLAY, "replay stream shorter than the run needs");
+      if (st & kErrReplay)
+        throw Error(SBP_ERR_REPLAY, "replay stream shorter than the run needs, or a replayed proposal out of range");
       char msg[160];
       snprintf(msg, sizeof msg, "device status 0x%x (table overflow=1, multinomial walk=2, bounds=8)", st);
       throw Error(SBP_ERR_DEVICE, msg);
@@ -494,11 +495,28 @@ struct MhResult {
 struct ReplayDev {
   DevBuf<uint4> buf;
   long long records = 0;
+  int moves = 0;   // 1: the records are proposals (sbp_*_replayed), 0: random words
   void upload(const SbpReplay* r) {
     if (!r || !r->words || r->records <= 0) return;
     buf.reserve((size_t)r->records);
     SBP_CUDA(SBP_COPY(buf.p, r->words, (size_t)r->records * sizeof(uint4), cudaMemcpyHostToDevice));
     records = r->records;
+  }
+  // Proposal records (s, 0, u_hi, u_lo): the proposed block and the bits of the accept uniform
+  // (2.0, which never accepts, where the stream has none).
+  void upload_moves(const SbpMoveReplay* r) {
+    if (!r || !r->proposal || r->records <= 0) return;
+    std::vector<uint4> h((size_t)r->records);
+    for (long long i = 0; i < r->records; ++i) {
+      const double u = r->uniform ? r->uniform[i] : 2.0;
+      unsigned long long bits;
+      std::memcpy(&bits, &u, sizeof bits);
+      h[i] = make_uint4((unsigned)r->proposal[i], 0u, (unsigned)(bits >> 32), (unsigned)bits);
+    }
+    buf.reserve((size_t)r->records);
+    SBP_CUDA(SBP_COPY(buf.p, h.data(), h.size() * sizeof(uint4), cudaMemcpyHostToDevice));
+    records = r->records;
+    moves = 1;
   }
 };
 
@@ -559,6 +577,18 @@ struct PartitionState {
   uint32_t call = 0;
   SbpStats st;
   bool done = false;
+  // A partition driven by recorded streams (sbp_partition_replayed): the k-th merge or finetune
+  // call takes replays[k]; the finetune sweep cap and the blocks after every call.
+  const SbpMoveReplay* replays = nullptr;
+  int nreplays = 0, next_replay = 0;
+  int max_sweeps = 0;
+  std::vector<int> block_counts;
+  const SbpMoveReplay* take_replay() {
+    if (!replays) return nullptr;
+    if (next_replay >= nreplays)
+      throw Error(SBP_ERR_REPLAY, "the partition makes more merge / finetune calls than the replay holds");
+    return &replays[next_replay++];
+  }
 };
 
 // Engine steps shared by the translation units (defined in sbp_engine.cu).
@@ -572,12 +602,24 @@ void gibbs_apply(SbpBlockmodel& bm, const SbpGraph& g, int batch);
 // One asynchronous-Gibbs batch with the plain proposal (evaluation + apply).
 void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, int bt, RngParams rng, int sweep);
 // finetune::{metropolis_hastings, asynchronous_gibbs, hybrid_mcmc} on the device.
+// `moves` (optional) replays proposals instead of random words.
 void finetune(SbpBlockmodel& bm, SbpGraph& g, int algo, const SbpFinetuneOptions& opt, const SbpReplay* replay,
-              SbpStats& st);
+              SbpStats& st, const SbpMoveReplay* moves = nullptr);
 // The finetune step of a partition, replaceable (the learned proposal's partition).
 using FinetuneStep = std::function<void(SbpBlockmodel&, SbpGraph&, int, const SbpFinetuneOptions&, SbpStats&)>;
-// sbp::stochastic_block_partition; `step` = nullptr runs the plain finetune.
-void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st, const FinetuneStep* step = nullptr);
+// Recorded streams of a partition's merge and finetune calls, in call order (in), and what
+// the partition made of them (out).
+struct PartitionReplay {
+  const SbpMoveReplay* calls = nullptr;
+  int num_calls = 0;
+  int max_sweeps = 0;
+  int calls_made = 0;
+  std::vector<int> block_counts;
+};
+// sbp::stochastic_block_partition; `step` = nullptr runs the plain finetune; `replay` drives
+// every call from recorded streams.
+void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st, const FinetuneStep* step = nullptr,
+               PartitionReplay* replay = nullptr);
 // The partition loop's steps: start at B = V; merge step of the next round (returns the
 // round's finetune algorithm and fills its options); statistics and golden-section step after
 // the round's finetune (writes `out` and sets done when the search ends).
@@ -586,7 +628,7 @@ int partition_merge(PartitionState& ps, SbpGraph& g, const SbpOptions& opt, SbpF
 void partition_finish_round(PartitionState& ps, SbpGraph& g, const SbpStats& fs, int* out);
 // block_merge::merge_blocks; best_out / dS_out optional.
 void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& opt, const SbpReplay* replay,
-                  int* best_out, double* dS_out, SbpStats& st);
+                  int* best_out, double* dS_out, SbpStats& st, const SbpMoveReplay* moves = nullptr);
 Snapshot snapshot(SbpBlockmodel& bm);
 void restore(SbpBlockmodel& bm, SbpGraph& g, const Snapshot& x);
 // One sequential Metropolis-Hastings pass over a device list of n vertices.

@@ -88,7 +88,7 @@ __device__ __forceinline__ void gibbs_eval_body(GraphView g, BlockView bm, const
     const int v = verts[i];
     const uint4 x = draw_record(rng, (uint32_t)v, (uint32_t)sweep, 0u, (long long)sweep * g.V + v, status);
     int r, k_out, k_in;
-    const EvalResult res = evaluate_vertex<ST>(g, bm, v, x, t, lane, status, &r, &k_out, &k_in);
+    const EvalResult res = evaluate_vertex<ST>(g, bm, v, x, t, lane, status, &r, &k_out, &k_in, rng.moves != 0);
     c_visit++;
     if (res.s != r) c_moved++;
     if (res.accepted) {
@@ -224,6 +224,29 @@ __global__ void k_mdl(GraphView g, BlockView bm, const int* __restrict__ out_src
   }
 }
 
+// entropy::mdl (src/entropy.cpp:584-589) from a list of nonzero cells, each term as
+// Blockmodel::log_posterior_probability (src/blockmodel/blockmodel.cpp:267-285) forms it.
+// Deterministic: grid-stride partials per CTA, then one CTA sums them in order.
+__global__ void k_mdl_cells_list(const int* __restrict__ rows, const int* __restrict__ cols,
+                                 const int* __restrict__ counts, long long nnz, const int* __restrict__ d_out,
+                                 const int* __restrict__ d_in, double* partial) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += stride) {
+    const double m = counts[i];
+    acc += m * log(m / ((double)d_out[rows[i]] * (double)d_in[cols[i]]));
+  }
+  const double t = block_sum(acc, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = t;
+}
+
+__global__ void k_mdl_cells_list_final(const double* partial, int n, int V, long long E, int B, double* out) {
+  __shared__ double red[32];
+  const double v = mdl_final_value(partial, n, V, E, B, red);
+  if (threadIdx.x == 0) *out = v;
+}
+
 // ------------------------------------------------------------------------------------------
 // Metropolis-Hastings over a vertex list, exact sequential semantics, one CTA.
 // Round: the W warps evaluate the next W vertices against the current state; the first
@@ -260,7 +283,7 @@ __global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, i
     if (i < n) {
       v = verts[i];
       const uint4 x = draw_record(rng, (uint32_t)v, (uint32_t)sweep, 0u, (long long)sweep * g.V + v, status);
-      res = evaluate_vertex(g, bm, v, x, t, lane, status, &r, &k_out, &k_in);
+      res = evaluate_vertex(g, bm, v, x, t, lane, status, &r, &k_out, &k_in, rng.moves != 0);
     }
     if (lane == 0) {
       s_acc[warp] = (i < n) ? res.accepted : 0;
@@ -580,7 +603,13 @@ __global__ void k_merge_propose(BlockView bm, Csr rows, Csr cols, RngParams rng,
     for (int i = 0; i < kProposalsPerBlock; ++i) {
       const uint4 x = draw_record(rng, (uint32_t)r, (uint32_t)i, 1u, (long long)r * kProposalsPerBlock + i, status);
       int s;
-      if (k == 0) {
+      if (rng.moves) {   // a replayed proposal
+        s = (int)x.x;
+        if (s < 0 || s >= B || s == r) {
+          if (lane == 0) atomicOr(status, kErrReplay);
+          s = r == 0 ? 1 : 0;
+        }
+      } else if (k == 0) {
         s = random_block(r, B, x.y);
       } else {
         const long long target = scale32(x.x, k);

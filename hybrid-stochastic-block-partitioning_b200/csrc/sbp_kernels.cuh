@@ -31,6 +31,12 @@ struct Csr {
 __global__ void k_rebuild_global(GraphView g, BlockView bm);
 __global__ void k_rebuild_smem(GraphView g, BlockView bm);
 __global__ void k_rebuild_degrees(BlockView bm);
+// entropy::mdl of host-supplied nonzero cells (row, col, count) and block degrees: the per-cell
+// form count * log(count / (d_out[row] * d_in[col])) of Blockmodel::log_posterior_probability.
+__global__ void k_mdl_cells_list(const int* __restrict__ rows, const int* __restrict__ cols,
+                                 const int* __restrict__ counts, long long nnz, const int* __restrict__ d_out,
+                                 const int* __restrict__ d_in, double* partial);
+__global__ void k_mdl_cells_list_final(const double* partial, int n, int V, long long E, int B, double* out);
 __global__ void k_mdl(GraphView g, BlockView bm, const int* __restrict__ out_src, int cells, double* partial,
                       unsigned* done, double* out, SweepCtl* ctl, cudaGraphConditionalHandle loop);
 // Asynchronous-Gibbs evaluation compiled for one storage of the block matrix.

@@ -611,15 +611,15 @@ static std::vector<float> mlp_init(uint64_t seed) {
   return SBP_OK;                             \
   }                                          \
   catch (const Error& e) {                   \
-    g_last_error = e.what();                 \
+    set_last_error(e.what());                 \
     return e.code;                           \
   }                                          \
   catch (const std::bad_alloc&) {            \
-    g_last_error = "host allocation failed"; \
+    set_last_error("host allocation failed"); \
     return SBP_ERR_OUT_OF_MEMORY;            \
   }                                          \
   catch (const std::exception& e) {          \
-    g_last_error = e.what();                 \
+    set_last_error(e.what());                 \
     return SBP_ERR_CUDA;                     \
   }
 

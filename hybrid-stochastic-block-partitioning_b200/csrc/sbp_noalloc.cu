@@ -20,11 +20,14 @@
 #include <mutex>
 
 #include "../../include/sbp_b200.h"
+#include "sbp_error.h"
 
 namespace sbpb_noalloc {
 
 constexpr int kNoAllocMaxBlocks = 32768;
 constexpr int kMaxDevices = 64;
+constexpr int kFinalThreads = 256;   // CTA size of k_noalloc_final (its reduction array is sized from it)
+static_assert(kFinalThreads % 32 == 0 && kFinalThreads <= 1024, "k_noalloc_final needs whole warps");
 
 // Per-row partial sums of M log M.  In host code this name is only a handle for
 // cudaGetSymbolAddress, never a device address.
@@ -47,10 +50,11 @@ __global__ void k_noalloc_rows(const int* __restrict__ M, int B, long long ld, d
 }
 
 // Fixed-order sum of the row partials and the degree terms, then the MDL formula
-// (entropy::mdl, src/entropy.cpp:584-589).  One CTA of 256 threads.
-__global__ void k_noalloc_final(const double* rows, int B, const int* __restrict__ d_out,
-                                const int* __restrict__ d_in, int V, long long E, double* result) {
-  __shared__ double red[8];
+// (entropy::mdl, src/entropy.cpp:584-589).  One CTA of kFinalThreads threads.
+__global__ void __launch_bounds__(kFinalThreads) k_noalloc_final(const double* rows, int B, const int* __restrict__ d_out,
+                                                                 const int* __restrict__ d_in, int V, long long E,
+                                                                 double* result) {
+  __shared__ double red[kFinalThreads / 32];
   double acc = 0.0;
   for (int i = threadIdx.x; i < B; i += blockDim.x)
     acc += rows[i] - na_xlogx((double)d_out[i]) - na_xlogx((double)d_in[i]);
@@ -59,7 +63,7 @@ __global__ void k_noalloc_final(const double* rows, int B, const int* __restrict
   __syncthreads();
   if (threadIdx.x == 0) {
     double L = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) L += red[w];
+    for (int w = 0; w < kFinalThreads / 32; ++w) L += red[w];
     const double x = pow((double)B, 2) / (double)E;
     const double h = ((1 + x) * log(1 + x)) - (x * log(x));
     *result = ((double)E * h) + ((double)V * log((double)B)) - L;
@@ -86,9 +90,12 @@ static cudaError_t scratch_for_current_device(double** out) {
   return cudaSuccess;
 }
 
-// Last failure of this entry point on the calling thread (kept for debuggers; the status code
-// is the interface).  A fixed buffer, so reporting an error allocates nothing either.
-static thread_local char g_msg[256];
+// Records a failure for sbp_last_error() (a fixed per-thread buffer: nothing is allocated).
+static void fail(const char* what, const char* detail = "") {
+  char msg[256];
+  snprintf(msg, sizeof msg, "sbp_mdl_device_noalloc: %s%s", what, detail);
+  sbpb::set_last_error(msg);
+}
 
 }  // namespace sbpb_noalloc
 
@@ -99,19 +106,20 @@ extern "C" SbpStatus sbp_mdl_device_noalloc(const int32_t* d_matrix, int32_t num
   using namespace sbpb_noalloc;
   if (!d_matrix || !d_degrees_out || !d_degrees_in || !d_result || num_blocks < 1 || ld < num_blocks ||
       num_vertices < 1 || num_edges < 1) {
-    snprintf(g_msg, sizeof g_msg, "sbp_mdl_device_noalloc: bad argument");
+    fail("bad argument (NULL pointer, ld < num_blocks or a size below 1)");
     return SBP_ERR_INVALID_ARGUMENT;
   }
   if (num_blocks > kNoAllocMaxBlocks) {
-    snprintf(g_msg, sizeof g_msg,
-             "sbp_mdl_device_noalloc: %d blocks exceed the %d-block limit of its static scratch array",
-             num_blocks, kNoAllocMaxBlocks);
+    char what[128];
+    snprintf(what, sizeof what, "%d blocks exceed the %d-block limit of its static scratch array", num_blocks,
+             kNoAllocMaxBlocks);
+    fail(what);
     return SBP_ERR_UNSUPPORTED;
   }
   double* rows = nullptr;
   cudaError_t e = scratch_for_current_device(&rows);
   if (e != cudaSuccess) {
-    snprintf(g_msg, sizeof g_msg, "sbp_mdl_device_noalloc: scratch lookup failed: %s", cudaGetErrorString(e));
+    fail("scratch lookup failed: ", cudaGetErrorString(e));
     return SBP_ERR_CUDA;
   }
   cudaStream_t s = (cudaStream_t)stream;
@@ -119,10 +127,10 @@ extern "C" SbpStatus sbp_mdl_device_noalloc(const int32_t* d_matrix, int32_t num
   int grid = (num_blocks + warps_per_cta - 1) / warps_per_cta;
   if (grid > 4096) grid = 4096;
   k_noalloc_rows<<<grid, 32 * warps_per_cta, 0, s>>>(d_matrix, num_blocks, ld, rows);
-  k_noalloc_final<<<1, 256, 0, s>>>(rows, num_blocks, d_degrees_out, d_degrees_in, num_vertices, num_edges, d_result);
+  k_noalloc_final<<<1, kFinalThreads, 0, s>>>(rows, num_blocks, d_degrees_out, d_degrees_in, num_vertices, num_edges, d_result);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
-    snprintf(g_msg, sizeof g_msg, "sbp_mdl_device_noalloc: launch failed: %s", cudaGetErrorString(e));
+    fail("launch failed: ", cudaGetErrorString(e));
     return SBP_ERR_CUDA;
   }
   return SBP_OK;

@@ -90,8 +90,10 @@ __global__ void k_scan_top(unsigned long long* partial, int g) {   // single thr
 }
 
 // out[i] = partial[cta] + exclusive prefix inside the tile (tile-serial chunks of blockDim).
+// in and out may be the same array (the radix sort scans its histogram in place): every
+// element is read by the thread that later writes it, so neither pointer is __restrict__.
 template <class OutT>
-__global__ void k_scan_down(const unsigned* __restrict__ in, OutT* __restrict__ out, long long n, long long tile,
+__global__ void k_scan_down(const unsigned* in, OutT* out, long long n, long long tile,
                             const unsigned long long* __restrict__ partial) {
   __shared__ unsigned long long wsum[32];
   __shared__ unsigned long long carry;

@@ -34,7 +34,8 @@ EXPORTED = [
     "sbp_mlp_gradients", "sbp_mlp_train", "sbp_dataset_create", "sbp_dataset_destroy", "sbp_dataset_size",
     "sbp_dataset_append", "sbp_dataset_read", "sbp_vertex_features", "sbp_learned_evaluate", "sbp_learned_q",
     "sbp_collect_moves", "sbp_finetune_learned", "sbp_partition_learned", "sbp_partition_batched",
-    "sbp_batched_reset_tuning", "sbp_mdl_device_noalloc",
+    "sbp_batched_reset_tuning", "sbp_mdl_device_noalloc", "sbp_finetune_replayed", "sbp_merge_blocks_replayed",
+    "sbp_partition_replayed", "sbp_set_degrees", "sbp_mdl_of_cells",
 ]
 
 MLP_FEATURES, MLP_OUTPUTS, MLP_SLOTS, MLP_ESCAPE, MLP_PARAMS = 64, 16, 14, 14, 26896
@@ -48,6 +49,11 @@ class SbpError(RuntimeError):
 
 class Replay(ctypes.Structure):
     _fields_ = [("words", ctypes.POINTER(ctypes.c_uint32)), ("records", ctypes.c_int64)]
+
+
+class MoveReplay(ctypes.Structure):
+    _fields_ = [("proposal", ctypes.POINTER(ctypes.c_int32)), ("uniform", ctypes.POINTER(ctypes.c_double)),
+                ("records", ctypes.c_int64)]
 
 
 class Stats(ctypes.Structure):
@@ -155,6 +161,15 @@ def load(path=LIB_PATH):
     L.sbp_merge_blocks.argtypes = [vp, vp, ctypes.POINTER(MergeOptions), ctypes.POINTER(Replay), _i32p, _f64p,
                                    ctypes.POINTER(Stats)]
     L.sbp_partition.argtypes = [vp, ctypes.POINTER(Options), _i32p, ctypes.POINTER(Stats)]
+    L.sbp_finetune_replayed.argtypes = [vp, vp, ctypes.c_int32, ctypes.POINTER(FinetuneOptions),
+                                        ctypes.POINTER(MoveReplay), ctypes.POINTER(Stats)]
+    L.sbp_merge_blocks_replayed.argtypes = [vp, vp, ctypes.POINTER(MergeOptions), ctypes.POINTER(MoveReplay), _i32p,
+                                            _f64p, ctypes.POINTER(Stats)]
+    L.sbp_set_degrees.argtypes = [vp, _i32p]
+    L.sbp_mdl_of_cells.argtypes = [ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _i32p, _i32p, _i32p, ctypes.c_int32,
+                                   ctypes.c_int64, _f64p]
+    L.sbp_partition_replayed.argtypes = [vp, ctypes.POINTER(Options), ctypes.c_int32, ctypes.c_int32,
+                                         ctypes.POINTER(MoveReplay), _i32p, _i32p, _i32p, ctypes.POINTER(Stats)]
     L.sbp_mdl_device_noalloc.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, vp, vp, ctypes.c_int32, ctypes.c_int64,
                                          vp, vp]
     f32p = ctypes.POINTER(ctypes.c_float)
@@ -189,6 +204,11 @@ def load(path=LIB_PATH):
 def _check(rc):
     if rc != 0:
         raise SbpError(rc, _lib.sbp_last_error().decode())
+
+
+def last_error():
+    """sbp_last_error(): the text of the calling thread's last failure."""
+    return _lib.sbp_last_error().decode()
 
 
 def _p(a, t=_i32p):
@@ -370,6 +390,22 @@ class finetune:
         return st.as_dict()
 
     @staticmethod
+    def replayed(blockmodel, algorithm, proposal, uniform, batches=10, bracket=False, max_sweeps=0):
+        """finetune with the proposals and accept uniforms of a recorded stream
+        (sbp_finetune_replayed): proposal[t*V + v], uniform[t*V + v] for vertex v in sweep t."""
+        prop = np.ascontiguousarray(proposal, np.int32)
+        uni = np.ascontiguousarray(uniform, np.float64)
+        if prop.shape != uni.shape:
+            raise ValueError("proposal and uniform streams differ in length")
+        opt = FinetuneOptions(int(batches), int(bool(bracket)), int(max_sweeps), 0, 0)
+        rp = MoveReplay(_p(prop), _p(uni, _f64p), len(prop))
+        st = Stats()
+        algo = ALGORITHMS[algorithm] if isinstance(algorithm, str) else int(algorithm)
+        _check(_lib.sbp_finetune_replayed(blockmodel.h, blockmodel.graph.h, algo, ctypes.byref(opt), ctypes.byref(rp),
+                                          ctypes.byref(st)))
+        return st.as_dict()
+
+    @staticmethod
     def metropolis_hastings(blockmodel, **kw):
         return finetune.run(blockmodel, METROPOLIS_HASTINGS, **kw)
 
@@ -396,6 +432,21 @@ class block_merge:
         del keep
         return dict(best=best, dS=dS, **st.as_dict())
 
+    @staticmethod
+    def merge_blocks_replayed(blockmodel, proposal, approximate=True):
+        """merge_blocks with every proposal taken from a recorded stream (sbp_merge_blocks_replayed):
+        proposal[block*10 + i] is proposal i of a block."""
+        B = blockmodel.B
+        best = np.zeros(B, np.int32)
+        dS = np.zeros(B, np.float64)
+        prop = np.ascontiguousarray(proposal, np.int32)
+        opt = MergeOptions(int(bool(approximate)), 0, 0)
+        rp = MoveReplay(_p(prop), None, len(prop))
+        st = Stats()
+        _check(_lib.sbp_merge_blocks_replayed(blockmodel.h, blockmodel.graph.h, ctypes.byref(opt), ctypes.byref(rp),
+                                              _p(best), _p(dS, _f64p), ctypes.byref(st)))
+        return dict(best=best, dS=dS, **st.as_dict())
+
 
 def mdl_device_noalloc(d_matrix, num_blocks, ld, d_degrees_out, d_degrees_in, num_vertices, num_edges, d_result,
                        stream=None):
@@ -405,8 +456,7 @@ def mdl_device_noalloc(d_matrix, num_blocks, ld, d_degrees_out, d_degrees_in, nu
     rc = load().sbp_mdl_device_noalloc(d_matrix, int(num_blocks), int(ld), d_degrees_out, d_degrees_in,
                                        int(num_vertices), int(num_edges), d_result, stream)
     if rc != 0:
-        raise SbpError(rc, "sbp_mdl_device_noalloc rejected the call (limit: 32768 blocks)"
-                       if rc == 3 else "sbp_mdl_device_noalloc failed")
+        raise SbpError(rc, last_error())
 
 
 class sbp:
@@ -419,6 +469,30 @@ class sbp:
         st = Stats()
         _check(_lib.sbp_partition(graph.h, ctypes.byref(opt), _p(out), ctypes.byref(st)))
         return out, st.as_dict()
+
+    @staticmethod
+    def stochastic_block_partition_replayed(graph, calls, algorithm="async_gibbs", batches=10, approximate=True,
+                                            max_sweeps=0):
+        """sbp_partition_replayed: `calls` lists the recorded stream of every merge and finetune
+        call in call order, each (proposal, uniform) with uniform None for a merge.  Returns
+        (assignment, stats, blocks after each call)."""
+        algo = ALGORITHMS[algorithm] if isinstance(algorithm, str) else int(algorithm)
+        opt = Options(algo, int(batches), int(bool(approximate)), 2**31 - 1, 0)
+        keep = []
+        arr = (MoveReplay * len(calls))()
+        for k, (prop, uni) in enumerate(calls):
+            p = np.ascontiguousarray(prop, np.int32)
+            u = None if uni is None else np.ascontiguousarray(uni, np.float64)
+            keep.append((p, u))
+            arr[k] = MoveReplay(_p(p), None if u is None else _p(u, _f64p), len(p))
+        out = np.zeros(graph.V, np.int32)
+        counts = np.zeros(len(calls), np.int32)
+        made = ctypes.c_int32()
+        st = Stats()
+        _check(_lib.sbp_partition_replayed(graph.h, ctypes.byref(opt), int(max_sweeps), len(calls), arr, _p(out),
+                                           _p(counts), ctypes.byref(made), ctypes.byref(st)))
+        del keep
+        return out, st.as_dict(), counts[:made.value]
 
 
 # ------------------------------------------------------------------------------------------

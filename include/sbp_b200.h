@@ -162,6 +162,19 @@ SbpStatus sbp_get_block_matrix(const SbpBlockmodel *bm, int32_t *out);
 /* Blockmodel::degrees_out / degrees_in / degrees. Each out: B ints. */
 SbpStatus sbp_get_degrees(const SbpBlockmodel *bm, int32_t *d_out, int32_t *d_in, int32_t *d);
 
+/* Blockmodel::degrees(std::vector<int>) (include/blockmodel/blockmodel.hpp:148): overwrite the
+ * block degrees d (B ints), e.g. with the drifted values of a reference Blockmodel being mirrored. */
+SbpStatus sbp_set_degrees(SbpBlockmodel *bm, const int32_t *d);
+
+/* entropy::mdl(blockmodel, num_vertices, num_edges) (src/entropy.cpp:584-589) of block counts
+ * given on the host as nonzero cells (rows[i], cols[i], counts[i]; ISparseMatrix::nonzero() and
+ * values()) and block degrees (num_blocks ints each), with each term count * log(count /
+ * (d_out[row] * d_in[col])) in FP64 (Blockmodel::log_posterior_probability,
+ * src/blockmodel/blockmodel.cpp:267-285).  Needs no graph or blockmodel handle. */
+SbpStatus sbp_mdl_of_cells(int32_t num_blocks, int64_t nnz, const int32_t *rows, const int32_t *cols,
+                           const int32_t *counts, const int32_t *d_out, const int32_t *d_in, int32_t num_vertices,
+                           int64_t num_edges, double *out);
+
 /* entropy::mdl (src/entropy.cpp:584-589), FP64 logs. */
 SbpStatus sbp_mdl(const SbpBlockmodel *bm, const SbpGraph *graph, double *out);
 
@@ -189,12 +202,47 @@ SbpStatus sbp_finetune(SbpBlockmodel *bm, const SbpGraph *graph, int32_t algorit
 SbpStatus sbp_merge_blocks(SbpBlockmodel *bm, const SbpGraph *graph, const SbpMergeOptions *opt,
                            const SbpReplay *replay, int32_t *best_merge, double *delta_mdl, SbpStats *stats);
 
+/* A recorded proposal stream: the proposed block and the accept uniform of every draw, as the
+ * reference's own proposal and accept steps made them (common::propose_new_block,
+ * src/common.cpp:131-182, and finetune::accept, src/finetune.cpp:19-29).  A finetune call reads
+ * record t*V + v for the visit of vertex v in its sweep t; a merge call reads record block*10 + i
+ * for proposal i of a block (NUM_AGG_PROPOSALS_PER_BLOCK = 10) and no uniforms.  A visit that
+ * keeps its block has the current block as proposal; its uniform is not read. */
+typedef struct {
+    const int32_t *proposal;   /* records proposed blocks */
+    const double *uniform;     /* records accept uniforms in [0, 1); NULL for a merge call */
+    int64_t records;
+} SbpMoveReplay;
+
+/* finetune::metropolis_hastings / asynchronous_gibbs / hybrid_mcmc (src/finetune.cpp:412-444,
+ * 31-89, 342-410) with the proposals and accept uniforms taken from `replay` instead of drawn:
+ * the Hastings correction, delta-MDL, accept test and move are the engine's.  Fails with
+ * SBP_ERR_REPLAY when a visit has no record or a proposal is out of range. */
+SbpStatus sbp_finetune_replayed(SbpBlockmodel *bm, const SbpGraph *graph, int32_t algorithm,
+                                const SbpFinetuneOptions *opt, const SbpMoveReplay *replay, SbpStats *stats);
+/* block_merge::merge_blocks (src/block_merge.cpp:278-311) with every merge proposal taken from
+ * `replay` (a proposal equal to its own block, or out of range, fails with SBP_ERR_REPLAY). */
+SbpStatus sbp_merge_blocks_replayed(SbpBlockmodel *bm, const SbpGraph *graph, const SbpMergeOptions *opt,
+                                    const SbpMoveReplay *replay, int32_t *best_merge, double *delta_mdl,
+                                    SbpStats *stats);
+
+/* sbp::stochastic_block_partition (src/sbp.cpp:61-98) driven by recorded streams: calls[k] is
+ * the stream of the partition's k-th merge or finetune call (merge, finetune, merge, ... in the
+ * order the loop makes them), read as by sbp_merge_blocks_replayed / sbp_finetune_replayed.
+ * max_sweeps caps every finetune call (<= 0: 100, MAX_NUM_ITERATIONS).  block_counts (num_calls
+ * ints, may be NULL) receives the number of blocks after each call and calls_made (may be NULL)
+ * the number of calls made; SBP_ERR_REPLAY if the partition needs more calls than given. */
+SbpStatus sbp_partition_replayed(const SbpGraph *graph, const SbpOptions *opt, int32_t max_sweeps, int32_t num_calls,
+                                 const SbpMoveReplay *calls, int32_t *out_assignment, int32_t *block_counts,
+                                 int32_t *calls_made, SbpStats *stats);
+
 /* sbp::stochastic_block_partition (src/sbp.cpp:61-98): golden-section search over B with
  * merge + finetune rounds.  out_assignment: V ints. */
 SbpStatus sbp_partition(const SbpGraph *graph, const SbpOptions *opt, int32_t *out_assignment, SbpStats *stats);
 
-/* MDL (entropy::mdl semantics, FP64 log terms) of block counts that are already on the device,
- * for callers that cannot allocate GPU memory: code running under a device-memory budget fixed
+/* MDL of block counts that are already on the device, E h(B^2/E) + V log B - sum_cells M log M
+ * + sum_blocks (d_out log d_out + d_in log d_in) with h(x) = (1+x) log(1+x) - x log x and FP64
+ * log terms, for callers that cannot allocate GPU memory: code running under a device-memory budget fixed
  * at start-up, or code that must not call cudaMalloc/cudaFree because those synchronize the
  * whole device while it has work in flight.  No counterpart in the reference (a CPU-only code
  * base).  It allocates nothing: the caller passes the inputs and the output, and the only

@@ -1,12 +1,18 @@
 """Build the reference (vtsynergy/Hybrid-Stochastic-Block-Partitioning) from its own sources.
 
-TEST INFRASTRUCTURE ONLY.  The reference's sources stay where they lie; nothing is copied.  Its
-build system (CMake with MPI, robin-map, abseil and googletest) is not used: its library
-sources are compiled directly with g++ -O3 -fopenmp against the project-written shims in
-oracle/ref_shims (single-process MPI, robin_map -> std::unordered_map, an empty abseil header,
-missing standard includes), together with oracle/ref_driver.cpp.  Output: oracle/_ref/.
+TEST INFRASTRUCTURE ONLY.  Its build system (CMake with MPI, robin-map, abseil and googletest) is
+not used: its library sources are compiled directly with g++ -O3 -fopenmp against the project-
+written shims in oracle/ref_shims (single-process MPI, robin_map -> std::unordered_map, an empty
+abseil header, missing standard includes), together with oracle/ref_driver.cpp.
 
-The built driver is the CPU baseline of bench.py (--impl reference and the cpu_baseline field).
+Two builds, both under oracle/_ref/ (git-ignored; nothing from the reference is committed):
+  * oracle/_ref/ref_driver: the unmodified sources where they lie.  The CPU baseline of
+    bench.py (--impl reference and the cpu_baseline field) and the unseeded end-to-end runs.
+  * oracle/_ref/replay/ref_driver: a copy of src/ and include/ under oracle/_ref/replay/ with
+    the patches of REPLAY_PATCHES applied (seeded engines and a log of every proposal and accept
+    uniform, FP64 logs, a fixed tie order of merges, a sweep cap) and the hooks of
+    oracle/ref_replay/sbp_replay.cpp.  The seeded-replay parity tests run the GPU engine on the
+    stream this build logs and compare every finetune and merge call's end state with it.
 """
 import json
 import os
@@ -18,7 +24,10 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("SBP_REFERENCE_DIR", "/root/reference")
+# The reference checkout: SBP_REFERENCE_DIR, else a sibling `reference` directory of the repo's
+# parent (where the build container mounts it).  Not needed on a machine that only runs the
+# prebuilt oracle/_ref binaries.
+REF = os.environ.get("SBP_REFERENCE_DIR") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 OUT = os.path.join(HERE, "_ref")
 DRIVER = os.path.join(OUT, "ref_driver")
 SOURCES = [
@@ -40,29 +49,182 @@ def built():
     return os.path.exists(DRIVER)
 
 
+def _compile(root, out_dir, driver, extra_sources=(), extra_flags=(), jobs=8, driver_main=True, link=()):
+    """Compile the reference's library sources under `root` (plus the project's driver, unless
+    driver_main is false, and `extra_sources`) into `driver`."""
+    os.makedirs(os.path.join(out_dir, "obj"), exist_ok=True)
+    shims = os.path.join(HERE, "ref_shims")
+    incs = [os.path.join(root, i) for i in INCLUDES if os.path.isdir(os.path.join(root, i))] + \
+           [os.path.join(REF, i) for i in INCLUDES]
+    flags = ["-std=c++17", "-O3", "-fopenmp", "-w", "-I" + shims, "-I" + HERE] + ["-I" + i for i in incs] + \
+            ["-include", os.path.join(shims, "ref_prelude.h")] + list(extra_flags)
+    procs, objs = [], []
+    srcs = [os.path.join(root if os.path.exists(os.path.join(root, s)) else REF, s) for s in SOURCES]
+    mains = [os.path.join(HERE, "ref_driver.cpp")] if driver_main else []
+    for path in srcs + mains + list(extra_sources):
+        obj = os.path.join(out_dir, "obj", os.path.basename(path).replace(".cpp", ".o"))
+        objs.append(obj)
+        procs.append((path, subprocess.Popen(["g++"] + flags + ["-c", path, "-o", obj])))
+        if len(procs) >= jobs:
+            path0, p0 = procs.pop(0)
+            if p0.wait() != 0:
+                raise RuntimeError("reference compile failed: " + path0)
+    for path0, p0 in procs:
+        if p0.wait() != 0:
+            raise RuntimeError("reference compile failed: " + path0)
+    subprocess.check_call(["g++", "-fopenmp", "-o", driver] + objs + list(link))
+    return driver
+
+
 def build(force=False, jobs=8):
     if built() and not force:
         return DRIVER
     if not reference_available():
         raise RuntimeError("reference sources not found")
-    os.makedirs(os.path.join(OUT, "obj"), exist_ok=True)
-    shims = os.path.join(HERE, "ref_shims")
-    flags = ["-std=c++17", "-O3", "-fopenmp", "-w", "-I" + shims] + ["-I" + os.path.join(REF, i) for i in INCLUDES] + \
-            ["-include", os.path.join(shims, "ref_prelude.h")]
-    procs, objs = [], []
-    for src in SOURCES + [os.path.join(HERE, "ref_driver.cpp")]:
-        path = src if os.path.isabs(src) else os.path.join(REF, src)
-        obj = os.path.join(OUT, "obj", os.path.basename(src).replace(".cpp", ".o"))
-        objs.append(obj)
-        procs.append(subprocess.Popen(["g++"] + flags + ["-c", path, "-o", obj]))
-        if len(procs) >= jobs:
-            if procs.pop(0).wait() != 0:
-                raise RuntimeError("reference compile failed: " + src)
-    for p in procs:
-        if p.wait() != 0:
-            raise RuntimeError("reference compile failed")
-    subprocess.check_call(["g++", "-fopenmp", "-o", DRIVER] + objs)
-    return DRIVER
+    return _compile(REF, OUT, DRIVER, jobs=jobs)
+
+
+# ---- the reference-facing C++ adapter, built into a program of the reference's own classes ----------
+ROOT = os.path.dirname(HERE)
+PKG = os.path.join(ROOT, "hybrid-stochastic-block-partitioning_b200")
+ADAPTER_OUT = os.path.join(OUT, "adapter")
+ADAPTER_CHECK = os.path.join(ADAPTER_OUT, "adapter_check")
+
+
+def adapter_built():
+    return os.path.exists(ADAPTER_CHECK)
+
+
+def build_adapter_check(force=False, jobs=8):
+    """oracle/adapter_check.cpp + include/sbp_b200_reference.hpp against the reference's headers and
+    library sources, linked with libsbp_b200.so (found at run time relative to the program)."""
+    if adapter_built() and not force:
+        return ADAPTER_CHECK
+    if not reference_available():
+        raise RuntimeError("reference sources not found")
+    lib = os.path.join(PKG, "libsbp_b200.so")
+    if not os.path.exists(lib):
+        raise RuntimeError("libsbp_b200.so is not built")
+    rpath = "$ORIGIN/" + os.path.relpath(PKG, ADAPTER_OUT)
+    return _compile(REF, ADAPTER_OUT, ADAPTER_CHECK, extra_sources=[os.path.join(HERE, "adapter_check.cpp")],
+                    extra_flags=["-I" + os.path.join(ROOT, "include"), "-I" + HERE], jobs=jobs, driver_main=False,
+                    link=["-L" + PKG, "-lsbp_b200", "-Wl,-rpath," + rpath])
+
+
+# ---- the replay build -------------------------------------------------------------------------
+REPLAY_OUT = os.path.join(OUT, "replay")
+REPLAY_DRIVER = os.path.join(REPLAY_OUT, "ref_driver")
+HOOKS = os.path.join(HERE, "ref_replay")
+_FT_PROPOSAL = r"(utils::ProposalAndEdgeCounts proposal = common::propose_new_block\([^;]*\);)"
+_MERGE_PROPOSAL = "common::propose_new_block(current_block, out_blocks, in_blocks, block_assignment, blockmodel, true);"
+
+# (file, kind, anchor, replacement, expected count).  kind: "lit" replaces every occurrence of a
+# literal (exactly `count` of them), "first" only the first, "re" a regular expression, "after"
+# the first occurrence of the anchor's second part that follows its first part.
+REPLAY_PATCHES = [
+    # P1: seeded per-translation-unit engines (include/common.hpp:25-26)
+    ("include/common.hpp", "lit", "static std::random_device seeder;\nstatic std::default_random_engine generator(seeder());",
+     "static std::default_random_engine generator(sbp_replay::seed());", 1),
+    # P2: FP64 cell entropy (include/common.hpp:35-44) and nat_log (include/utils.hpp:145-151)
+    ("include/common.hpp", "lit",
+     "inline float cell_entropy(float value, float degree_in, float degree_out) {\n    if (value == 0.0) return 0.0;\n"
+     "    float entropy = value * logf(value / (degree_in * degree_out));",
+     "inline double cell_entropy(double value, double degree_in, double degree_out) {\n    if (value == 0.0) return 0.0;\n"
+     "    double entropy = value * log(value / (degree_in * degree_out));", 1),
+    ("include/utils.hpp", "lit", "result.push_back(logf(value));", "result.push_back(log(value));", 1),
+    # P4: sweep cap of the finetune loops (include/finetune.hpp:56)
+    ("include/finetune.hpp", "lit", "static const int MAX_NUM_ITERATIONS = 100;",
+     "static const int MAX_NUM_ITERATIONS = sbp_replay::max_sweeps();", 1),
+    # P1: accept uniform (src/finetune.cpp:22), visit proposals (:494, :510, :538), call records
+    ("src/finetune.cpp", "lit", "double random_probability = distribution(common::generator);",
+     "double random_probability = distribution(common::generator);\n    sbp_replay::on_uniform(random_probability);", 1),
+    ("src/finetune.cpp", "re", _FT_PROPOSAL, r"\1\n    sbp_replay::on_proposal(vertex, proposal.proposal);", 3),
+    ("src/finetune.cpp", "lit", 'std::cout << "Asynchronous Gibbs iteration" << std::endl;',
+     'std::cout << "Asynchronous Gibbs iteration" << std::endl;\n'
+     "    sbp_replay::CallScope sbp_replay_call(sbp_replay::kAsyncGibbs, blockmodel, blockmodels.get(2).empty ? 0 : 1);", 1),
+    ("src/finetune.cpp", "lit", 'std::cout << "Hybrid MCMC iteration" << std::endl;',
+     'std::cout << "Hybrid MCMC iteration" << std::endl;\n'
+     "    sbp_replay::CallScope sbp_replay_call(sbp_replay::kHybrid, blockmodel, blockmodels.get(2).empty ? 0 : 1);", 1),
+    ("src/finetune.cpp", "lit", 'std::cout << "Metropolis hastings iteration" << std::endl;',
+     'std::cout << "Metropolis hastings iteration" << std::endl;\n'
+     "    sbp_replay::CallScope sbp_replay_call(sbp_replay::kMetropolisHastings, blockmodel, blockmodels.get(2).empty ? 0 : 1);", 1),
+    # P1: merge call, proposal slots and records, per-block scores (src/block_merge.cpp:278-304, 335-345)
+    ("src/block_merge.cpp", "lit", "Blockmodel &merge_blocks(Blockmodel &blockmodel, const Graph &graph, int num_edges) {",
+     "Blockmodel &merge_blocks(Blockmodel &blockmodel, const Graph &graph, int num_edges) {\n"
+     "    sbp_replay::CallScope sbp_replay_call(sbp_replay::kMerge, blockmodel);", 1),
+    ("src/block_merge.cpp", "first", "for (int i = 0; i < NUM_AGG_PROPOSALS_PER_BLOCK; ++i) {",
+     "for (int i = 0; i < NUM_AGG_PROPOSALS_PER_BLOCK; ++i) {\n            sbp_replay::on_merge_slot(current_block, i);", 1),
+    ("src/block_merge.cpp", "first", '    std::cout << "Avoided " << num_avoided',
+     "    sbp_replay::on_merge_scores(best_merge_for_each_block, delta_entropy_for_each_block);\n"
+     '    std::cout << "Avoided " << num_avoided', 1),
+    ("src/block_merge.cpp", "after", ("ProposalEvaluation propose_merge_sparse(int current_block", _MERGE_PROPOSAL),
+     _MERGE_PROPOSAL + "\n    sbp_replay::on_merge_proposal(proposal.proposal);", 1),
+    # P3: merge delta in one orientation (src/block_merge.cpp:342-345) and stable tie order
+    # (src/blockmodel/blockmodel.cpp:52)
+    ("src/block_merge.cpp", "after", ("ProposalEvaluation propose_merge_sparse(int current_block",
+                                      "    Delta delta = blockmodel_delta(current_block, proposal.proposal, blockmodel);\n"
+                                      "    //==========NEW==============\n"
+                                      "    double delta_entropy = entropy::block_merge_delta_mdl(current_block, proposal, "
+                                      "blockmodel, delta);"),
+     "    double delta_entropy = sbp_replay::merge_delta_canonical(current_block, proposal.proposal,\n"
+     "        proposal.num_out_neighbor_edges, proposal.num_in_neighbor_edges, blockmodel);", 1),
+    ("src/blockmodel/blockmodel.cpp", "lit", "std::vector<int> best_merges = utils::sort_indices(delta_entropy_for_each_block);",
+     "std::vector<int> best_merges = sbp_replay::stable_sort_indices(delta_entropy_for_each_block);", 1),
+]
+
+
+def _apply(text, kind, anchor, repl, count, name):
+    import re
+    if kind == "lit":
+        n = text.count(anchor)
+        if n != count:
+            raise RuntimeError(f"replay patch anchor found {n}x (want {count}) in {name}: {anchor[:60]!r}")
+        return text.replace(anchor, repl)
+    if kind == "first":
+        if anchor not in text:
+            raise RuntimeError(f"replay patch anchor missing in {name}: {anchor[:60]!r}")
+        return text.replace(anchor, repl, 1)
+    if kind == "re":
+        new, n = re.subn(anchor, repl, text)
+        if n != count:
+            raise RuntimeError(f"replay patch pattern matched {n}x (want {count}) in {name}: {anchor[:60]!r}")
+        return new
+    if kind == "after":
+        head, target = anchor
+        i = text.find(head)
+        j = text.find(target, i) if i >= 0 else -1
+        if j < 0:
+            raise RuntimeError(f"replay patch anchor missing in {name}: {target[:60]!r}")
+        return text[:j] + repl + text[j + len(target):]
+    raise ValueError(kind)
+
+
+def replay_built():
+    return os.path.exists(REPLAY_DRIVER)
+
+
+def build_replay(force=False, jobs=8):
+    """Copy the reference's src/ and include/ to oracle/_ref/replay/, apply REPLAY_PATCHES and
+    build the replay driver with the hooks of oracle/ref_replay."""
+    import shutil
+    if replay_built() and not force:
+        return REPLAY_DRIVER
+    if not reference_available():
+        raise RuntimeError("reference sources not found")
+    root = os.path.join(REPLAY_OUT, "tree")
+    if os.path.isdir(root):
+        shutil.rmtree(root)
+    for d in ("src", "include"):
+        shutil.copytree(os.path.join(REF, d), os.path.join(root, d))
+    for rel, kind, anchor, repl, count in REPLAY_PATCHES:
+        path = os.path.join(root, rel)
+        with open(path) as f:
+            text = f.read()
+        text = _apply(text, kind, anchor, repl, count, rel)
+        with open(path, "w") as f:
+            f.write(text)
+    return _compile(root, REPLAY_OUT, REPLAY_DRIVER, extra_sources=[os.path.join(HOOKS, "sbp_replay.cpp")],
+                    extra_flags=["-I" + HOOKS, "-include", os.path.join(HOOKS, "sbp_replay.h")], jobs=jobs)
 
 
 def _write_edges(path, V, src, dst):

@@ -4,6 +4,7 @@
 //
 //   ref_driver finetune <edges.bin> <algo> <assignment.bin> <batches> <threads>
 //   ref_driver sbp      <edges.bin> <algo> <batches> <threads> <approximate> <assignment_out.bin>
+//   ref_driver merge    <edges.bin> <assignment.bin> <num_blocks_to_merge> <threads> <approximate>
 //
 // edges.bin: int32 V, int64 n, int32 src[n], int32 dst[n]; assignment.bin: int32 B, int32 b[V].
 // Prints one JSON line.  The reference's own progress output is discarded.
@@ -21,44 +22,17 @@
 #include "args.hpp"
 #include "blockmodel/blockmodel.hpp"
 #include "blockmodel/blockmodel_triplet.hpp"
+#include "block_merge.hpp"
 #include "entropy.hpp"
 #include "finetune.hpp"
 #include "graph.hpp"
 #include "mpi_data.hpp"
 #include "sbp.hpp"
 #include "utils.hpp"
+#include "ref_graph.hpp"
 
 MPI_t mpi;
 Args args;
-
-static bool read_edges(const char* path, int& V, std::vector<int>& src, std::vector<int>& dst) {
-    FILE* f = fopen(path, "rb");
-    if (!f) return false;
-    int64_t n = 0;
-    bool ok = fread(&V, 4, 1, f) == 1 && fread(&n, 8, 1, f) == 1;
-    src.resize(n);
-    dst.resize(n);
-    ok = ok && fread(src.data(), 4, n, f) == (size_t)n && fread(dst.data(), 4, n, f) == (size_t)n;
-    fclose(f);
-    return ok;
-}
-
-// Graph(out_neighbors, in_neighbors, V, E, self_edges) as the reference's tests build it
-// (test/toy_example.hpp), E counted like Graph::load_text (src/graph.cpp:132-135).
-static Graph make_graph(int V, const std::vector<int>& src, const std::vector<int>& dst) {
-    NeighborList out_neighbors, in_neighbors;
-    std::vector<bool> self_edges(V, false);
-    for (size_t i = 0; i < src.size(); ++i) {
-        utils::insert_nodup(out_neighbors, src[i], dst[i]);
-        utils::insert_nodup(in_neighbors, dst[i], src[i]);
-        if (src[i] == dst[i]) self_edges[src[i]] = true;
-    }
-    while ((int)out_neighbors.size() < V) out_neighbors.push_back(std::vector<int>());
-    while ((int)in_neighbors.size() < V) in_neighbors.push_back(std::vector<int>());
-    int E = 0;
-    for (const auto& nb : out_neighbors) E += (int)nb.size();
-    return Graph(out_neighbors, in_neighbors, V, E, self_edges);
-}
 
 static long long visits_per_sweep(const Graph& g, const std::string& algo, int batches) {
     const int V = g.num_vertices();
@@ -117,6 +91,27 @@ int main(int argc, char** argv) {
                "\"E\": %d, \"B\": %d}\n",
                secs, finetune::MCMC_iterations, visits, (double)bm.getOverall_entropy(), args.threads, V,
                graph.num_edges(), B);
+        return 0;
+    }
+    if (mode == "merge" && argc >= 7) {
+        args.threads = atoi(argv[5]);
+        args.approximate = atoi(argv[6]) != 0;
+        omp_set_num_threads(args.threads);
+        FILE* f = fopen(argv[3], "rb");
+        int B = 0;
+        std::vector<int> a(V);
+        bool ok = f && fread(&B, 4, 1, f) == 1 && fread(a.data(), 4, V, f) == (size_t)V;
+        if (f) fclose(f);
+        if (!ok) return 2;
+        Graph graph = make_graph(V, src, dst);
+        Blockmodel bm(B, graph, 0.5, a);
+        bm.setNum_blocks_to_merge(atoi(argv[4]));
+        auto t0 = std::chrono::steady_clock::now();
+        bm = block_merge::merge_blocks(bm, graph, graph.num_edges());
+        auto t1 = std::chrono::steady_clock::now();
+        std::cout.rdbuf(saved);
+        printf("{\"seconds\": %.6f, \"num_blocks\": %d, \"threads\": %d, \"V\": %d, \"E\": %d}\n",
+               std::chrono::duration<double>(t1 - t0).count(), bm.getNum_blocks(), args.threads, V, graph.num_edges());
         return 0;
     }
     if (mode == "sbp" && argc >= 8) {

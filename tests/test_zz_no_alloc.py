@@ -5,8 +5,9 @@ call cudaMalloc/cudaFree because those synchronize the device while work is in f
 their own device buffers; the entry point's only scratch is a static device array.  This test
 owns every buffer (allocated here with torch, as such a caller would), calls the entry point
 through the C ABI twice in a row and checks each result against sbp_mdl, the allocating entry
-point, within the MDL tolerance of the other GPU tests.  It is collected last so that a run that
-stops at the first failure has already run everything else, and it also passes alone.
+point, and against the CPU oracle's MDL, within the MDL tolerance of the other GPU tests.  It is
+collected last so that a run that stops at the first failure has already run everything else,
+and it also passes alone.
 """
 import numpy as np
 import pytest
@@ -31,14 +32,17 @@ def call(S, torch, M, do, di, V, E, out):
     return float(out.item())
 
 
-def test_noalloc_mdl_matches_allocating_mdl_twice(S):
+def test_noalloc_mdl_matches_allocating_mdl_twice(S, O):
     import torch
     V, s, d, _ = random_graph(2000, 8, 91)
-    g = S.Graph(V, s, d)
+    g, og = S.Graph(V, s, d), O.Graph(V, s, d)
     cases = []
     for B, seed in ((300, 1), (40, 2)):
-        bm = S.Blockmodel(g, B, random_assignment(V, B, seed))
-        cases.append((bm, S.entropy.mdl(bm)))
+        a = random_assignment(V, B, seed)
+        bm = S.Blockmodel(g, B, a)
+        ref = S.entropy.mdl(bm)
+        assert ref == pytest.approx(O.Blockmodel(og, B, a).mdl(), rel=RTOL_MDL)
+        cases.append((bm, ref))
     out = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
     # two calls in a row on the same inputs, then a different B, then the first again: the
     # shared scratch array keeps the previous call's contents, which must not leak
@@ -62,3 +66,5 @@ def test_noalloc_mdl_rejects_sizes_beyond_its_limit(S):
     with pytest.raises(S.SbpError) as e:
         S.mdl_device_noalloc(M.data_ptr(), 32769, 32769, deg.data_ptr(), deg.data_ptr(), 10, 10, out.data_ptr(), None)
     assert e.value.code == 3
+    assert "32768-block limit" in S.last_error()
+    assert "32768-block limit" in str(e.value)
