@@ -3,18 +3,24 @@
 
 Metric: vertex moves/s (vertex visits = MCMC proposals evaluated, per second) of a complete
 sbp::stochastic_block_partition run (block merges + asynchronous-Gibbs finetune, golden-section
-search over B) on the 20,000-vertex, 32-block directed DC-SBM (Dirichlet alpha = 1 block sizes,
-power-law degrees gamma 2.5 on [10,100], within-block fraction 0.6, seed 2).  One step = one
-full partition from B = V to the final B.
+search over B) on the 200,000-vertex, 71-block directed DC-SBM (Dirichlet alpha = 1 block sizes,
+power-law degrees gamma 2.5 on [10,100], within-block fraction 0.7, seed 4).  One step = one full
+partition from B = V to the final B; visits are counted over the whole partition, and its whole
+device time (merges included) is the denominator.  `--config 2` runs the 20,000-vertex graph.
 
   value : graph already resident on the device; CUDA events on the library's stream.
   e2e   : the public C-ABI path from host buffers: sbp_graph_create from pinned host edge
           arrays (host->device inside the timed region) + sbp_partition + the assignment read back.
   roofline : the vertex-evaluation kernel (k_gibbs_eval), algorithmic bytes per launch
-          = sum over its vertices of 12 + 8 (k_out + k_in), over its CUDA-event duration.
+          = sum over its vertices of 12 + 8 (k_out + k_in), over its CUDA-event duration;
+          traffic = the DRAM bytes ncu measured for one launch of it (profiles/).
 
---impl reference times the reference's CPU implementation on the host cores (the reference
-built from its own sources under oracle/_ref when present, else the CPU oracle port).
+--impl reference times the reference's own CPU implementation on every host core: the reference
+built from its sources (oracle/_ref; the timing build's only change is a cap on the sweeps of a
+finetune call), one 1-sweep asynchronous-Gibbs call per step at the block counts the partition
+passes through (V/2, V/4, ... down to the planted B, cycled over the steps).  The reference's
+full-partition wall time on the same graph, measured once, is carried beside it (oracle/
+reference_anchors.json).
 Multi-GPU: the path does not shard; every rank runs its own replica partitions ("replicas
 only"), value = all ranks' visits / max-over-ranks time.
 """
@@ -33,7 +39,12 @@ sys.path.insert(0, PKG)
 
 METRIC = "vertex moves/s"
 UNIT = "vertex visits/s"
-WORKLOAD = "plain SBP, async Gibbs (batches 10) + approximate block merge, directed DC-SBM 20000 V / 32 blocks"
+WORKLOADS = {
+    2: "plain SBP, async Gibbs (batches 10) + approximate block merge, directed DC-SBM 20000 V / 32 blocks "
+       "(alpha 1, gamma 2.5 on [10,100], w 0.6, seed 2)",
+    4: "plain SBP, async Gibbs (batches 10) + approximate block merge, directed DC-SBM 200000 V / 71 blocks "
+       "(alpha 1, gamma 2.5 on [10,100], w 0.7, seed 4)",
+}
 
 
 def args_parse():
@@ -42,7 +53,7 @@ def args_parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--config", type=int, default=4, choices=sorted(WORKLOADS))
     ap.add_argument("--algorithm", default="async_gibbs")
     ap.add_argument("--batches", type=int, default=10)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain comparison")
@@ -133,16 +144,27 @@ def cpu_baseline_port(V, src, dst, truth, budget_s=12.0):
                       f"{visits} visits in {dt:.1f} s"}
 
 
+def reference_module():
+    sys.path.insert(0, ORACLE)
+    import build_reference as rb
+    return rb
+
+
 def reference_baseline(V, src, dst, truth, budget_s):
-    ref = os.path.join(ORACLE, "build_reference.py")
-    if os.path.exists(ref):
-        import importlib.util
-        spec = importlib.util.spec_from_file_location("sbp_reference_build", ref)
-        rb = importlib.util.module_from_spec(spec)
-        spec.loader.exec_module(rb)
-        if rb.built():
-            return rb.time_reference(V, src, dst, truth, budget_s)
+    rb = reference_module()
+    if rb.capped_built():
+        return rb.time_reference(V, src, dst, truth, budget_s)
     return cpu_baseline_port(V, src, dst, truth, budget_s)
+
+
+def reference_anchor(config):
+    """The reference's full stochastic_block_partition on the same graph, measured once
+    (oracle/record_reference_anchor.py writes oracle/reference_anchors.json)."""
+    try:
+        with open(os.path.join(ORACLE, "reference_anchors.json")) as f:
+            return json.load(f).get(str(config))
+    except (OSError, ValueError):
+        return None
 
 
 def reduce_over_ranks(ms, count, device):
@@ -249,7 +271,7 @@ def main():
     import dcsbm
 
     V, src, dst, truth = dcsbm.config_graph(a.config)
-    config = {"workload": WORKLOAD if a.config == 2 else f"config {a.config}", "V": V, "edges_raw": int(len(src)),
+    config = {"workload": WORKLOADS[a.config], "V": V, "edges_raw": int(len(src)),
               "blocks_planted": int(truth.max()) + 1, "algorithm": a.algorithm, "batches": a.batches,
               "merge": "approximate", "step": "one full stochastic_block_partition (B = V -> final B)",
               "l2": "256 MB buffer written before every timed step (L2 flush)", "parallelism": f"replicas x{world}",
@@ -258,28 +280,40 @@ def main():
     if a.impl == "reference":
         if rank != 0:
             return
-        sys.path.insert(0, ORACLE)
-        import build_reference as R
-        if not R.built():
+        rb = reference_module()
+        K = int(truth.max()) + 1
+        ref_config = dict(config, step="one reference finetune::asynchronous_gibbs call capped at 1 sweep (batches "
+                          f"{a.batches}, --transpose) at B = the step's level of the partition's halving schedule "
+                          "(V/2, V/4, ... the planted B), from the planted partition split into B/K sub-blocks",
+                          sweep_driver="reference host loop (OpenMP, every host core)",
+                          l2="not applicable (host CPU; each step reloads the graph in a fresh process)")
+        if not rb.capped_built():
             base = cpu_baseline_port(V, src, dst, truth, 20.0)
-            v = base["value"]
+            v, ms_step, levels = base["value"], None, []
         else:
-            for _ in range(a.warmup):   # short untimed runs: one call at the planted B
-                R.run_finetune(V, src, dst, truth.astype(np.int32), algo="async_gibbs", batches=a.batches)
-            visits, secs, base = 0, 0.0, None
-            for _ in range(a.steps):
-                base = R.time_reference(V, src, dst, truth, batches=a.batches)
-                r = base["value"]
-                n = int(base["sample"].split(" visits in ")[0].split()[-1])
-                visits += n
-                secs += n / r
+            for _ in range(a.warmup):   # untimed: one capped sweep at the planted B
+                rb.time_reference_level(V, src, dst, truth, K, a.batches)
+            levels = rb.halving_levels(V, K)
+            visits, secs, used = 0, 0.0, []
+            for k in range(a.steps):
+                r = rb.time_reference_level(V, src, dst, truth, levels[k % len(levels)], a.batches)
+                visits += r["visits"]
+                secs += r["seconds"]
+                used.append(r["B"])
             v = visits / secs if secs > 0 else 0.0
-            base["value"] = v
-        print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
-                          "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
-                          "vs_baseline": None, "dtype": "int32 counts, fp32 logs (reference)",
-                          "data": "synthetic (seeded DC-SBM generator)", "config": config, "cpu_baseline": base,
-                          "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+            ms_step = 1e3 * secs / max(1, a.steps)
+            base = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                    "sample": f"{a.steps} capped 1-sweep reference asynchronous_gibbs calls at B = {used}: {visits} "
+                              f"visits in {secs:.2f} s"}
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "int32 counts, fp32 logs (reference)",
+                "data": "synthetic (seeded DC-SBM generator)", "config": ref_config, "cpu_baseline": base,
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        anchor = reference_anchor(a.config)
+        if anchor:
+            line["reference_full_partition"] = anchor
+        print(json.dumps(line))
         return
 
     import torch

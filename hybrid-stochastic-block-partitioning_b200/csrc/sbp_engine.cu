@@ -504,6 +504,8 @@ void finetune(SbpBlockmodel& bm, SbpGraph& g, int algo, const SbpFinetuneOptions
   st.mcmc_seconds = ms * 1e-3;
   st.num_blocks = bm.B;
   st.overflow_rebuilds = (int)(g_overflow_rebuilds - ovf0);
+  g_mcmc_iterations += st.sweeps;
+  g_mcmc_time += st.mcmc_seconds;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -785,6 +787,75 @@ void restore(SbpBlockmodel& bm, SbpGraph& g, const Snapshot& x) {
   c.sync();
 }
 
+// entropy::null_mdl_v1 / null_mdl_v2 (src/entropy.cpp:567-583).
+static double null_mdl_v1(long long E) {
+  const double lp = (double)E * std::log(1.0 / (double)E);
+  const double x = 1.0 / (double)E;
+  const double h = ((1 + x) * std::log(1 + x)) - (x * std::log(x));
+  return ((double)E * h) - lp;
+}
+static double null_mdl_v2(long long V, long long E) {
+  const double lp = (double)E * std::log(1.0 / (double)E);
+  const double x = std::pow((double)V, 2) / (double)E;
+  const double h = ((1 + x) * std::log(1 + x)) - (x * std::log(x));
+  return ((double)E * h) + ((double)V * std::log((double)V)) - lp;
+}
+
+// sbp::add_intermediate (src/sbp.cpp:36-59) with Blockmodel::interblock_edges
+// (src/blockmodel/blockmodel.cpp:257-261), Blockmodel::block_size_variation (blockmodel.cpp:9-27)
+// and, for the final record, Graph::modularity (src/graph.cpp:142-163) in its block form
+// (sum_b M[b,b] - sum_b d_out[b] d_in[b] / E) / E.
+void add_intermediate(PartitionState& ps, const SbpGraph& g, float iteration, double mdl, bool modularity) {
+  Context& c = Context::get();
+  SbpBlockmodel& bm = ps.bm;
+  DevBuf<unsigned long long> stats;
+  DevBuf<int> sizes;
+  stats.reserve(3);
+  sizes.reserve(bm.B);
+  SBP_CUDA(cudaMemsetAsync(stats.p, 0, 3 * sizeof(unsigned long long), c.stream));
+  SBP_CUDA(cudaMemsetAsync(sizes.p, 0, bm.B * sizeof(int), c.stream));
+  k_block_stats<<<grid_for(bm.B, 256, 4 * c.num_sms), 256, 0, c.stream>>>(bm.view(), stats.p);
+  k_block_sizes<<<grid_for(g.V, 256, 8 * c.num_sms), 256, 0, c.stream>>>(bm.b.p, g.V, sizes.p);
+  SBP_CHECK_LAUNCH();
+  unsigned long long st[3];
+  std::vector<int> sz(bm.B);
+  SBP_CUDA(SBP_COPY_ASYNC(st, stats.p, sizeof st, cudaMemcpyDeviceToHost, c.stream));
+  SBP_CUDA(SBP_COPY_ASYNC(sz.data(), sizes.p, bm.B * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  cudaEvent_t now;
+  SBP_CUDA(cudaEventCreate(&now));
+  SBP_CUDA(cudaEventRecord(now, c.stream));
+  c.sync();
+  float ms = 0.f;
+  if (ps.t_start) SBP_CUDA(cudaEventElapsedTime(&ms, ps.t_start, now));
+  cudaEventDestroy(now);
+  SbpIntermediate r;
+  std::memset(&r, 0, sizeof r);
+  r.iteration = iteration;
+  r.num_blocks = bm.B;
+  r.mdl = mdl;
+  r.normalized_mdl_v1 = mdl / null_mdl_v1(g.E);
+  r.normalized_mdl_v2 = mdl / null_mdl_v2(g.V, g.E);
+  const double E = (double)g.E;
+  r.modularity = modularity ? ((double)st[0] - (double)st[2] / E) / E : -1.0;
+  r.interblock_edges = ((double)st[1] - (double)st[0]) / (double)st[1];
+  double total = 0.0, mn = std::numeric_limits<double>::max(), mx = std::numeric_limits<double>::min();
+  for (int x : sz) total += x;
+  const double mean = total / double(bm.B);
+  double var = 0.0;
+  for (int x : sz) {
+    mn = std::min(mn, (double)x);
+    mx = std::max(mx, (double)x);
+    var += double(x - mean) * double(x - mean);
+  }
+  var /= double(bm.B);
+  r.block_size_variation = float(var / ((double(mx - mn) * double(mx - mean)) / 4.0));
+  r.mcmc_iterations = (int32_t)g_mcmc_iterations;
+  r.mcmc_time = g_mcmc_time;
+  r.visits = ps.st.visits;
+  r.seconds = ms * 1e-3;
+  g_intermediates.push_back(r);
+}
+
 // sbp::stochastic_block_partition (src/sbp.cpp:61-98) as a per-graph state machine: the
 // single-graph driver below and the batched driver (sbp_batched.cu) run the same steps.
 void partition_begin(PartitionState& ps, SbpGraph& g) {
@@ -799,6 +870,7 @@ void partition_begin(PartitionState& ps, SbpGraph& g) {
   bm.num_blocks_to_merge = (int)(g.V * 0.5f);
   rebuild(bm, g);
   c.sync();
+  if (ps.record) add_intermediate(ps, g, 0.f, mdl(bm, g), false);
 }
 
 int partition_merge(PartitionState& ps, SbpGraph& g, const SbpOptions& opt, SbpFinetuneOptions* fo) {
@@ -808,6 +880,7 @@ int partition_merge(PartitionState& ps, SbpGraph& g, const SbpOptions& opt, SbpF
   mo.seed = opt.seed;
   merge_blocks(ps.bm, g, mo, nullptr, nullptr, nullptr, ps.st, ps.take_replay());
   if (ps.replays) ps.block_counts.push_back(ps.bm.B);
+  if (ps.record && ps.iteration < 1) add_intermediate(ps, g, 0.5f, mdl(ps.bm, g), false);
   int algo = opt.algorithm;
   if (algo == SBP_ASYNC_GIBBS && !(ps.iteration < (float)opt.asynciterations)) algo = SBP_METROPOLIS_HASTINGS;
   fo->batches = opt.batches;
@@ -827,6 +900,7 @@ void partition_finish_round(PartitionState& ps, SbpGraph& g, const SbpStats& fs,
   st.mcmc_seconds += fs.mcmc_seconds;
   st.learned_sweeps += fs.learned_sweeps;
   ++ps.iteration;
+  if (ps.record) add_intermediate(ps, g, ps.iteration, ps.bm.overall_entropy, false);
   ++ps.call;
   st.outer_iterations++;
   int to_merge = 0;
@@ -836,6 +910,10 @@ void partition_finish_round(PartitionState& ps, SbpGraph& g, const SbpStats& fs,
     st.mdl = nxt.entropy;
     st.num_blocks = nxt.B;
     ps.done = true;
+    if (ps.record) {   // the final record is taken on the blockmodel the partition returns
+      restore(ps.bm, g, nxt);
+      add_intermediate(ps, g, -1.f, nxt.entropy, true);
+    }
     return;
   }
   restore(ps.bm, g, nxt);
@@ -850,6 +928,8 @@ void partition(SbpGraph& g, const SbpOptions& opt, int* out, SbpStats& st, const
   SBP_CUDA(cudaEventCreate(&t1));
   SBP_CUDA(cudaEventRecord(t0, c.stream));
   PartitionState ps;
+  ps.record = step == nullptr && replay == nullptr;
+  ps.t_start = t0;
   if (replay) {
     ps.replays = replay->calls;
     ps.nreplays = replay->num_calls;
@@ -1437,6 +1517,20 @@ SbpStatus sbp_merge_blocks_replayed(SbpBlockmodel* bm, const SbpGraph* g, const 
   std::memset(&st, 0, sizeof st);
   merge_blocks(*bm, const_cast<SbpGraph&>(*g), *opt, nullptr, best_merge, delta_mdl, st, replay);
   if (stats) *stats = st;
+  SBP_API_END
+}
+
+SbpStatus sbp_get_intermediates(SbpIntermediate* out, int32_t capacity, int32_t* count) {
+  SBP_API_BEGIN
+  SBP_REQUIRE(count && (capacity == 0 || out) && capacity >= 0, "bad argument");
+  *count = (int32_t)g_intermediates.size();
+  for (int32_t i = 0; i < capacity && i < *count; ++i) out[i] = g_intermediates[i];
+  SBP_API_END
+}
+
+SbpStatus sbp_clear_intermediates(void) {
+  SBP_API_BEGIN
+  g_intermediates.clear();
   SBP_API_END
 }
 

@@ -583,6 +583,9 @@ struct PartitionState {
   int nreplays = 0, next_replay = 0;
   int max_sweeps = 0;
   std::vector<int> block_counts;
+  // sbp::add_intermediate records (src/sbp.cpp:36-59) of a single-graph partition
+  bool record = false;
+  cudaEvent_t t_start = nullptr;
   const SbpMoveReplay* take_replay() {
     if (!replays) return nullptr;
     if (next_replay >= nreplays)
@@ -590,6 +593,15 @@ struct PartitionState {
     return &replays[next_replay++];
   }
 };
+
+// Process-wide finetune counters (finetune::MCMC_iterations / MCMC_time, src/finetune.cpp:15-16)
+// and intermediate records of partitions (sbp::intermediate_results, src/sbp.cpp:16-20).
+inline long long g_mcmc_iterations = 0;
+inline double g_mcmc_time = 0.0;
+inline std::vector<SbpIntermediate> g_intermediates;
+// Record one intermediate of a partition in progress (modularity only when asked: the reference
+// computes it for the final record alone).
+void add_intermediate(PartitionState& ps, const SbpGraph& g, float iteration, double mdl, bool modularity);
 
 // Engine steps shared by the translation units (defined in sbp_engine.cu).
 void rebuild(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_d = true);

@@ -666,6 +666,18 @@ __global__ void k_block_sizes(const int* b, int V, int* size) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) atomicAdd(size + b[v], 1);
 }
 
+__global__ void k_block_stats(BlockView bm, unsigned long long* out) {
+  unsigned long long tr = 0, din = 0, prod = 0;
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < bm.B; x += gridDim.x * blockDim.x) {
+    tr += (unsigned long long)bm_get(bm, x, x);
+    din += (unsigned long long)bm.d_in[x];
+    prod += (unsigned long long)bm.d_out[x] * (unsigned long long)bm.d_in[x];
+  }
+  atomicAdd(out + 0, tr);
+  atomicAdd(out + 1, din);
+  atomicAdd(out + 2, prod);
+}
+
 __global__ void k_relabel(int* b, int V, const int* map) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) b[v] = map[b[v]];
 }

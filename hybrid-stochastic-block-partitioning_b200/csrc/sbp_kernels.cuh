@@ -67,6 +67,9 @@ __global__ void k_row_fill(const int* A, int B, int ld, const int* ptr, int* idx
 __global__ void k_merge_propose(BlockView bm, Csr rows, Csr cols, RngParams rng, int* best_s, double* best_dS,
                                 unsigned long long* counters, int* status);
 __global__ void k_block_sizes(const int* b, int V, int* size);
+// Integer block statistics: out[0] = sum_b M[b,b], out[1] = sum_b d_in[b], out[2] = sum_b
+// d_out[b] * d_in[b] (the interblock-edge fraction and the modularity of a partition).
+__global__ void k_block_stats(BlockView bm, unsigned long long* out);
 __global__ void k_relabel(int* b, int V, const int* map);
 
 // row-hashed block matrix (sbp_sparse.cu)

@@ -35,7 +35,8 @@ EXPORTED = [
     "sbp_dataset_append", "sbp_dataset_read", "sbp_vertex_features", "sbp_learned_evaluate", "sbp_learned_q",
     "sbp_collect_moves", "sbp_finetune_learned", "sbp_partition_learned", "sbp_partition_batched",
     "sbp_batched_reset_tuning", "sbp_mdl_device_noalloc", "sbp_finetune_replayed", "sbp_merge_blocks_replayed",
-    "sbp_partition_replayed", "sbp_set_degrees", "sbp_mdl_of_cells",
+    "sbp_partition_replayed", "sbp_set_degrees", "sbp_mdl_of_cells", "sbp_contingency_metrics",
+    "sbp_evaluate_blockmodel", "sbp_get_intermediates", "sbp_clear_intermediates",
 ]
 
 MLP_FEATURES, MLP_OUTPUTS, MLP_SLOTS, MLP_ESCAPE, MLP_PARAMS = 64, 16, 14, 14, 26896
@@ -54,6 +55,27 @@ class Replay(ctypes.Structure):
 class MoveReplay(ctypes.Structure):
     _fields_ = [("proposal", ctypes.POINTER(ctypes.c_int32)), ("uniform", ctypes.POINTER(ctypes.c_double)),
                 ("records", ctypes.c_int64)]
+
+
+class Evaluation(ctypes.Structure):
+    _fields_ = [("f1_score", ctypes.c_double), ("nmi", ctypes.c_double), ("accuracy", ctypes.c_double),
+                ("rand_index", ctypes.c_double), ("precision", ctypes.c_double), ("recall", ctypes.c_double),
+                ("true_mdl", ctypes.c_double), ("counted_vertices", ctypes.c_int64), ("num_blocks", ctypes.c_int32),
+                ("true_num_blocks", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Intermediate(ctypes.Structure):
+    _fields_ = [("iteration", ctypes.c_float), ("num_blocks", ctypes.c_int32), ("mdl", ctypes.c_double),
+                ("normalized_mdl_v1", ctypes.c_double), ("normalized_mdl_v2", ctypes.c_double),
+                ("modularity", ctypes.c_double), ("interblock_edges", ctypes.c_double),
+                ("block_size_variation", ctypes.c_double), ("mcmc_iterations", ctypes.c_int32), ("_pad", ctypes.c_int32),
+                ("mcmc_time", ctypes.c_double), ("visits", ctypes.c_int64), ("seconds", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("_")}
 
 
 class Stats(ctypes.Structure):
@@ -166,6 +188,12 @@ def load(path=LIB_PATH):
     L.sbp_merge_blocks_replayed.argtypes = [vp, vp, ctypes.POINTER(MergeOptions), ctypes.POINTER(MoveReplay), _i32p,
                                             _f64p, ctypes.POINTER(Stats)]
     L.sbp_set_degrees.argtypes = [vp, _i32p]
+    L.sbp_get_intermediates.argtypes = [ctypes.POINTER(Intermediate), ctypes.c_int32, _i32p]
+    L.sbp_clear_intermediates.argtypes = []
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    L.sbp_contingency_metrics.argtypes = [ctypes.c_int32, ctypes.c_int32, i64p, ctypes.c_int64,
+                                          ctypes.POINTER(Evaluation)]
+    L.sbp_evaluate_blockmodel.argtypes = [vp, vp, _i32p, ctypes.POINTER(Evaluation), i64p]
     L.sbp_mdl_of_cells.argtypes = [ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _i32p, _i32p, _i32p, ctypes.c_int32,
                                    ctypes.c_int64, _f64p]
     L.sbp_partition_replayed.argtypes = [vp, ctypes.POINTER(Options), ctypes.c_int32, ctypes.c_int32,
@@ -459,6 +487,48 @@ def mdl_device_noalloc(d_matrix, num_blocks, ld, d_degrees_out, d_degrees_in, nu
         raise SbpError(rc, last_error())
 
 
+class evaluate:
+    """evaluate::evaluate_blockmodel / calculate_f1_score / calculate_nmi (src/evaluate.cpp:7-178)."""
+
+    @staticmethod
+    def contingency_metrics(table, num_vertices):
+        t = np.ascontiguousarray(table, np.int64)
+        ev = Evaluation()
+        _check(load().sbp_contingency_metrics(t.shape[0], t.shape[1], t.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                              int(num_vertices), ctypes.byref(ev)))
+        return ev.as_dict()
+
+    @staticmethod
+    def evaluate_blockmodel(blockmodel, true_assignment, with_table=False):
+        truth = np.ascontiguousarray(true_assignment, np.int32)
+        ev = Evaluation()
+        known = truth[truth >= 0]
+        K = len(np.unique(known))
+        table = np.zeros((blockmodel.B, max(K, 1)), np.int64)
+        _check(_lib.sbp_evaluate_blockmodel(blockmodel.h, blockmodel.graph.h, _p(truth), ctypes.byref(ev),
+                                            table.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        out = ev.as_dict()
+        if with_table:
+            out["table"] = table
+        return out
+
+
+def set_degrees(blockmodel, d):
+    """sbp_set_degrees: overwrite the block degrees d of a blockmodel."""
+    dd = np.ascontiguousarray(d, np.int32)
+    _check(_lib.sbp_set_degrees(blockmodel.h, _p(dd)))
+
+
+def mdl_of_cells(num_blocks, rows, cols, counts, d_out, d_in, num_vertices, num_edges):
+    """sbp_mdl_of_cells: entropy::mdl of host cell lists and degrees."""
+    r, c, v = (np.ascontiguousarray(x, np.int32) for x in (rows, cols, counts))
+    do, di = np.ascontiguousarray(d_out, np.int32), np.ascontiguousarray(d_in, np.int32)
+    out = ctypes.c_double()
+    _check(load().sbp_mdl_of_cells(int(num_blocks), len(v), _p(r), _p(c), _p(v), _p(do), _p(di), int(num_vertices),
+                                   int(num_edges), ctypes.byref(out)))
+    return out.value
+
+
 class sbp:
     @staticmethod
     def stochastic_block_partition(graph, algorithm="async_gibbs", batches=10, approximate=True,
@@ -469,6 +539,19 @@ class sbp:
         st = Stats()
         _check(_lib.sbp_partition(graph.h, ctypes.byref(opt), _p(out), ctypes.byref(st)))
         return out, st.as_dict()
+
+    @staticmethod
+    def get_intermediates():
+        """sbp::get_intermediates: the records of every partition of this process (list of dicts)."""
+        n = ctypes.c_int32()
+        _check(load().sbp_get_intermediates(None, 0, ctypes.byref(n)))
+        arr = (Intermediate * max(1, n.value))()
+        _check(_lib.sbp_get_intermediates(arr, n.value, ctypes.byref(n)))
+        return [arr[i].as_dict() for i in range(n.value)]
+
+    @staticmethod
+    def clear_intermediates():
+        _check(load().sbp_clear_intermediates())
 
     @staticmethod
     def stochastic_block_partition_replayed(graph, calls, algorithm="async_gibbs", batches=10, approximate=True,

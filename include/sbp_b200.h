@@ -226,6 +226,61 @@ SbpStatus sbp_merge_blocks_replayed(SbpBlockmodel *bm, const SbpGraph *graph, co
                                     const SbpMoveReplay *replay, int32_t *best_merge, double *delta_mdl,
                                     SbpStats *stats);
 
+/* One intermediate record of a partition (sbp::Intermediate, include/sbp.hpp:18-28, recorded by
+ * sbp::add_intermediate, src/sbp.cpp:36-59): at the start (iteration 0, B = V), after the first
+ * merge (0.5), after the k-th finetune (k) and for the result (-1). */
+typedef struct {
+    float iteration;
+    int32_t num_blocks;
+    double mdl;                  /* entropy::mdl; after a finetune the float overall entropy */
+    double normalized_mdl_v1;    /* entropy::normalize_mdl_v1 / v2 (src/entropy.cpp:559-583) */
+    double normalized_mdl_v2;
+    double modularity;           /* Graph::modularity of the result (src/graph.cpp:142-163); -1 before */
+    double interblock_edges;     /* Blockmodel::interblock_edges (src/blockmodel/blockmodel.cpp:257-261) */
+    double block_size_variation; /* Blockmodel::block_size_variation (src/blockmodel/blockmodel.cpp:9-27) */
+    int32_t mcmc_iterations;     /* finetune sweeps so far in this process (finetune::MCMC_iterations) */
+    int32_t _pad;
+    double mcmc_time;            /* device seconds of finetune so far in this process (finetune::MCMC_time) */
+    int64_t visits;              /* vertex visits of this partition so far (no reference counterpart) */
+    double seconds;              /* device seconds since this partition started (no reference counterpart) */
+} SbpIntermediate;
+
+/* sbp::get_intermediates (src/sbp.cpp:18-20): the records of every sbp_partition call of this
+ * process so far (count receives their number; at most capacity are copied).  The batched,
+ * learned and replayed partitions record none. */
+SbpStatus sbp_get_intermediates(SbpIntermediate *out, int32_t capacity, int32_t *count);
+SbpStatus sbp_clear_intermediates(void);
+
+/* Quality of a partition against a known one (evaluate::Eval and the printed figures of
+ * evaluate::calculate_f1_score / calculate_nmi, src/evaluate.cpp:7-96). */
+typedef struct {
+    double f1_score;          /* pair-counting F1 */
+    double nmi;               /* normalised mutual information */
+    double accuracy;          /* matched vertices of the best block <-> community matching, over V */
+    double rand_index;
+    double precision;         /* pairs together in both / pairs together in the true partition */
+    double recall;            /* pairs together in both / pairs together in the algorithm's */
+    double true_mdl;          /* entropy::mdl of the true partition (NaN when some labels are unknown) */
+    int64_t counted_vertices; /* vertices with a known true community */
+    int32_t num_blocks;       /* rows of the table: algorithm blocks */
+    int32_t true_num_blocks;  /* columns: true communities */
+} SbpEvaluation;
+
+/* calculate_f1_score and calculate_nmi (src/evaluate.cpp:7-96) of a contingency table given on the
+ * host (nrows x ncols, row-major; rows = algorithm blocks, columns = true communities) over
+ * num_vertices vertices, plus the accuracy of the best one-to-one matching (the reference's
+ * Hungarian step, src/evaluate.cpp:114-178).  Host arithmetic only; needs no device.  Pair
+ * counts are 64-bit (the reference's int products wrap above 46340 in the Rand index). */
+SbpStatus sbp_contingency_metrics(int32_t nrows, int32_t ncols, const int64_t *table, int64_t num_vertices,
+                                  SbpEvaluation *out);
+/* evaluate::evaluate_blockmodel (src/evaluate.cpp:98-112): the contingency table of the
+ * blockmodel's assignment against true_assignment (V ints; community ids numbered in order of
+ * first appearance as evaluate::hungarian does; -1 = unknown, not counted) is counted on the
+ * device, then the metrics above and the true partition's MDL.  table_out (optional,
+ * B x K int64, columns in first-appearance order) receives the table. */
+SbpStatus sbp_evaluate_blockmodel(const SbpBlockmodel *bm, const SbpGraph *graph, const int32_t *true_assignment,
+                                  SbpEvaluation *out, int64_t *table_out);
+
 /* sbp::stochastic_block_partition (src/sbp.cpp:61-98) driven by recorded streams: calls[k] is
  * the stream of the partition's k-th merge or finetune call (merge, finetune, merge, ... in the
  * order the loop makes them), read as by sbp_merge_blocks_replayed / sbp_finetune_replayed.

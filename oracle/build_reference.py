@@ -203,28 +203,60 @@ def replay_built():
     return os.path.exists(REPLAY_DRIVER)
 
 
-def build_replay(force=False, jobs=8):
-    """Copy the reference's src/ and include/ to oracle/_ref/replay/, apply REPLAY_PATCHES and
-    build the replay driver with the hooks of oracle/ref_replay."""
+def _patched_tree(out_dir, patches):
+    """A copy of the reference's src/ and include/ under out_dir/tree with `patches` applied."""
     import shutil
-    if replay_built() and not force:
-        return REPLAY_DRIVER
-    if not reference_available():
-        raise RuntimeError("reference sources not found")
-    root = os.path.join(REPLAY_OUT, "tree")
+    root = os.path.join(out_dir, "tree")
     if os.path.isdir(root):
         shutil.rmtree(root)
     for d in ("src", "include"):
         shutil.copytree(os.path.join(REF, d), os.path.join(root, d))
-    for rel, kind, anchor, repl, count in REPLAY_PATCHES:
+    for rel, kind, anchor, repl, count in patches:
         path = os.path.join(root, rel)
         with open(path) as f:
             text = f.read()
         text = _apply(text, kind, anchor, repl, count, rel)
         with open(path, "w") as f:
             f.write(text)
+    return root
+
+
+def build_replay(force=False, jobs=8):
+    """Copy the reference's src/ and include/ to oracle/_ref/replay/, apply REPLAY_PATCHES and
+    build the replay driver with the hooks of oracle/ref_replay."""
+    if replay_built() and not force:
+        return REPLAY_DRIVER
+    if not reference_available():
+        raise RuntimeError("reference sources not found")
+    root = _patched_tree(REPLAY_OUT, REPLAY_PATCHES)
     return _compile(root, REPLAY_OUT, REPLAY_DRIVER, extra_sources=[os.path.join(HOOKS, "sbp_replay.cpp")],
                     extra_flags=["-I" + HOOKS, "-include", os.path.join(HOOKS, "sbp_replay.h")], jobs=jobs)
+
+
+# ---- the capped timing build: the reference unchanged except for a sweep cap -------------------
+# Bounded CPU-baseline samples need finetune calls of a few sweeps; MAX_NUM_ITERATIONS is a
+# compile-time 100 (include/finetune.hpp:56).  Only that bound changes (SBP_REF_MAX_SWEEPS, default
+# 100); FP32 logs, unseeded engines and everything else stay the reference's.
+CAPPED_OUT = os.path.join(OUT, "capped")
+CAPPED_DRIVER = os.path.join(CAPPED_OUT, "ref_driver")
+CAPPED_PATCHES = [
+    ("include/finetune.hpp", "lit", "static const int MAX_NUM_ITERATIONS = 100;",
+     "static const int MAX_NUM_ITERATIONS = sbp_ref_sweep_cap();", 1),
+]
+
+
+def capped_built():
+    return os.path.exists(CAPPED_DRIVER)
+
+
+def build_capped(force=False, jobs=8):
+    if capped_built() and not force:
+        return CAPPED_DRIVER
+    if not reference_available():
+        raise RuntimeError("reference sources not found")
+    root = _patched_tree(CAPPED_OUT, CAPPED_PATCHES)
+    return _compile(root, CAPPED_OUT, CAPPED_DRIVER,
+                    extra_flags=["-include", os.path.join(HERE, "ref_shims", "sweep_cap.h")], jobs=jobs)
 
 
 def _write_edges(path, V, src, dst):
@@ -235,16 +267,22 @@ def _write_edges(path, V, src, dst):
         f.write(np.ascontiguousarray(dst, np.int32).tobytes())
 
 
-def run_finetune(V, src, dst, assignment, algo="async_gibbs", batches=10, threads=None):
+def run_finetune(V, src, dst, assignment, algo="async_gibbs", batches=10, threads=None, driver=None, max_sweeps=0):
+    """One reference finetune call from `assignment` (labels 0..B-1, every block non-empty);
+    max_sweeps > 0 caps the call's sweeps (the capped build)."""
     threads = threads or os.cpu_count()
+    env = dict(os.environ)
+    if max_sweeps > 0:
+        driver = driver or CAPPED_DRIVER
+        env["SBP_REF_MAX_SWEEPS"] = str(max_sweeps)
     with tempfile.TemporaryDirectory() as d:
         e, a = os.path.join(d, "e.bin"), os.path.join(d, "a.bin")
         _write_edges(e, V, src, dst)
         with open(a, "wb") as f:
             f.write(np.int32(int(assignment.max()) + 1).tobytes())
             f.write(np.ascontiguousarray(assignment, np.int32).tobytes())
-        out = subprocess.run([DRIVER, "finetune", e, algo, a, str(batches), str(threads)], capture_output=True,
-                             text=True, check=True).stdout
+        out = subprocess.run([driver or DRIVER, "finetune", e, algo, a, str(batches), str(threads)],
+                             capture_output=True, text=True, check=True, env=env).stdout
     return json.loads(out.strip().splitlines()[-1])
 
 
@@ -262,23 +300,54 @@ def run_sbp(V, src, dst, algo="async_gibbs", batches=10, threads=None, approxima
 
 
 def split_blocks(truth, parts=10, seed=0):
-    """The planted partition with every block split into `parts` random sub-blocks: a structured
-    mid-range state (B = parts * K) like the ones the SBP search passes through."""
+    """The planted partition with every block split into `parts` random sub-blocks, relabelled
+    0..B-1 (no empty block): a structured state with B near parts x planted blocks, like the
+    ones the SBP search passes through."""
     rng = np.random.default_rng(seed)
-    return (truth.astype(np.int64) * parts + rng.integers(0, parts, len(truth))).astype(np.int32)
+    a = truth.astype(np.int64) * parts + rng.integers(0, parts, len(truth))
+    _, a = np.unique(a, return_inverse=True)
+    return a.astype(np.int32)
 
 
-def time_reference(V, src, dst, truth, budget_s=12.0, algo="async_gibbs", batches=10, parts=10):
-    """Vertex visits/s of one reference finetune call on every host core, started from the
-    planted partition split into `parts` sub-blocks per block (the bounded sample)."""
-    a = split_blocks(truth, parts)
-    r = run_finetune(V, src, dst, a, algo=algo, batches=batches)
-    name = "asynchronous_gibbs" if algo == "async_gibbs" else algo
-    return {"value": r["visits"] / r["seconds"], "unit": "vertex visits/s", "cores": r["threads"],
-            "kind": "reference",
-            "sample": f"one reference finetune::{name} call (batches {batches}, --transpose) from the planted "
-                      f"partition split into {parts} sub-blocks per block (B={int(a.max()) + 1}) on the same graph: "
-                      f"{r['sweeps']} sweeps, {r['visits']} visits in {r['seconds']:.2f} s"}
+def halving_levels(V, K):
+    """Block counts of sbp::stochastic_block_partition's first descent: V/2, V/4, ... while above
+    the planted K, then K (the merges halve B each round, src/sbp.cpp:61-98)."""
+    levels, B = [], V // 2
+    while B > K:
+        levels.append(B)
+        B //= 2
+    return levels + [K]
+
+
+def time_reference_level(V, src, dst, truth, B, batches=10, threads=None, algo="async_gibbs"):
+    """One capped (1-sweep) reference finetune call at about B blocks: the planted partition split
+    into B / K sub-blocks per block."""
+    K = int(truth.max()) + 1
+    a = split_blocks(truth, max(1, B // K), seed=B)
+    r = run_finetune(V, src, dst, a, algo=algo, batches=batches, threads=threads, max_sweeps=1)
+    r["B"] = int(a.max()) + 1
+    return r
+
+
+def time_reference(V, src, dst, truth, budget_s=20.0, batches=10, threads=None):
+    """Vertex visits/s of the reference's asynchronous Gibbs on every host core, over 1-sweep
+    calls at the partition's block-count levels (halving_levels), taken from the smallest B up
+    until `budget_s` of sweep time: the bounded CPU baseline."""
+    K = int(truth.max()) + 1
+    levels = halving_levels(V, K)[::-1]
+    visits, secs, done = 0, 0.0, []
+    for B in levels:
+        r = time_reference_level(V, src, dst, truth, B, batches, threads)
+        visits += r["visits"]
+        secs += r["seconds"]
+        done.append(r["B"])
+        if secs >= budget_s:
+            break
+    return {"value": visits / secs, "unit": "vertex visits/s", "cores": threads or os.cpu_count(), "kind": "reference",
+            "sample": f"reference finetune::asynchronous_gibbs (batches {batches}, --transpose; the build's only change "
+                      f"is a sweep cap) for 1 sweep at each of B = {done} (the planted partition split into B/K "
+                      f"sub-blocks; the partition's halving schedule from the planted K upwards): {visits} visits "
+                      f"in {secs:.2f} s"}
 
 
 if __name__ == "__main__":

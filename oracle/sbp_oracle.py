@@ -280,3 +280,50 @@ def sbp(graph, algo=GIBBS, batches=10, approximate=True, asynciterations=2**31 -
         raise RuntimeError("oracle sbp failed")
     return out, dict(mdl=rs.mdl, num_blocks=rs.num_blocks, outer_iterations=rs.outer_iterations,
                      mcmc_sweeps=rs.mcmc_sweeps, visits=rs.visits, accepted=rs.accepted)
+
+
+# ------------------------------------------------------------------------------------------
+# Partition quality (src/evaluate.cpp:7-178), restated in numpy; the block <-> community
+# matching of the accuracy is scipy's linear_sum_assignment (the reference uses the Hungarian
+# method of extern/hungarian).
+# ------------------------------------------------------------------------------------------
+def contingency(alg, truth):
+    """Table with rows = algorithm blocks, columns = true communities numbered in order of first
+    appearance (evaluate::hungarian's translator); vertices with truth < 0 are not counted."""
+    alg = np.asarray(alg, np.int64)
+    truth = np.asarray(truth, np.int64)
+    known = truth >= 0
+    _, first = np.unique(truth[known], return_index=True)
+    order = np.unique(truth[known])[np.argsort(first)]
+    col = {int(t): i for i, t in enumerate(order)}
+    cols = np.array([col[int(t)] for t in truth[known]], np.int64)
+    table = np.zeros((int(alg.max()) + 1, len(order)), np.int64)
+    np.add.at(table, (alg[known], cols), 1)
+    return table
+
+
+def contingency_metrics(table, num_vertices):
+    """calculate_f1_score and calculate_nmi (src/evaluate.cpp:7-96) with exact integer pair counts."""
+    from scipy.optimize import linear_sum_assignment
+    t = np.asarray(table, np.int64)
+    N = float(num_vertices)
+    rows, cols = t.sum(1).astype(np.float64), t.sum(0).astype(np.float64)
+    cell_pairs = float((t * (t - 1)).sum()) / 2.0
+    row_pairs = float((rows * (rows - 1)).sum()) / 2.0
+    col_pairs = float((cols * (cols - 1)).sum()) / 2.0
+    agree_diff = (N * N + float((t * t).sum()) - float((rows ** 2).sum() + (cols ** 2).sum())) / 2.0
+    recall, precision = cell_pairs / row_pairs, cell_pairs / col_pairs
+    p = t / N
+    pr, pc = rows / N, cols / N
+    h = lambda q: -float(np.sum(q[q > 0] * np.log(q[q > 0])))
+    nz = p > 0
+    mi = float(np.sum(p[nz] * np.log(p[nz] / np.outer(pr, pc)[nz])))
+    ri, ci = linear_sum_assignment(t, maximize=True)
+    return {"f1": 2 * precision * recall / (precision + recall), "precision": precision, "recall": recall,
+            "rand_index": (cell_pairs + agree_diff) / (N * (N - 1) / 2.0), "nmi": mi / np.sqrt(h(pr) * h(pc)),
+            "accuracy": float(t[ri, ci].sum()) / N}
+
+
+def evaluate(alg, truth):
+    t = contingency(alg, truth)
+    return dict(contingency_metrics(t, len(alg)), table=t)
