@@ -181,6 +181,9 @@ def reduce_over_ranks(ms, count, device):
     return float(t.item()), float(c.item())
 
 
+FALLBACK = 0.05   # a learned sweep accepting fewer than 5 % of its visits hands the call to the plain proposal
+
+
 def learned_vs_plain(S, O, dcsbm, np):
     """Time to final MDL, learned vs plain proposal, on the 200,000-vertex / 71-block DC-SBM.
 
@@ -190,8 +193,11 @@ def learned_vs_plain(S, O, dcsbm, np):
     random blocks).  Then three full stochastic_block_partition runs on the 200k graph (second
     of two runs timed, device clock):
       plain   - the plain proposal with the reference's asynchronous-Gibbs schedule;
-      learned - the learned proposal, early stop on per-sweep MDL changes;
-      plain_same_stop - ablation: the plain proposal with that same early stop."""
+      learned - the learned proposal, early stop on per-sweep MDL changes, the plain proposal as
+                the fallback of a sweep whose acceptance drops below FALLBACK;
+      learned_untrained - the same with the network's initial weights (what training adds);
+      learned_no_fallback - the learned proposal without the fallback;
+      plain_same_stop - ablation: the plain proposal with the learned runs' early stop."""
     c4 = dict(dcsbm.CONFIGS[4])
     K = c4["K"]
     t0 = time.perf_counter()
@@ -213,9 +219,15 @@ def learned_vs_plain(S, O, dcsbm, np):
     prep = time.perf_counter() - t0
     V, s, d, truth = dcsbm.config_graph(4)
     g = S.Graph(V, s, d)
+    untrained = S.Mlp(seed=1)   # the same network, features and mixture, weights as initialised
     runs = {}
     for name, fn in (("plain", lambda: S.sbp.stochastic_block_partition(g, batches=10, seed=1)),
-                     ("learned", lambda: S.learned.stochastic_block_partition(g, mlp, batches=10, seed=1, stop_rule=1)),
+                     ("learned", lambda: S.learned.stochastic_block_partition(g, mlp, batches=10, seed=1, stop_rule=1,
+                                                                              fallback_acceptance=FALLBACK)),
+                     ("learned_untrained", lambda: S.learned.stochastic_block_partition(
+                         g, untrained, batches=10, seed=1, stop_rule=1, fallback_acceptance=FALLBACK)),
+                     ("learned_no_fallback", lambda: S.learned.stochastic_block_partition(g, mlp, batches=10, seed=1,
+                                                                                          stop_rule=1)),
                      ("plain_same_stop", lambda: S.learned.stochastic_block_partition(g, None, batches=10, seed=1,
                                                                                        stop_rule=1))):
         fn()
@@ -223,14 +235,17 @@ def learned_vs_plain(S, O, dcsbm, np):
         runs[name] = {"seconds": st["total_seconds"], "mdl": st["mdl"], "blocks": st["num_blocks"],
                       "sweeps": st["sweeps"], "learned_sweeps": st["learned_sweeps"],
                       "nmi_vs_planted": float(O.nmi(out, truth))}
-    p, l = runs["plain"], runs["learned"]
+    p, l, u = runs["plain"], runs["learned"], runs["learned_untrained"]
     return {"workload": "directed DC-SBM 200000 V / 71 blocks (Dirichlet alpha 1, gamma 2.5 on [10,100], w 0.7, seed 4)",
             "edges": int(g.E), "training": {"graphs": 20, "vertices_each": 50_000, "samples": samples,
                                            "steps": tst["steps"], "first_loss": tst["first_loss"],
                                            "last_loss": tst["last_loss"], "train_seconds": tst["seconds"],
                                            "collect_and_train_seconds": prep},
+            "fallback_acceptance": FALLBACK,
             **runs, "time_ratio_plain_over_learned": p["seconds"] / l["seconds"],
             "mdl_gap_learned_vs_plain": (l["mdl"] - p["mdl"]) / p["mdl"],
+            "time_ratio_untrained_over_trained": u["seconds"] / l["seconds"],
+            "mdl_gap_untrained_vs_plain": (u["mdl"] - p["mdl"]) / p["mdl"],
             "target": "learned reaches the plain final MDL within 0.5 % in at least 2x less wall time"}
 
 

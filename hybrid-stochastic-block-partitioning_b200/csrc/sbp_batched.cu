@@ -72,7 +72,7 @@ struct SweepParams {
   int ngraphs;                 // graphs in this launch (indices in glist)
   int mdl_ctas;
   int heavy_cap;
-  int pad;
+  unsigned wait_limit;         // idle claim attempts of a CTA before the launch gives up
 };
 
 constexpr int kBWarps = 8;
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kBThreads, 2)
         if (cg < 0) {
           if (*(volatile int*)nfinished >= P.ngraphs || *(volatile int*)abort_flag) {
             ex = 1;
-          } else if (++idle > (1u << 22)) {   // bounded: no stage opened for seconds
+          } else if (++idle > P.wait_limit) {   // bounded: no stage opened for too long
             atomicExch(abort_flag, 1);
             atomicOr(status, kErrBatchWait);
             ex = 1;
@@ -356,6 +356,7 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
 
   DevBuf<BGraph> dG;
   DevBuf<int> dList, dSync;   // dSync: nfinished, abort
+  Queue* hQ = nullptr;        // the queues' start state, copied in before every launch
   DevBuf<Queue> dQ;
   DevBuf<SweepParams> dP;
   DevBuf<double> dMdl;
@@ -375,8 +376,10 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
   SBP_CUDA(cudaMallocHost(&hP, sizeof(SweepParams)));
   SBP_CUDA(cudaMallocHost(&hMdl, n * sizeof(double)));
   SBP_CUDA(cudaMallocHost(&hStatus, sizeof(int)));
+  SBP_CUDA(cudaMallocHost(&hQ, n * sizeof(Queue)));
+  std::memset(hQ, 0, n * sizeof(Queue));
   struct Cleanup {
-    void* pinned[5];
+    void* pinned[6];
     std::map<int, cudaGraphExec_t> execs;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     ~Cleanup() {
@@ -386,7 +389,7 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
       if (e0) cudaEventDestroy(e0);
       if (e1) cudaEventDestroy(e1);
     }
-  } cl{{hG, hList, hP, hMdl, hStatus}, {}, nullptr, nullptr};
+  } cl{{hG, hList, hP, hMdl, hStatus, hQ}, {}, nullptr, nullptr};
   SBP_CUDA(cudaEventCreate(&cl.e0));
   SBP_CUDA(cudaEventCreate(&cl.e1));
 
@@ -506,6 +509,14 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
     hP->ngraphs = (int)act.size();
     hP->mdl_ctas = c.npartial;
     hP->heavy_cap = heavy_cap;
+    hP->wait_limit = (unsigned)g_batched_wait_limit;
+    // fault injection for the failure-detection test: the stalled graph's first stage starts
+    // with every item taken, so it never completes and no stage of that graph opens again
+    for (Slot* s : act) {
+      Queue& q = hQ[s->index];
+      std::memset(&q, 0, sizeof q);
+      if (g_batched_stall_graph == s->index) q.ctr = 1ull << 20;   // stage 0, item 2^20: beyond every stage
+    }
     const int grid = shape.ctas_per_sm * c.num_sms;
     auto ex = cl.execs.find(grid);
     if (ex == cl.execs.end()) {
@@ -514,7 +525,7 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
       cudaMemcpyAsync(dG.p, hG, n * sizeof(BGraph), cudaMemcpyHostToDevice, c.stream);
       cudaMemcpyAsync(dList.p, hList, n * sizeof(int), cudaMemcpyHostToDevice, c.stream);
       cudaMemcpyAsync(dP.p, hP, sizeof(SweepParams), cudaMemcpyHostToDevice, c.stream);
-      cudaMemsetAsync(dQ.p, 0, n * sizeof(Queue), c.stream);
+      cudaMemcpyAsync(dQ.p, hQ, n * sizeof(Queue), cudaMemcpyHostToDevice, c.stream);
       cudaMemsetAsync(dSync.p, 0, 2 * sizeof(int), c.stream);
       k_batched_sweep<<<grid, kBThreads, smem, c.stream>>>(dG.p, dList.p, dQ.p, dSync.p, dSync.p + 1, dP.p, cap,
                                                            c.status);
@@ -531,7 +542,7 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
     SBP_CUDA(cudaGraphLaunch(ex->second, c.stream));
     SBP_CUDA(cudaEventRecord(cl.e1, c.stream));
     ++g_launches;
-    g_h2d += (long long)(n * (sizeof(BGraph) + sizeof(int)) + sizeof(SweepParams));
+    g_h2d += (long long)(n * (sizeof(BGraph) + sizeof(int) + sizeof(Queue)) + sizeof(SweepParams));
     g_d2h += (long long)(n * sizeof(double) + sizeof(int));
     c.sync();
     info.sweep_launches++;

@@ -1042,6 +1042,12 @@ SbpStatus sbp_set_option(const char* name, int64_t value) {
   } else if (n == "graph_sweeps") {
     SBP_REQUIRE(value == 0 || value == 1, "graph_sweeps must be 0 or 1");
     g_graph_sweeps = (int)value;
+  } else if (n == "batched_wait_limit") {
+    SBP_REQUIRE(value >= 16 && value <= (1LL << 30), "batched_wait_limit must be in [16, 2^30]");
+    g_batched_wait_limit = value;
+  } else if (n == "batched_stall_graph") {
+    SBP_REQUIRE(value >= -1 && value < (1LL << 30), "batched_stall_graph must be -1 or a graph index");
+    g_batched_stall_graph = (int)value;
   } else {
     throw Error(SBP_ERR_INVALID_ARGUMENT, "unknown option: " + n);
   }

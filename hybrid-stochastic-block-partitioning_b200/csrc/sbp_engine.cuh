@@ -223,8 +223,10 @@ struct Context {
       SBP_CUDA(cudaMemsetAsync(status, 0, sizeof(int), stream));
       if (st & kErrReplay)
         throw Error(SBP_ERR_REPLAY, "replay stream shorter than the run needs, or a replayed proposal out of range");
-      char msg[160];
-      snprintf(msg, sizeof msg, "device status 0x%x (table overflow=1, multinomial walk=2, bounds=8)", st);
+      char msg[200];
+      snprintf(msg, sizeof msg,
+               "device status 0x%x (table overflow=1, multinomial walk=2, bounds=8, batched sweep found no "
+               "claimable work within its wait limit=16)", st);
       throw Error(SBP_ERR_DEVICE, msg);
     }
   }
@@ -292,6 +294,11 @@ inline int g_hashed_row_factor = 4;
 // sweep loop decided on the GPU; 0: one host-driven launch sequence per sweep (sbp_set_option).
 inline int g_graph_sweeps = 1;
 inline long long g_overflow_rebuilds = 0;   // rebuilds forced by a full hashed row
+// Batched partitioner: idle claim attempts of a persistent CTA before the launch gives up with an
+// error (each attempt sleeps ~0.25 us), and the fault injection of the failure-detection test
+// (index of a graph whose sweep queue never opens; -1: none).  sbp_set_option.
+inline long long g_batched_wait_limit = 1LL << 22;
+inline int g_batched_stall_graph = -1;
 
 }  // namespace sbpb
 

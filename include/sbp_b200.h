@@ -117,7 +117,12 @@ int32_t sbp_device_count(void);
  * for factor x its cells, at most 2 x for rows of more than 128 cells (larger: rows fill up and
  * are regrown less often; smaller: less memory and a cheaper walk of the row).  "graph_sweeps" (default 1): an
  * asynchronous-Gibbs finetune on dense storage runs as one CUDA graph launch whose sweep loop and
- * early stop are decided on the GPU; 0 drives every sweep from the host (same results). */
+ * early stop are decided on the GPU; 0 drives every sweep from the host (same results).
+ * "batched_wait_limit" (default 2^22, range 16-2^30): idle claim attempts (about 0.25 us each) of a
+ * persistent CTA of sbp_partition_batched before its launch gives up and the call fails with
+ * SBP_ERR_DEVICE.  "batched_stall_graph" (default -1): fault injection for failure-detection
+ * tests -- the sweep queue of that graph of a batched launch starts with its first stage taken,
+ * so no stage of it ever opens and the launch must end by its wait limit. */
 SbpStatus sbp_set_option(const char *name, int64_t value);
 
 /* The CUDA stream every call of this library runs on (cudaStream_t), for interop and timing.

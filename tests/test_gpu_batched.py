@@ -34,6 +34,22 @@ def assert_same(out_b, st_b, out_s, st_s):
         assert st_b[k] == st_s[k], k
 
 
+def test_batched_partitions_equal_the_oracle(S, O):
+    """Each graph of a batch against the CPU oracle's own partition of it (same Philox stream):
+    assignment, block count, sweeps, visits and accepted moves bit-exact, MDL within 1e-6 (the
+    float overall entropy)."""
+    specs = uneven_graphs(400, [350, 900, 1300, 600])
+    graphs = [S.Graph(V, s, d) for V, s, d, _ in specs]
+    outs, stats, info = S.batched.stochastic_block_partition(graphs, batches=10, seed=8)
+    assert info["batched_finetunes"] > 0
+    for (V, s, d, _), out, st in zip(specs, outs, stats):
+        o_out, o_st = O.sbp(O.Graph(V, s, d), batches=10, seed=8)
+        assert np.array_equal(out, o_out)
+        assert st["num_blocks"] == o_st["num_blocks"] and st["sweeps"] == o_st["mcmc_sweeps"]
+        assert st["visits"] == o_st["visits"] and st["accepted"] == o_st["accepted"]
+        assert st["mdl"] == pytest.approx(o_st["mdl"], rel=1e-6)
+
+
 def test_batched_equals_single_partitions(S):
     specs = uneven_graphs(100, [300, 1700, 800, 2500, 450, 1200])
     graphs = []
@@ -88,3 +104,24 @@ def test_batched_single_graph_and_errors(S):
     assert_same(outs[0], stats[0], out_s, st_s)
     with pytest.raises(S.SbpError):
         S.batched.stochastic_block_partition([g], batches=0)
+
+
+def test_batched_wait_runs_out_and_the_library_stays_usable(S):
+    """Failure detection without a GPU fault: a graph's sweep queue is made on the host so that it
+    never opens (sbp_set_option "batched_stall_graph"); the persistent CTAs' bounded idle wait
+    (set short here) runs out, the call fails with SBP_ERR_DEVICE naming the wait, and the next
+    call on the same context succeeds."""
+    graphs = [S.Graph(*random_graph(600, 5, 301)[:3]), S.Graph(*random_graph(800, 6, 302)[:3])]
+    S.set_option("batched_wait_limit", 4096)
+    S.set_option("batched_stall_graph", 1)
+    try:
+        with pytest.raises(S.SbpError) as e:
+            S.batched.stochastic_block_partition(graphs, batches=4, seed=3)
+        assert e.value.code == 5 and "wait limit" in str(e.value)
+    finally:
+        S.set_option("batched_stall_graph", -1)
+        S.set_option("batched_wait_limit", 1 << 22)
+    outs, _, _ = S.batched.stochastic_block_partition(graphs, batches=4, seed=3)
+    for g, out in zip(graphs, outs):
+        single, _ = S.sbp.stochastic_block_partition(g, batches=4, seed=3)
+        assert np.array_equal(out, single)

@@ -254,3 +254,47 @@ def test_learned_partition_recovers_the_planted_blocks(S, O):
     assert O.nmi(out, truth) > 0.9
     ob = O.Blockmodel(O.Graph(V, s, d), int(out.max()) + 1, out)
     assert st["mdl"] == pytest.approx(ob.mdl(), rel=1e-5)
+
+
+def sweeps_to_reach(trace, target):
+    hit = np.nonzero(np.asarray(trace) <= target)[0]
+    return int(hit[0]) + 1 if len(hit) else None
+
+
+def test_trained_network_beats_the_untrained_one_on_a_held_out_graph(S):
+    """What training adds: on a graph it never saw (same law, other seed), the trained network
+    reaches the plain finetune's final MDL (within 0.5 %) in fewer sweeps than the same proposal
+    (same features, same mixture, same epsilon) with untrained weights."""
+    import dcsbm
+    law = dict(dcsbm.CONFIGS[4], V=20_000, K=24)
+    ds = S.Dataset(2_000_000)
+    for seed in (200, 201, 202):
+        V, s, d, tr = dcsbm.generate(**{**law, "seed": seed})
+        g = S.Graph(V, s, d)
+        rng = np.random.default_rng(seed)
+        for frac, sweeps in ((0.2, 3), (0.5, 4), (1.0, 4)):
+            a = tr.copy()
+            f = rng.random(V) < frac
+            a[f] = rng.integers(0, law["K"], f.sum())
+            S.learned.collect_moves(S.Blockmodel(g, law["K"], a.astype(np.int32)), ds, batches=10, sweeps=sweeps,
+                                    seed=seed)
+    trained = S.Mlp(seed=1)
+    tst = trained.train(ds, epochs=3, batch=1024, lr=2e-3, seed=0)
+    assert tst["last_loss"] < tst["first_loss"]
+    untrained = S.Mlp(seed=1)
+    V, s, d, tr = dcsbm.generate(**{**law, "seed": 300})
+    g = S.Graph(V, s, d)
+    rng = np.random.default_rng(300)
+    start = tr.copy()
+    f = rng.random(V) < 0.6
+    start[f] = rng.integers(0, law["K"], f.sum())
+    start = start.astype(np.int32)
+    # every run makes all 40 sweeps (the asynchronous-Gibbs early stop compares with the start MDL)
+    plain = S.learned.finetune(S.Blockmodel(g, law["K"], start), None, batches=10, seed=5, max_sweeps=40)
+    target = plain["trace_mdl"].min() * 1.005
+    runs = {"plain": sweeps_to_reach(plain["trace_mdl"], target)}
+    for name, net in (("trained", trained), ("untrained", untrained)):
+        st = S.learned.finetune(S.Blockmodel(g, law["K"], start), net, batches=10, seed=5, max_sweeps=40)
+        runs[name] = sweeps_to_reach(st["trace_mdl"], target)
+    assert runs["trained"] is not None, runs
+    assert runs["untrained"] is None or runs["trained"] < runs["untrained"], runs
