@@ -9,7 +9,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 SOURCES = ["sbp_kernels.cu", "sbp_sparse.cu", "sbp_sort.cu", "sbp_engine.cu", "sbp_mlp.cu", "sbp_learned.cu",
-           "sbp_batched.cu", "sbp_noalloc.cu", "sbp_ingest.cu", "sbp_evaluate.cu"]
+           "sbp_batched.cu", "sbp_noalloc.cu", "sbp_ingest.cu", "sbp_evaluate.cu",
+           "sbp_eval_small.cu"]
 HEADERS = ["sbp_device.cuh", "sbp_kernels.cuh", "sbp_sort.cuh", "sbp_engine.cuh", "sbp_mlp.cuh", "sbp_steps.cuh",
            "sbp_error.h",
            os.path.join("..", "..", "include", "sbp_b200.h")]

@@ -294,6 +294,10 @@ inline int g_hashed_row_factor = 4;
 // sweep loop decided on the GPU; 0: one host-driven launch sequence per sweep (sbp_set_option).
 inline int g_graph_sweeps = 1;
 inline long long g_overflow_rebuilds = 0;   // rebuilds forced by a full hashed row
+// 1: light vertices of dense blockmodels with B <= kSmallB are evaluated by the group kernel
+// (sbp_eval_small.cu); 0: by the warp-per-vertex kernel (sbp_set_option "small_b_kernel").
+inline int g_small_b_kernel = 1;
+inline bool use_small_kernel(const SbpBlockmodel& bm);
 // Batched partitioner: idle claim attempts of a persistent CTA before the launch gives up with an
 // error (each attempt sleeps ~0.25 us), and the fault injection of the failure-detection test
 // (index of a graph whose sweep queue never opens; -1: none).  sbp_set_option.
@@ -493,6 +497,8 @@ struct SbpBlockmodel {
 };
 
 namespace sbpb {
+
+inline bool use_small_kernel(const SbpBlockmodel& bm) { return g_small_b_kernel && !bm.sparse && bm.B <= kSmallB; }
 
 struct MhResult {
   long long visits = 0, moved = 0, accepted = 0;

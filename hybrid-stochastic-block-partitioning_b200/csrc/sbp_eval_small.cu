@@ -1,0 +1,302 @@
+// Asynchronous-Gibbs vertex evaluation for a dense block matrix with at most kSmallB blocks:
+// the regime of the last outer iterations of a partition, where the block count is near the
+// planted one (the same proposal, Hastings correction, delta-MDL and accept test as
+// evaluate_vertex in sbp_device.cuh; src/common.cpp:131-192, src/entropy.cpp:296-401, 495-557,
+// src/finetune.cpp:19-29).
+//
+// Layout of the work:
+//  * a group of G lanes evaluates one vertex, so a warp carries 32 / G vertices at a time; every
+//    loop runs to the largest trip count of the warp's groups (lanes past their own count are
+//    predicated off), so the group shuffles always see the whole warp converged;
+//  * the neighbour-block histogram of a vertex is a direct-indexed array of B words in shared
+//    memory (out count | in count << 15 | presence << 30) plus the list of blocks present: no
+//    hashing, one shared atomic per neighbour;
+//  * the frozen state of the batch (assignment, block matrix, degrees, log table) is read through
+//    the read-only data cache;
+//  * the FP64 terms of a changed cell are computed by the lane that loaded the cell.
+// Summation orders differ from evaluate_vertex, so delta-MDL and the Hastings factor agree with
+// it to rounding; the integer zero-snap scale T and every integer input are the same.
+#include "sbp_engine.cuh"
+
+namespace sbpb {
+namespace {
+
+constexpr unsigned kInShift = 15;
+constexpr unsigned kCountMask = (1u << 15) - 1;
+constexpr unsigned kPresent = 1u << 30;
+
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o, G);
+  return v;
+}
+template <int G>
+__device__ __forceinline__ long long group_sum_ll(long long v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o, G);
+  return v;
+}
+__device__ __forceinline__ unsigned long long warp_sum_ull(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+__device__ __forceinline__ int warp_max_int(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+template <int G>
+__global__ void __launch_bounds__(kSmallThreads)
+    k_gibbs_eval_small(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
+                       int* prop, int* moved_list, int* n_moved, unsigned long long* counters, int* status,
+                       const SweepCtl* ctl, int batch) {
+  constexpr int kGroups = kSmallThreads / G;
+  __shared__ unsigned s_w[kGroups][kSmallB];
+  __shared__ int s_list[kGroups][kSmallB];
+  __shared__ int s_n[kGroups];
+  if (ctl) {
+    sweep = ctl->sweep;
+    n_moved = ctl->n_moved + ((ctl->gen0 + (unsigned)batch) & 1u);
+  }
+  const int lane = threadIdx.x & 31;
+  const int gl = lane & (G - 1);
+  const int gid = threadIdx.x / G;
+  const int gbase = lane & ~(G - 1);   // first lane of this group in the warp
+  unsigned* W = s_w[gid];
+  int* L = s_list[gid];
+  const int B = bm.B;
+  const int ld = bm.ld;
+  for (int i = gl; i < kSmallB; i += G) W[i] = 0u;
+  if (gl == 0) s_n[gid] = 0;
+  __syncwarp();
+  unsigned long long c_visit = 0, c_moved = 0, c_acc = 0;
+  const bool given = rng.moves != 0;
+  const int groups_total = gridDim.x * kGroups;
+  // warp-uniform outer loop: the warp's groups take consecutive list entries
+  const int warp_first = (blockIdx.x * kSmallThreads + (threadIdx.x & ~31)) / G;
+  for (int base = warp_first; base < n; base += groups_total) {
+    const int item = base + (lane / G);
+    const bool valid = item < n;
+    int v = 0, r = 0, o0 = 0, i0 = 0, k_out = 0, k_in = 0, self = 0;
+    uint4 x = make_uint4(0, 0, 0, 0);
+    if (valid) {
+      v = __ldg(verts + item);
+      r = __ldg(bm.b + v);
+      o0 = __ldg(g.out_ptr + v);
+      k_out = __ldg(g.out_ptr + v + 1) - o0;
+      i0 = __ldg(g.in_ptr + v);
+      k_in = __ldg(g.in_ptr + v + 1) - i0;
+      self = __ldg(g.self + v);
+      x = draw_record(rng, (uint32_t)v, (uint32_t)sweep, 0u, (long long)sweep * g.V + v, status);
+    }
+    const int k = k_out + k_in;
+    const int idx = (valid && k > 0 && !given) ? (int)scale32(x.x, k) : -1;
+    // 1. neighbour-block histogram and the proposal's neighbour block
+    int tblk = -1;
+    const int gather_iters = warp_max_int((k + G - 1) / G);
+    for (int it = 0; it < gather_iters; ++it) {
+      const int e = it * G + gl;
+      int bu = -1;
+      if (e < k) {
+        const bool out = e < k_out;
+        const int u = out ? __ldg(g.out_idx + o0 + e) : __ldg(g.in_idx + i0 + (e - k_out));
+        bu = __ldg(bm.b + u);
+        if (!(out && u == v)) {   // the self loop is not counted (its block enters as present)
+          const unsigned old = atomicAdd(W + bu, out ? 1u : (1u << kInShift));
+          if (old == 0u) L[atomicAdd(&s_n[gid], 1)] = bu;
+        }
+      }
+      const int src = idx - it * G;
+      const int pick = __shfl_sync(kFull, bu, (src >= 0 && src < G) ? src : 0, G);
+      if (src >= 0 && src < G) tblk = pick;
+    }
+    if (valid && self && gl == 0) {
+      const unsigned old = atomicOr(W + r, kPresent);
+      if (old == 0u) L[atomicAdd(&s_n[gid], 1)] = r;
+    }
+    __syncwarp();
+    // 2. the proposal: the multinomial over row t of M then column t (ascending), as the
+    //    dense walks of evaluate_vertex
+    int s = r;
+    {
+      const bool walk = valid && !given && k > 0;
+      const int t = walk ? tblk : 0;
+      long long tg = -1;
+      bool in_row = true;
+      if (walk) {
+        const int dot = __ldg(bm.d_out + t), dit = __ldg(bm.d_in + t);
+        const long long target = scale32(x.y, (long long)dot + (long long)dit);
+        in_row = target < dot;
+        tg = in_row ? target : target - dot;
+      }
+      const int* row = (in_row ? bm.M : bm.MT) + (size_t)t * ld;
+      constexpr int kPer = kSmallB / G;   // counts per lane
+      int vals[kPer];
+      long long lsum = 0;
+#pragma unroll
+      for (int q = 0; q < kPer / 4; ++q) {
+        const int4 c4 = __ldg(reinterpret_cast<const int4*>(row + gl * kPer) + q);
+        vals[4 * q] = c4.x;
+        vals[4 * q + 1] = c4.y;
+        vals[4 * q + 2] = c4.z;
+        vals[4 * q + 3] = c4.w;
+        lsum += (long long)c4.x + c4.y + c4.z + c4.w;
+      }
+      long long incl = lsum;
+#pragma unroll
+      for (int o = 1; o < G; o <<= 1) {
+        const long long y = __shfl_up_sync(kFull, incl, o, G);
+        if (gl >= o) incl += y;
+      }
+      const unsigned gmask = (G == 32 ? kFull : ((1u << G) - 1u) << gbase);
+      const unsigned hit = __ballot_sync(kFull, walk && incl > tg) & gmask;
+      int col = -1;
+      if (walk && hit && gl == __ffs(hit) - 1 - gbase) {
+        long long rem = tg - (incl - lsum);
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+          if (col < 0) {
+            if (rem < vals[q]) col = gl * kPer + q;
+            else rem -= vals[q];
+          }
+        }
+      }
+      const int found = __shfl_sync(kFull, col, hit ? __ffs(hit) - 1 - gbase : 0, G);
+      if (walk) {
+        s = found;
+        if (s < 0 || s >= B) {
+          if (gl == 0) atomicOr(status, kErrScan);
+          s = r;
+        }
+      } else if (valid && given) {
+        s = (int)x.x;
+        if (s < 0 || s >= B) {   // a visit the stream has no proposal for
+          if (gl == 0) atomicOr(status, kErrReplay);
+          s = r;
+        }
+      } else if (valid) {
+        s = random_block(r, B, x.y);
+      }
+    }
+    const bool active = valid && s != r;
+    // 3. delta-MDL and the Hastings correction of the move r -> s
+    double fwd = 0.0, bwd = 0.0, dS = 0.0;
+    long long T = 0;
+    int co_r = 0, ci_r = 0, co_s = 0, ci_s = 0;
+    int M_rr = 0, M_rs = 0, M_sr = 0, M_ss = 0, dout_r = 0, dout_s = 0, din_r = 0, din_s = 0;
+    if (active) {
+      const unsigned wr = W[r], ws = W[s];
+      co_r = wr & kCountMask;
+      ci_r = (wr >> kInShift) & kCountMask;
+      co_s = ws & kCountMask;
+      ci_s = (ws >> kInShift) & kCountMask;
+      M_rr = __ldg(bm.M + (size_t)r * ld + r);
+      M_rs = __ldg(bm.M + (size_t)r * ld + s);
+      M_sr = __ldg(bm.M + (size_t)s * ld + r);
+      M_ss = __ldg(bm.M + (size_t)s * ld + s);
+      dout_r = __ldg(bm.d_out + r);
+      dout_s = __ldg(bm.d_out + s);
+      din_r = __ldg(bm.d_in + r);
+      din_s = __ldg(bm.d_in + s);
+    }
+    const int d_rr = -co_r - ci_r - self;
+    const int d_rs = -co_s + ci_r;
+    const int d_sr = co_r - ci_s;
+    const int d_ss = co_s + ci_s + self;
+    const int kin_self = k_in + self;
+    const int nent = active ? s_n[gid] : 0;
+    const int ent_iters = warp_max_int((nent + G - 1) / G);
+    for (int it = 0; it < ent_iters; ++it) {
+      const int j = it * G + gl;
+      if (j < nent) {
+        const int u = L[j];
+        const unsigned wu = W[u];
+        const int co = wu & kCountMask, ci = (wu >> kInShift) & kCountMask;
+        const int M_ru = __ldg(bm.M + (size_t)r * ld + u);
+        const int M_ur = __ldg(bm.MT + (size_t)r * ld + u);
+        const int M_su = __ldg(bm.M + (size_t)s * ld + u);
+        const int M_us = __ldg(bm.MT + (size_t)s * ld + u);
+        const int du = __ldg(bm.d + u);
+        const bool is_r = u == r, is_s = u == s;
+        const double c = (double)(co + ci + (is_r ? self : 0));
+        fwd += c * (M_su + M_us + 1.0) / ((double)du + (double)B);
+        const double bw = is_r ? (double)(M_rr + d_rr) + (double)(M_rr + d_rr) + 1.0
+                        : is_s ? (double)(M_rs + d_rs) + (double)(M_sr + d_sr) + 1.0
+                               : (double)(M_ru - co) + (double)(M_ur - ci) + 1.0;
+        const int nd = is_r ? (dout_r - k_out) + (din_r - k_in) - (M_rr + d_rr)
+                     : is_s ? (dout_s + k_out) + (din_s + k_in) - (M_ss + d_ss) : du;
+        bwd += c * bw / ((double)nd + (double)B);
+        if (!is_r && !is_s) {   // cells (r,u) (s,u) for out-edges to u, (u,r) (u,s) for in-edges
+          if (co) {
+            dS += dxlogx_int(bm.logt, M_ru, M_ru - co) + dxlogx_int(bm.logt, M_su, M_su + co);
+            T += 2LL * (M_ru + M_su);
+          }
+          if (ci) {
+            dS += dxlogx_int(bm.logt, M_ur, M_ur - ci) + dxlogx_int(bm.logt, M_us, M_us + ci);
+            T += 2LL * (M_ur + M_us);
+          }
+        }
+      }
+    }
+    if (active) {
+      // corner cells (r,r) (r,s) (s,r) (s,s), then the out- and in-degrees of r and s
+      for (int q = gl; q < 8; q += G) {
+        const int a = q == 0 ? M_rr : q == 1 ? M_rs : q == 2 ? M_sr : q == 3 ? M_ss
+                    : q == 4 ? dout_r : q == 5 ? dout_s : q == 6 ? din_r : din_s;
+        const int d = q == 0 ? d_rr : q == 1 ? d_rs : q == 2 ? d_sr : q == 3 ? d_ss
+                    : q == 4 ? -k_out : q == 5 ? k_out : q == 6 ? -kin_self : kin_self;
+        if (d) dS += (q < 4 ? 1.0 : -1.0) * dxlogx_int(bm.logt, a, a + d);
+        T += q < 4 ? (d ? 2LL * a + d : 0LL) : 2LL * a;
+      }
+      // the double count of a present net-zero (r,s) / (s,r) Delta cell
+      if (gl == 0 && (co_s > 0 || ci_r > 0) && d_rs == 0 && M_rs > 0)
+        dS += (double)M_rs * (log1p((double)kin_self / (double)din_s) + log1p(-(double)k_out / (double)dout_r));
+      if (gl == (G > 1 ? 1 : 0) && (co_r > 0 || ci_s > 0) && d_sr == 0 && M_sr > 0)
+        dS += (double)M_sr * (log1p(-(double)kin_self / (double)din_r) + log1p((double)k_out / (double)dout_s));
+    }
+    fwd = group_sum<G>(fwd);
+    bwd = group_sum<G>(bwd);
+    dS = group_sum<G>(dS);
+    T = group_sum_ll<G>(T);
+    if (active) {
+      if (fabs(dS) <= 0x1p-40 * (double)T * g.log_E) dS = 0.0;
+      const double H = (k == 0) ? 1.0 : bwd / fwd;
+      double ap = exp(-3.0 * dS) * H;
+      ap = ap >= 1.0 ? 1.0 : ap;
+      const double u = given ? record_uniform(x) : u53(x.z, x.w);
+      if (u <= ap && gl == 0) {
+        c_acc++;
+        prop[v] = s;
+        moved_list[atomicAdd(n_moved, 1)] = v;
+      }
+    }
+    if (valid && gl == 0) {
+      c_visit++;
+      if (s != r) c_moved++;
+    }
+    // 4. clear the histogram of the group's vertex
+    __syncwarp();
+    const int nclear = valid ? s_n[gid] : 0;
+    for (int j = gl; j < nclear; j += G) W[L[j]] = 0u;
+    __syncwarp();
+    if (gl == 0) s_n[gid] = 0;
+    __syncwarp();
+  }
+  c_visit = warp_sum_ull(c_visit);
+  c_moved = warp_sum_ull(c_moved);
+  c_acc = warp_sum_ull(c_acc);
+  if (lane == 0 && c_visit) {
+    atomicAdd(counters + 0, c_visit);
+    atomicAdd(counters + 1, c_moved);
+    atomicAdd(counters + 2, c_acc);
+  }
+}
+
+}  // namespace
+
+GibbsEvalSmallKernel gibbs_eval_small_kernel() { return k_gibbs_eval_small<kSmallGroup>; }
+
+}  // namespace sbpb

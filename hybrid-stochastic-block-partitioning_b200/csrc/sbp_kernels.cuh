@@ -51,6 +51,14 @@ __global__ void __launch_bounds__(256, 2)
 using GibbsEvalKernel = void (*)(GraphView, BlockView, const int* __restrict__, int, RngParams, int, int*, int*, int*,
                                  unsigned long long*, int, int*, const SweepCtl*, int);
 inline GibbsEvalKernel gibbs_eval_kernel(bool hashed) { return hashed ? k_gibbs_eval_hashed : k_gibbs_eval_dense; }
+// Asynchronous-Gibbs evaluation for dense storage with B <= kSmallB (sbp_eval_small.cu): groups of
+// kSmallGroup lanes per vertex, direct-indexed neighbour-block histograms in shared memory.
+constexpr int kSmallB = 128;
+constexpr int kSmallThreads = 256;
+constexpr int kSmallGroup = 8;
+using GibbsEvalSmallKernel = void (*)(GraphView, BlockView, const int* __restrict__, int, RngParams, int, int*, int*,
+                                      int*, unsigned long long*, int*, const SweepCtl*, int);
+GibbsEvalSmallKernel gibbs_eval_small_kernel();
 __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, const int* n_moved, const int* prop,
                               int* qr, int* qs, unsigned long long* last, unsigned gen, const SweepCtl* ctl, int batch);
 __global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved, int* prop,
