@@ -58,6 +58,7 @@ def args_parse():
     ap.add_argument("--batches", type=int, default=10)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain comparison")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched 64-graph comparison")
+    ap.add_argument("--no-mh", action="store_true", help="skip the Metropolis-Hastings / hybrid partitions")
     ap.add_argument("--host-sweeps", action="store_true",
                     help="drive every finetune sweep from the host (same kernels and results) instead of one CUDA "
                          "graph per finetune call; for kernel profilers, which do not profile the kernel nodes of a "
@@ -142,6 +143,20 @@ def cpu_baseline_port(V, src, dst, truth, budget_s=12.0):
     return {"value": visits / dt, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"{sweeps} async-Gibbs sweeps (batches 10) at the planted B={K} on the same graph, "
                       f"{visits} visits in {dt:.1f} s"}
+
+
+def profiled_traffic(kernel, config):
+    """DRAM bytes per launch of `kernel` on workload `config` as one ncu capture measured them
+    (dram__bytes_read.sum + dram__bytes_write.sum), from the summaries under profiles/: a line
+    `traffic_bytes_per_launch[<kernel>@config<N>]: <bytes>` with the capture's command beside it."""
+    import glob
+    import re
+    pat = re.compile(r"traffic_bytes_per_launch\[" + re.escape(kernel) + r"@config" + str(config) + r"\]:\s*([0-9.eE+]+)")
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        m = pat.search(open(path).read())
+        if m:
+            return float(m.group(1)), os.path.relpath(path, ROOT)
+    return None, None
 
 
 def reference_module():
@@ -247,6 +262,24 @@ def learned_vs_plain(S, O, dcsbm, np):
             "time_ratio_untrained_over_trained": u["seconds"] / l["seconds"],
             "mdl_gap_untrained_vs_plain": (u["mdl"] - p["mdl"]) / p["mdl"],
             "target": "learned reaches the plain final MDL within 0.5 % in at least 2x less wall time"}
+
+
+def mh_and_hybrid(S, O, dcsbm):
+    """Full partitions with Metropolis-Hastings and with the hybrid schedule (batches 10) on the
+    20,000-vertex / 32-block graph, second of two runs timed on the device clock."""
+    V, s, d, truth = dcsbm.config_graph(2)
+    g = S.Graph(V, s, d)
+    out = {"workload": WORKLOADS[2]}
+    for algo in ("metropolis_hastings", "hybrid_mcmc"):
+        S.sbp.stochastic_block_partition(g, algorithm=algo, batches=10, seed=2)
+        a, st = S.sbp.stochastic_block_partition(g, algorithm=algo, batches=10, seed=2)
+        out[algo] = {"seconds": st["total_seconds"], "mcmc_seconds": st["mcmc_seconds"], "sweeps": st["sweeps"],
+                     "visits": st["visits"], "visits_per_s": st["visits"] / st["total_seconds"], "mdl": st["mdl"],
+                     "blocks": st["num_blocks"], "nmi_vs_planted": float(O.nmi(a, truth))}
+    anchor = reference_anchor(2)
+    if anchor:
+        out["reference_full_partition_async_gibbs"] = anchor
+    return out
 
 
 def batched_vs_sequential(S, dcsbm, np):
@@ -413,6 +446,7 @@ def main():
     pr = S.profile_read(reset=True)
     S.profile_enable(False)
     peak, peak_kind = peaks()
+    traffic, traffic_src = profiled_traffic("k_gibbs_eval", a.config)
     avg_ms = pr["eval_ms"] / max(1, pr["eval_launches"])
     achieved = (pr["eval_bytes"] / max(1, pr["eval_launches"])) / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
 
@@ -436,8 +470,9 @@ def main():
                     "h2d_bytes_per_step": int((pe1["h2d_bytes"] - pe0["h2d_bytes"]) / max(1, a.steps)),
                     "d2h_bytes_per_step": int((pe1["d2h_bytes"] - pe0["d2h_bytes"]) / max(1, a.steps)),
                     "ms_per_step": e2e_ms / max(1, a.steps)},
-            "roofline": {"bound": "hbm", "kernel": "k_gibbs_eval_dense / _hashed", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+            "roofline": {"bound": "hbm", "kernel": "k_gibbs_eval (small / dense / hashed)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic, "traffic_source": traffic_src,
                          "avg_launch_us": avg_ms * 1e3, "launches_profiled": int(pr["eval_launches"]),
                          "bytes_per_launch": pr["eval_bytes"] / max(1, pr["eval_launches"])},
             "gpu_launches": launches,
@@ -450,6 +485,8 @@ def main():
             line["learned_vs_plain"] = learned_vs_plain(S, O, dcsbm, np)
         if world == 1 and not a.no_batched:
             line["batched"] = batched_vs_sequential(S, dcsbm, np)
+        if world == 1 and not a.no_mh:
+            line["mh_and_hybrid"] = mh_and_hybrid(S, O, dcsbm)
         print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
