@@ -120,6 +120,13 @@ __device__ __forceinline__ double dxlogx_int(const double2* __restrict__ logt, i
   return dxlogx((double)a, (double)b);
 }
 
+// Merge delta-MDLs are rounded to a multiple of 2^-20 (about 1e-6) before merges are ranked:
+// values that are equal but for the rounding of different summation orders then compare equal
+// on every implementation, and equal values rank by proposal order and block index, as the
+// reference's loops rank exact ties.  (rint: round half to even, the same as the host's
+// nearbyint in the default rounding mode.)
+__host__ __device__ __forceinline__ double merge_score(double dS) { return rint(dS * 1048576.0) / 1048576.0; }
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
@@ -242,17 +249,26 @@ __device__ __forceinline__ void hashed_add(const long long* base, const int* mas
 // M[row, col] and MT[row, col] = M[col, row] in either representation.
 // Storage of the block matrix as a compile-time choice (kAny: decided by bm.sparse at run time).
 // Kernels instantiated for one storage carry no code for the other.
-enum class Store { kAny, kDense, kHashed };
+enum class Store { kAny, kDense, kHashed, kDenseFrozen };
+// kDenseFrozen: dense storage that no thread of the launch writes (the evaluation half of an
+// asynchronous-Gibbs batch), read through the read-only data cache.
+template <Store S>
+__device__ __forceinline__ int ldi(const int* p) {
+  if constexpr (S == Store::kDenseFrozen) return __ldg(p);
+  else return *p;
+}
 
 template <Store S = Store::kAny>
 __device__ __forceinline__ int bm_get(const BlockView& bm, int row, int col) {
   if constexpr (S == Store::kDense) return bm.M[(size_t)row * bm.ld + col];
+  else if constexpr (S == Store::kDenseFrozen) return __ldg(bm.M + (size_t)row * bm.ld + col);
   else if constexpr (S == Store::kHashed) return hashed_get(bm.rbase, bm.rmask, bm.rslot, row, col);
   else return bm.sparse ? hashed_get(bm.rbase, bm.rmask, bm.rslot, row, col) : bm.M[(size_t)row * bm.ld + col];
 }
 template <Store S = Store::kAny>
 __device__ __forceinline__ int bm_getT(const BlockView& bm, int row, int col) {
   if constexpr (S == Store::kDense) return bm.MT[(size_t)row * bm.ld + col];
+  else if constexpr (S == Store::kDenseFrozen) return __ldg(bm.MT + (size_t)row * bm.ld + col);
   else if constexpr (S == Store::kHashed) return hashed_get(bm.cbase, bm.cmask, bm.cslot, row, col);
   else return bm.sparse ? hashed_get(bm.cbase, bm.cmask, bm.cslot, row, col) : bm.MT[(size_t)row * bm.ld + col];
 }
@@ -535,6 +551,7 @@ __device__ __forceinline__ void table_add_dir(const WarpTable& t, int key, bool 
 // it) gathers every neighbour's block into the table (self loop excluded from the counts, its
 // block r inserted with zero counts).  Returns the block of neighbour element `idx` (-1 when
 // idx is out of range), the proposal's neighbour of src/common.cpp:11-26.
+template <Store ST = Store::kAny>
 __device__ __forceinline__ int gather_neighbour_blocks(const GraphView& g, const BlockView& bm, int v, int r, int o0,
                                                        int k_out, int i0, int k, int self, int idx,
                                                        const WarpTable& t, int lane, int* status) {
@@ -544,8 +561,8 @@ __device__ __forceinline__ int gather_neighbour_blocks(const GraphView& g, const
     int u0 = -1, u1 = -1;
     if (e0 < k) u0 = e0 < k_out ? __ldg(g.out_idx + o0 + e0) : __ldg(g.in_idx + i0 + (e0 - k_out));
     if (e1 < k) u1 = e1 < k_out ? __ldg(g.out_idx + o0 + e1) : __ldg(g.in_idx + i0 + (e1 - k_out));
-    const int b0 = u0 >= 0 ? bm.b[u0] : -1;
-    const int b1 = u1 >= 0 ? bm.b[u1] : -1;
+    const int b0 = u0 >= 0 ? ldi<ST>(bm.b + u0) : -1;
+    const int b1 = u1 >= 0 ? ldi<ST>(bm.b + u1) : -1;
     if (idx >= base && idx < base + kWarp) tblk = __shfl_sync(kFull, b0, idx - base);
     if (idx >= base + kWarp && idx < base + 2 * kWarp) tblk = __shfl_sync(kFull, b1, idx - base - kWarp);
     table_add_dir(t, b0, u0 >= 0 && u0 != v, e0 >= k_out, status);
@@ -576,11 +593,11 @@ __device__ __forceinline__ void prefetch_nb(const BlockView& bm, int r, const Wa
     p->ci = t.cin[h];
     p->M_ru = bm_get<ST>(bm, r, u);
     p->M_ur = bm_getT<ST>(bm, r, u);
-    p->du = bm.d[u];
+    p->du = ldi<ST>(bm.d + u);
   }
   p->M_rr = bm_get<ST>(bm, r, r);
-  p->dout_r = bm.d_out[r];
-  p->din_r = bm.d_in[r];
+  p->dout_r = ldi<ST>(bm.d_out + r);
+  p->din_r = ldi<ST>(bm.d_in + r);
 }
 
 // Position of the n-th (0-based) set bit of m; requires n < popc(m).
@@ -621,8 +638,8 @@ __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView
   const int d_ss = mc.co_s + mc.ci_s + self;
   const int M_rr = pre ? pre->M_rr : bm_get<ST>(bm, r, r), M_rs = bm_get<ST>(bm, r, s);
   const int M_sr = bm_get<ST>(bm, s, r), M_ss = bm_get<ST>(bm, s, s);
-  const int dout_r = pre ? pre->dout_r : bm.d_out[r], dout_s = bm.d_out[s];
-  const int din_r = pre ? pre->din_r : bm.d_in[r], din_s = bm.d_in[s];
+  const int dout_r = pre ? pre->dout_r : ldi<ST>(bm.d_out + r), dout_s = ldi<ST>(bm.d_out + s);
+  const int din_r = pre ? pre->din_r : ldi<ST>(bm.d_in + r), din_s = ldi<ST>(bm.d_in + s);
   const int kin_self = k_in + self;
 
   double fwd = 0.0, bwd = 0.0, dS = 0.0;
@@ -647,7 +664,7 @@ __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView
         ci = t.cin[h];
         M_ru = bm_get<ST>(bm, r, u);
         M_ur = bm_getT<ST>(bm, r, u);
-        du = bm.d[u];
+        du = ldi<ST>(bm.d + u);
       }
       M_su = bm_get<ST>(bm, s, u);
       M_us = bm_getT<ST>(bm, s, u);
@@ -741,7 +758,7 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
                                                       const WarpTable& t, int lane, int* status, int* r_out,
                                                       int* k_out_out, int* k_in_out, bool given = false) {
   EvalResult res;
-  const int r = bm.b[v];
+  const int r = ldi<ST>(bm.b + v);
   const int o0 = g.out_ptr[v], o1 = g.out_ptr[v + 1];
   const int i0 = g.in_ptr[v], i1 = g.in_ptr[v + 1];
   const int self = g.self[v];
@@ -753,7 +770,7 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
   res.dS = 0.0;
   res.H = 1.0;
   const int idx = (k > 0 && !given) ? (int)scale32(x.x, k) : -1;
-  const int tblk = gather_neighbour_blocks(g, bm, v, r, o0, k_out, i0, k, self, idx, t, lane, status);
+  const int tblk = gather_neighbour_blocks<ST>(g, bm, v, r, o0, k_out, i0, k, self, idx, t, lane, status);
   res.t = (k > 0 && !given) ? tblk : -1;
 
   NbPrefetch pre;
@@ -780,16 +797,21 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
       // the degrees of t and, in the same round trip, row t of M and of MT (B <= kChunk: the
       // whole rows, four counts per lane) or their chunk sums (up to 32 chunks); the walk then
       // picks the row (target < d_out[t]) or the column
-      const int dot = bm.d_out[tblk], dit = bm.d_in[tblk];
+      const int dot = ldi<ST>(bm.d_out + tblk), dit = ldi<ST>(bm.d_in + tblk);
       const size_t ro = (size_t)tblk * bm.ld, co = (size_t)tblk * bm.nch;
       int4 qa = make_int4(0, 0, 0, 0), qb = make_int4(0, 0, 0, 0);
       int ca = 0, cb = 0;
       if (bm.nch == 1) {
-        qa = *reinterpret_cast<const int4*>(bm.M + ro + 4 * lane);
-        qb = *reinterpret_cast<const int4*>(bm.MT + ro + 4 * lane);
+        if constexpr (ST == Store::kDenseFrozen) {
+          qa = __ldg(reinterpret_cast<const int4*>(bm.M + ro) + lane);
+          qb = __ldg(reinterpret_cast<const int4*>(bm.MT + ro) + lane);
+        } else {
+          qa = *reinterpret_cast<const int4*>(bm.M + ro + 4 * lane);
+          qb = *reinterpret_cast<const int4*>(bm.MT + ro + 4 * lane);
+        }
       } else if (lane < bm.nch) {
-        ca = bm.CS[co + lane];
-        cb = bm.CST[co + lane];
+        ca = ldi<ST>(bm.CS + co + lane);
+        cb = ldi<ST>(bm.CST + co + lane);
       }
       const long long target = scale32(x.y, (long long)dot + (long long)dit);
       const bool in_row = target < dot;

@@ -586,7 +586,7 @@ static void carry_out_advanced(int B, int to_merge, const std::vector<int>& rptr
     v += g(mss) - g(mss + get(r, r) + get(r, s) + get(s, r));
     v -= g(d_out[r]) + g(d_out[s]) - g((double)d_out[r] + d_out[s]);
     v -= g(d_in[r]) + g(d_in[s]) - g((double)d_in[r] + d_in[s]);
-    return v;
+    return merge_score(v);
   };
   struct Item {
     int from, to;

@@ -111,8 +111,8 @@ __global__ void __launch_bounds__(256, 2)
     k_gibbs_eval_dense(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
                        int* prop, int* moved_list, int* n_moved, unsigned long long* counters, int cap, int* status,
                        const SweepCtl* ctl, int batch) {
-  gibbs_eval_body<Store::kDense>(g, bm, verts, n, rng, sweep, prop, moved_list, n_moved, counters, cap, status, ctl,
-                                 batch);
+  gibbs_eval_body<Store::kDenseFrozen>(g, bm, verts, n, rng, sweep, prop, moved_list, n_moved, counters, cap, status,
+                                       ctl, batch);
 }
 __global__ void __launch_bounds__(256, 2)
     k_gibbs_eval_hashed(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
@@ -647,7 +647,7 @@ __global__ void k_merge_propose(BlockView bm, Csr rows, Csr cols, RngParams rng,
       }
       seen[nseen++] = s;
       // same value for r->s and s->r; one fixed orientation makes mutual pairs tie exactly
-      const double dS = merge_delta(bm, rows, cols, min(r, s), max(r, s), lane);
+      const double dS = merge_score(merge_delta(bm, rows, cols, min(r, s), max(r, s), lane));
       if (dS < bdS) {
         bdS = dS;
         best = s;

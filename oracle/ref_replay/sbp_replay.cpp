@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
+#include <cmath>
 #include <cstdlib>
 #include <mutex>
 #include <numeric>
@@ -183,11 +184,14 @@ void on_merge_scores(const std::vector<int> &best, const std::vector<double> &de
     }
 }
 
+// The engine's ranking score of a merge: the delta-MDL rounded to a multiple of 2^-20.
+static double merge_score(double dS) { return std::nearbyint(dS * 1048576.0) / 1048576.0; }
+
 double merge_delta_canonical(int r, int s, int k_out, int k_in, const Blockmodel &bm) {
     if (r < s) {
         const utils::ProposalAndEdgeCounts p{s, k_out, k_in, k_out + k_in};
         const Delta d = block_merge::blockmodel_delta(r, s, bm);
-        return entropy::block_merge_delta_mdl(r, p, bm, d);
+        return merge_score(entropy::block_merge_delta_mdl(r, p, bm, d));
     }
     // the same merge seen from the higher block: s into r, with s's edge counts taken as
     // common::propose_new_block takes them for a merge (outgoing / incoming edge weights)
@@ -197,7 +201,7 @@ double merge_delta_canonical(int r, int s, int k_out, int k_in, const Blockmodel
     const int ki = std::accumulate(in_b.values.begin(), in_b.values.end(), 0);
     const utils::ProposalAndEdgeCounts q{r, ko, ki, ko + ki};
     const Delta d = block_merge::blockmodel_delta(s, r, bm);
-    return entropy::block_merge_delta_mdl(s, q, bm, d);
+    return merge_score(entropy::block_merge_delta_mdl(s, q, bm, d));
 }
 
 std::vector<int> stable_sort_indices(const std::vector<double> &values) {

@@ -15,7 +15,8 @@
  *   P1 call records        src/finetune.cpp:32, 343, 413 and src/block_merge.cpp:278 (CallScope)
  *   P2 FP64 logs           include/common.hpp:35-44 (cell_entropy), include/utils.hpp:148 (nat_log)
  *   P3 merge tie order     src/block_merge.cpp:342-345 (merge_delta_canonical: the lower block id is
- *                          merged into the higher, so r->s and s->r give the same double),
+ *                          merged into the higher, so r->s and s->r give the same double, and the
+ *                          value is rounded to a multiple of 2^-20 as the engine ranks merges),
  *                          src/blockmodel/blockmodel.cpp:52 (stable order of equal delta-MDLs)
  *   P4 bounded sweeps      include/finetune.hpp:56 (MAX_NUM_ITERATIONS = max_sweeps())
  */
@@ -61,7 +62,9 @@ void on_merge_proposal(int s);
 /* Best proposal and its delta-MDL per block, before the carry-out. */
 void on_merge_scores(const std::vector<int> &best, const std::vector<double> &delta);
 /* block_merge_delta_mdl of merging r into s, always evaluated in the orientation lower id into
- * higher id with the reference's own functions (the merged blockmodel is the same either way). */
+ * higher id with the reference's own functions (the merged blockmodel is the same either way),
+ * rounded to a multiple of 2^-20: values that differ only by the rounding of their summation
+ * order then rank as ties, which the reference's loops break by proposal order and block index. */
 double merge_delta_canonical(int r, int s, int k_out, int k_in, const Blockmodel &bm);
 /* utils::sort_indices with equal values kept in index order. */
 std::vector<int> stable_sort_indices(const std::vector<double> &values);

@@ -808,6 +808,10 @@ double sbpo_merge_delta_mdl(const SbpoBM *bm, int r, int s) {
     return dS;
 }
 
+/* The ranking score of a merge: its delta-MDL rounded to a multiple of 2^-20 (D4), so that values
+ * equal but for the rounding of their summation order compare equal on every implementation. */
+static double merge_score(double dS) { return nearbyint(dS * 1048576.0) / 1048576.0; }
+
 /* common::propose_new_block(block_merge = true) for block r with record x (D2 order). */
 static int propose_merge(const SbpoBM *bm, int r, const uint32_t x[4]) {
     int B = bm->B;
@@ -908,7 +912,7 @@ static int carry_out_advanced(SbpoBM *bm, const double *dS, const int *best) {
         Delta dl;
         merge_delta(&dl, bm, from, to);
         int prop_self = MAT(bm, to, to) + delta_get(&dl, to, to);
-        double actual = sbpo_merge_delta_mdl(bm, from, to);
+        double actual = merge_score(sbpo_merge_delta_mdl(bm, from, to));
         if (n > 0 && actual > heap[0].dS) {
             merge.dS = actual;
             h_push(heap, &n, merge);
@@ -959,7 +963,7 @@ int sbpo_merge_blocks(SbpoBM *bm, const SbpoGraph *g, int approximate, uint64_t 
             int s = propose_merge(bm, r, x);
             if (ms) ms->proposals++;
             if (past[s]) { if (ms) ms->avoided++; continue; }
-            double d = sbpo_merge_delta_mdl(bm, r, s);
+            double d = merge_score(sbpo_merge_delta_mdl(bm, r, s));
             past[s] = 1; pl[npl++] = s;
             if (d < dS[r]) { best[r] = s; dS[r] = d; }
         }
