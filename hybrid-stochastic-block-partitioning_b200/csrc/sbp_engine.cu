@@ -270,7 +270,7 @@ void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, in
   int* n_cur = bm.n_moved.p + (bm.gen & 1);
   const GibbsEvalKernel k_eval = gibbs_eval_kernel(bm.sparse);
   if (nl > 0) {
-    const bool small = use_small_kernel(bm);
+    const bool small = use_group_kernel(bm);
     const size_t smem = (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps;
     if (!small) set_smem_limit((const void*)k_eval, smem);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -280,9 +280,7 @@ void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, in
       SBP_CUDA(cudaEventRecord(e0, c.stream));
     }
     if (small) {
-      gibbs_eval_small_kernel()<<<grid_for(nl, kSmallThreads / kSmallGroup, 64 * c.num_sms), kSmallThreads, 0,
-                                  c.stream>>>(g.view(), bm.view(), plan.order.p + plan.light_begin[bt], nl, rng,
-                                              sweep, bm.prop.p, bm.moved.p, n_cur, c.counters, c.status, nullptr, 0);
+      launch_group_eval(g, bm, plan.order.p + plan.light_begin[bt], nl, rng, sweep, n_cur, nullptr, 0, c.stream);
     } else {
       k_eval<<<grid_for(nl, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem, c.stream>>>(
           g.view(), bm.view(), plan.order.p + plan.light_begin[bt], nl, rng, sweep, bm.prop.p, bm.moved.p, n_cur,
@@ -400,10 +398,8 @@ static int gibbs_sweeps_graph(SbpBlockmodel& bm, const SbpGraph& g, const BatchP
   for (int bt = 0; bt < nb; ++bt) {
     const int nl = plan.light_n[bt], nh = plan.heavy_n[bt];
     if (nl > 0) {
-      if (use_small_kernel(bm))
-        gibbs_eval_small_kernel()<<<grid_for(nl, kSmallThreads / kSmallGroup, 64 * c.num_sms), kSmallThreads, 0,
-                                    c.stream>>>(g.view(), bm.view(), plan.order.p + plan.light_begin[bt], nl, rng, 0,
-                                                bm.prop.p, bm.moved.p, nullptr, c.counters, c.status, g_ctl.p, bt);
+      if (use_group_kernel(bm))
+        launch_group_eval(g, bm, plan.order.p + plan.light_begin[bt], nl, rng, 0, nullptr, g_ctl.p, bt, c.stream);
       else
         k_eval<<<grid_for(nl, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem_light, c.stream>>>(
             g.view(), bm.view(), plan.order.p + plan.light_begin[bt], nl, rng, 0, bm.prop.p, bm.moved.p, nullptr,
@@ -1053,9 +1049,9 @@ SbpStatus sbp_set_option(const char* name, int64_t value) {
   } else if (n == "graph_sweeps") {
     SBP_REQUIRE(value == 0 || value == 1, "graph_sweeps must be 0 or 1");
     g_graph_sweeps = (int)value;
-  } else if (n == "small_b_kernel") {
-    SBP_REQUIRE(value == 0 || value == 1, "small_b_kernel must be 0 or 1");
-    g_small_b_kernel = (int)value;
+  } else if (n == "group_kernel") {
+    SBP_REQUIRE(value == 0 || value == 1, "group_kernel must be 0 or 1");
+    g_group_kernel = (int)value;
   } else if (n == "batched_wait_limit") {
     SBP_REQUIRE(value >= 16 && value <= (1LL << 30), "batched_wait_limit must be in [16, 2^30]");
     g_batched_wait_limit = value;

@@ -294,10 +294,9 @@ inline int g_hashed_row_factor = 4;
 // sweep loop decided on the GPU; 0: one host-driven launch sequence per sweep (sbp_set_option).
 inline int g_graph_sweeps = 1;
 inline long long g_overflow_rebuilds = 0;   // rebuilds forced by a full hashed row
-// 1: light vertices of dense blockmodels with B <= kSmallB are evaluated by the group kernel
-// (sbp_eval_small.cu); 0: by the warp-per-vertex kernel (sbp_set_option "small_b_kernel").
-inline int g_small_b_kernel = 1;
-inline bool use_small_kernel(const SbpBlockmodel& bm);
+// Light vertices of dense blockmodels: 1 evaluated by the group kernel (sbp_eval_small.cu), 0 by
+// the warp-per-vertex kernel (sbp_set_option "group_kernel").
+inline int g_group_kernel = 1;
 // Batched partitioner: idle claim attempts of a persistent CTA before the launch gives up with an
 // error (each attempt sleeps ~0.25 us), and the fault injection of the failure-detection test
 // (index of a graph whose sweep queue never opens; -1: none).  sbp_set_option.
@@ -498,7 +497,25 @@ struct SbpBlockmodel {
 
 namespace sbpb {
 
-inline bool use_small_kernel(const SbpBlockmodel& bm) { return g_small_b_kernel && !bm.sparse && bm.B <= kSmallB; }
+inline bool use_group_kernel(const SbpBlockmodel& bm) { return g_group_kernel && !bm.sparse; }
+
+// Launch of the group kernel over n light vertices (dense storage).
+inline void launch_group_eval(const SbpGraph& g, SbpBlockmodel& bm, const int* verts, int n, const RngParams& rng,
+                              int sweep, int* n_moved, const SweepCtl* ctl, int batch, cudaStream_t stream) {
+  Context& c = Context::get();
+  const bool hashed_table = bm.B > kSmallB;
+  const int cap = g.light_cap;
+  const size_t smem = gibbs_eval_group_smem(hashed_table, cap);
+  const GibbsEvalGroupKernel k = gibbs_eval_group_kernel(hashed_table);
+  static size_t set_for[2] = {0, 0};
+  if (set_for[hashed_table] < smem) {
+    SBP_CUDA(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    set_for[hashed_table] = smem;
+  }
+  k<<<grid_for(n, kSmallThreads / kSmallGroup, 64 * c.num_sms), kSmallThreads, smem, stream>>>(
+      g.view(), bm.view(), verts, n, rng, sweep, bm.prop.p, bm.moved.p, n_moved, c.counters, cap, c.status, ctl,
+      batch);
+}
 
 struct MhResult {
   long long visits = 0, moved = 0, accepted = 0;

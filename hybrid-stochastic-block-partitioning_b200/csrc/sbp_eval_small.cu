@@ -1,6 +1,5 @@
-// Asynchronous-Gibbs vertex evaluation for a dense block matrix with at most kSmallB blocks:
-// the regime of the last outer iterations of a partition, where the block count is near the
-// planted one (the same proposal, Hastings correction, delta-MDL and accept test as
+// Asynchronous-Gibbs evaluation of the light vertices of a batch on a dense block matrix, one
+// group of lanes per vertex (the same proposal, Hastings correction, delta-MDL and accept test as
 // evaluate_vertex in sbp_device.cuh; src/common.cpp:131-192, src/entropy.cpp:296-401, 495-557,
 // src/finetune.cpp:19-29).
 //
@@ -8,9 +7,12 @@
 //  * a group of G lanes evaluates one vertex, so a warp carries 32 / G vertices at a time; every
 //    loop runs to the largest trip count of the warp's groups (lanes past their own count are
 //    predicated off), so the group shuffles always see the whole warp converged;
-//  * the neighbour-block histogram of a vertex is a direct-indexed array of B words in shared
-//    memory (out count | in count << 15 | presence << 30) plus the list of blocks present: no
-//    hashing, one shared atomic per neighbour;
+//  * the neighbour-block histogram of a vertex is a per-group structure in shared memory: for
+//    B <= kSmallB a direct-indexed array of B words (out count | in count << 15 | presence << 30),
+//    above it an open-addressing table of twice the light-vertex degree bound; plus the list of
+//    entries present;
+//  * the multinomial walk finds the chunk through the chunk sums, four per lane per step, then
+//    the column inside it, sixteen counts per lane;
 //  * the frozen state of the batch (assignment, block matrix, degrees, log table) is read through
 //    the read-only data cache;
 //  * the FP64 terms of a changed cell are computed by the lane that loaded the cell.
@@ -48,15 +50,172 @@ __device__ __forceinline__ int warp_max_int(int v) {
   return v;
 }
 
+// Neighbour-block histogram of one group: direct-indexed by block (kHash false, B <= kSmallB) or
+// an open-addressing table of `mask + 1` slots (kHash true).  Slot words hold out count | in count
+// << 15 | presence << 30; the list holds the slots in use.
+template <bool kHash>
+struct GroupTable {
+  int* keys;        // kHash: block of each slot, -1 = empty
+  unsigned* w;      // counts per slot (per block when direct)
+  int* list;        // slots in use
+  int* n;           // their number
+  int mask;
+  int* status;
+  // slot of `key`, inserted if absent (*created set for the inserting lane)
+  __device__ __forceinline__ int insert(int key, bool* created) const {
+    *created = false;
+    if constexpr (!kHash) {
+      return key;
+    } else {
+      unsigned h = ((unsigned)key * 2654435761u) & (unsigned)mask;
+      for (int probe = 0; probe <= mask; ++probe) {
+        const int k = keys[h];
+        if (k == key) return (int)h;
+        if (k == -1) {
+          const int prev = atomicCAS(keys + h, -1, key);
+          if (prev == -1) {
+            *created = true;
+            return (int)h;
+          }
+          if (prev == key) return (int)h;
+        }
+        h = (h + 1) & (unsigned)mask;
+      }
+      atomicOr(status, kErrTableFull);
+      return -1;
+    }
+  }
+  __device__ __forceinline__ unsigned counts_of(int key) const {
+    if constexpr (!kHash) {
+      return w[key];
+    } else {
+      unsigned h = ((unsigned)key * 2654435761u) & (unsigned)mask;
+      for (int probe = 0; probe <= mask; ++probe) {
+        const int k = keys[h];
+        if (k == key) return w[h];
+        if (k == -1) return 0u;
+        h = (h + 1) & (unsigned)mask;
+      }
+      return 0u;
+    }
+  }
+  __device__ __forceinline__ void add(int key, unsigned delta) const {
+    bool created;
+    const int slot = insert(key, &created);
+    if (slot < 0) return;
+    const unsigned old = delta == kPresent ? atomicOr(w + slot, kPresent) : atomicAdd(w + slot, delta);
+    if (kHash ? created : old == 0u) list[atomicAdd(n, 1)] = slot;
+  }
+  __device__ __forceinline__ int key_of(int slot) const { return kHash ? keys[slot] : slot; }
+  __device__ __forceinline__ void clear(int slot) const {
+    w[slot] = 0u;
+    if constexpr (kHash) keys[slot] = -1;
+  }
+};
+
+// The multinomial walk of evaluate_vertex over a dense row (or column) of M: the first column
+// whose running count exceeds tg.  Chunk sums (kChunk columns each) locate the chunk, four per
+// lane per step; the chunk's counts are then scanned sixteen per lane.  Every lane of the warp
+// takes part (loop bounds are warp-uniform); groups with walk == false get -1.
 template <int G>
+__device__ __forceinline__ int group_walk(const int* row, const int* csum, int nch, long long tg, bool walk, int gl,
+                                          int gbase) {
+  const unsigned gmask = (G == 32 ? kFull : ((1u << G) - 1u) << gbase);
+  int chunk = 0;
+  long long before = 0;   // counts of the row before the chosen chunk
+  if (nch > 1) {
+    bool found = !walk;
+    chunk = -1;
+    long long acc = 0;
+    for (int c0 = 0; c0 < nch; c0 += 4 * G) {
+      int cs[4];
+      long long lsum = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int c = c0 + gl * 4 + q;
+        cs[q] = (walk && c < nch) ? __ldg(csum + c) : 0;
+        lsum += cs[q];
+      }
+      long long incl = lsum;
+#pragma unroll
+      for (int o = 1; o < G; o <<= 1) {
+        const long long y = __shfl_up_sync(kFull, incl, o, G);
+        if (gl >= o) incl += y;
+      }
+      const long long tot = __shfl_sync(kFull, incl, G - 1, G);
+      const unsigned hit = __ballot_sync(kFull, !found && acc + incl > tg) & gmask;
+      int pick = -1;
+      long long pb = 0;
+      if (hit && gl == __ffs(hit) - 1 - gbase) {
+        long long run = acc + incl - lsum;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (pick < 0) {
+            if (tg < run + cs[q]) {
+              pick = c0 + gl * 4 + q;
+              pb = run;
+            } else {
+              run += cs[q];
+            }
+          }
+        }
+      }
+      const int src = hit ? __ffs(hit) - 1 - gbase : 0;
+      const int pk = __shfl_sync(kFull, pick, src, G);
+      const long long pbb = __shfl_sync(kFull, pb, src, G);
+      if (hit && !found) {
+        chunk = pk;
+        before = pbb;
+        found = true;
+      }
+      acc += tot;
+    }
+    if (walk && chunk < 0) walk = false;
+  }
+  constexpr int kPer = kChunk / G;   // counts per lane
+  const int* base = row + (size_t)(chunk < 0 ? 0 : chunk) * kChunk + gl * kPer;
+  int vals[kPer];
+  long long lsum = 0;
+#pragma unroll
+  for (int q = 0; q < kPer / 4; ++q) {
+    const int4 c4 = __ldg(reinterpret_cast<const int4*>(base) + q);
+    vals[4 * q] = c4.x;
+    vals[4 * q + 1] = c4.y;
+    vals[4 * q + 2] = c4.z;
+    vals[4 * q + 3] = c4.w;
+    lsum += (long long)c4.x + c4.y + c4.z + c4.w;
+  }
+  long long incl = lsum;
+#pragma unroll
+  for (int o = 1; o < G; o <<= 1) {
+    const long long y = __shfl_up_sync(kFull, incl, o, G);
+    if (gl >= o) incl += y;
+  }
+  const long long t2 = tg - before;
+  const unsigned hit = __ballot_sync(kFull, walk && incl > t2) & gmask;
+  int col = -1;
+  if (walk && hit && gl == __ffs(hit) - 1 - gbase) {
+    long long rem = t2 - (incl - lsum);
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+      if (col < 0) {
+        if (rem < vals[q]) col = (chunk < 0 ? 0 : chunk) * kChunk + gl * kPer + q;
+        else rem -= vals[q];
+      }
+    }
+  }
+  const int found = __shfl_sync(kFull, col, hit ? __ffs(hit) - 1 - gbase : 0, G);
+  return walk ? found : -1;
+}
+
+template <int G, bool kHash>
 __global__ void __launch_bounds__(kSmallThreads)
-    k_gibbs_eval_small(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
-                       int* prop, int* moved_list, int* n_moved, unsigned long long* counters, int* status,
+    k_gibbs_eval_group(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
+                       int* prop, int* moved_list, int* n_moved, unsigned long long* counters, int cap, int* status,
                        const SweepCtl* ctl, int batch) {
   constexpr int kGroups = kSmallThreads / G;
-  __shared__ unsigned s_w[kGroups][kSmallB];
-  __shared__ int s_list[kGroups][kSmallB];
-  __shared__ int s_n[kGroups];
+  extern __shared__ int group_smem[];
+  const int slots = kHash ? cap : kSmallB;
   if (ctl) {
     sweep = ctl->sweep;
     n_moved = ctl->n_moved + ((ctl->gen0 + (unsigned)batch) & 1u);
@@ -65,13 +224,22 @@ __global__ void __launch_bounds__(kSmallThreads)
   const int gl = lane & (G - 1);
   const int gid = threadIdx.x / G;
   const int gbase = lane & ~(G - 1);   // first lane of this group in the warp
-  unsigned* W = s_w[gid];
-  int* L = s_list[gid];
+  int* mine = group_smem + kGroups + (size_t)gid * (kHash ? 3 : 2) * slots;
+  GroupTable<kHash> T;
+  T.w = reinterpret_cast<unsigned*>(mine);
+  T.list = mine + slots;
+  T.keys = kHash ? mine + 2 * slots : nullptr;
+  T.n = group_smem + gid;
+  T.mask = slots - 1;
+  T.status = status;
+  for (int i = gl; i < slots; i += G) {
+    T.w[i] = 0u;
+    if constexpr (kHash) T.keys[i] = -1;
+  }
+  if (gl == 0) *T.n = 0;
+  __syncwarp();
   const int B = bm.B;
   const int ld = bm.ld;
-  for (int i = gl; i < kSmallB; i += G) W[i] = 0u;
-  if (gl == 0) s_n[gid] = 0;
-  __syncwarp();
   unsigned long long c_visit = 0, c_moved = 0, c_acc = 0;
   const bool given = rng.moves != 0;
   const int groups_total = gridDim.x * kGroups;
@@ -104,19 +272,13 @@ __global__ void __launch_bounds__(kSmallThreads)
         const bool out = e < k_out;
         const int u = out ? __ldg(g.out_idx + o0 + e) : __ldg(g.in_idx + i0 + (e - k_out));
         bu = __ldg(bm.b + u);
-        if (!(out && u == v)) {   // the self loop is not counted (its block enters as present)
-          const unsigned old = atomicAdd(W + bu, out ? 1u : (1u << kInShift));
-          if (old == 0u) L[atomicAdd(&s_n[gid], 1)] = bu;
-        }
+        if (!(out && u == v)) T.add(bu, out ? 1u : (1u << kInShift));   // the self loop only marks r present
       }
       const int src = idx - it * G;
       const int pick = __shfl_sync(kFull, bu, (src >= 0 && src < G) ? src : 0, G);
       if (src >= 0 && src < G) tblk = pick;
     }
-    if (valid && self && gl == 0) {
-      const unsigned old = atomicOr(W + r, kPresent);
-      if (old == 0u) L[atomicAdd(&s_n[gid], 1)] = r;
-    }
+    if (valid && self && gl == 0) T.add(r, kPresent);
     __syncwarp();
     // 2. the proposal: the multinomial over row t of M then column t (ascending), as the
     //    dense walks of evaluate_vertex
@@ -133,38 +295,8 @@ __global__ void __launch_bounds__(kSmallThreads)
         tg = in_row ? target : target - dot;
       }
       const int* row = (in_row ? bm.M : bm.MT) + (size_t)t * ld;
-      constexpr int kPer = kSmallB / G;   // counts per lane
-      int vals[kPer];
-      long long lsum = 0;
-#pragma unroll
-      for (int q = 0; q < kPer / 4; ++q) {
-        const int4 c4 = __ldg(reinterpret_cast<const int4*>(row + gl * kPer) + q);
-        vals[4 * q] = c4.x;
-        vals[4 * q + 1] = c4.y;
-        vals[4 * q + 2] = c4.z;
-        vals[4 * q + 3] = c4.w;
-        lsum += (long long)c4.x + c4.y + c4.z + c4.w;
-      }
-      long long incl = lsum;
-#pragma unroll
-      for (int o = 1; o < G; o <<= 1) {
-        const long long y = __shfl_up_sync(kFull, incl, o, G);
-        if (gl >= o) incl += y;
-      }
-      const unsigned gmask = (G == 32 ? kFull : ((1u << G) - 1u) << gbase);
-      const unsigned hit = __ballot_sync(kFull, walk && incl > tg) & gmask;
-      int col = -1;
-      if (walk && hit && gl == __ffs(hit) - 1 - gbase) {
-        long long rem = tg - (incl - lsum);
-#pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-          if (col < 0) {
-            if (rem < vals[q]) col = gl * kPer + q;
-            else rem -= vals[q];
-          }
-        }
-      }
-      const int found = __shfl_sync(kFull, col, hit ? __ffs(hit) - 1 - gbase : 0, G);
+      const int* csum = (in_row ? bm.CS : bm.CST) + (size_t)t * bm.nch;
+      const int found = group_walk<G>(row, csum, bm.nch, tg, walk, gl, gbase);
       if (walk) {
         s = found;
         if (s < 0 || s >= B) {
@@ -184,11 +316,11 @@ __global__ void __launch_bounds__(kSmallThreads)
     const bool active = valid && s != r;
     // 3. delta-MDL and the Hastings correction of the move r -> s
     double fwd = 0.0, bwd = 0.0, dS = 0.0;
-    long long T = 0;
+    long long Tz = 0;
     int co_r = 0, ci_r = 0, co_s = 0, ci_s = 0;
     int M_rr = 0, M_rs = 0, M_sr = 0, M_ss = 0, dout_r = 0, dout_s = 0, din_r = 0, din_s = 0;
     if (active) {
-      const unsigned wr = W[r], ws = W[s];
+      const unsigned wr = T.counts_of(r), ws = T.counts_of(s);
       co_r = wr & kCountMask;
       ci_r = (wr >> kInShift) & kCountMask;
       co_s = ws & kCountMask;
@@ -207,13 +339,14 @@ __global__ void __launch_bounds__(kSmallThreads)
     const int d_sr = co_r - ci_s;
     const int d_ss = co_s + ci_s + self;
     const int kin_self = k_in + self;
-    const int nent = active ? s_n[gid] : 0;
+    const int nent = active ? *T.n : 0;
     const int ent_iters = warp_max_int((nent + G - 1) / G);
     for (int it = 0; it < ent_iters; ++it) {
       const int j = it * G + gl;
       if (j < nent) {
-        const int u = L[j];
-        const unsigned wu = W[u];
+        const int slot = T.list[j];
+        const int u = T.key_of(slot);
+        const unsigned wu = T.w[slot];
         const int co = wu & kCountMask, ci = (wu >> kInShift) & kCountMask;
         const int M_ru = __ldg(bm.M + (size_t)r * ld + u);
         const int M_ur = __ldg(bm.MT + (size_t)r * ld + u);
@@ -232,11 +365,11 @@ __global__ void __launch_bounds__(kSmallThreads)
         if (!is_r && !is_s) {   // cells (r,u) (s,u) for out-edges to u, (u,r) (u,s) for in-edges
           if (co) {
             dS += dxlogx_int(bm.logt, M_ru, M_ru - co) + dxlogx_int(bm.logt, M_su, M_su + co);
-            T += 2LL * (M_ru + M_su);
+            Tz += 2LL * (M_ru + M_su);
           }
           if (ci) {
             dS += dxlogx_int(bm.logt, M_ur, M_ur - ci) + dxlogx_int(bm.logt, M_us, M_us + ci);
-            T += 2LL * (M_ur + M_us);
+            Tz += 2LL * (M_ur + M_us);
           }
         }
       }
@@ -249,7 +382,7 @@ __global__ void __launch_bounds__(kSmallThreads)
         const int d = q == 0 ? d_rr : q == 1 ? d_rs : q == 2 ? d_sr : q == 3 ? d_ss
                     : q == 4 ? -k_out : q == 5 ? k_out : q == 6 ? -kin_self : kin_self;
         if (d) dS += (q < 4 ? 1.0 : -1.0) * dxlogx_int(bm.logt, a, a + d);
-        T += q < 4 ? (d ? 2LL * a + d : 0LL) : 2LL * a;
+        Tz += q < 4 ? (d ? 2LL * a + d : 0LL) : 2LL * a;
       }
       // the double count of a present net-zero (r,s) / (s,r) Delta cell
       if (gl == 0 && (co_s > 0 || ci_r > 0) && d_rs == 0 && M_rs > 0)
@@ -260,9 +393,9 @@ __global__ void __launch_bounds__(kSmallThreads)
     fwd = group_sum<G>(fwd);
     bwd = group_sum<G>(bwd);
     dS = group_sum<G>(dS);
-    T = group_sum_ll<G>(T);
+    Tz = group_sum_ll<G>(Tz);
     if (active) {
-      if (fabs(dS) <= 0x1p-40 * (double)T * g.log_E) dS = 0.0;
+      if (fabs(dS) <= 0x1p-40 * (double)Tz * g.log_E) dS = 0.0;
       const double H = (k == 0) ? 1.0 : bwd / fwd;
       double ap = exp(-3.0 * dS) * H;
       ap = ap >= 1.0 ? 1.0 : ap;
@@ -279,10 +412,10 @@ __global__ void __launch_bounds__(kSmallThreads)
     }
     // 4. clear the histogram of the group's vertex
     __syncwarp();
-    const int nclear = valid ? s_n[gid] : 0;
-    for (int j = gl; j < nclear; j += G) W[L[j]] = 0u;
+    const int nclear = valid ? *T.n : 0;
+    for (int j = gl; j < nclear; j += G) T.clear(T.list[j]);
     __syncwarp();
-    if (gl == 0) s_n[gid] = 0;
+    if (gl == 0) *T.n = 0;
     __syncwarp();
   }
   c_visit = warp_sum_ull(c_visit);
@@ -297,6 +430,14 @@ __global__ void __launch_bounds__(kSmallThreads)
 
 }  // namespace
 
-GibbsEvalSmallKernel gibbs_eval_small_kernel() { return k_gibbs_eval_small<kSmallGroup>; }
+GibbsEvalGroupKernel gibbs_eval_group_kernel(bool hashed_table) {
+  return hashed_table ? k_gibbs_eval_group<kSmallGroup, true> : k_gibbs_eval_group<kSmallGroup, false>;
+}
+
+size_t gibbs_eval_group_smem(bool hashed_table, int cap) {
+  const int groups = kSmallThreads / kSmallGroup;
+  const int slots = hashed_table ? cap : kSmallB;
+  return sizeof(int) * ((size_t)groups + (size_t)groups * (hashed_table ? 3 : 2) * slots);
+}
 
 }  // namespace sbpb

@@ -51,14 +51,17 @@ __global__ void __launch_bounds__(256, 2)
 using GibbsEvalKernel = void (*)(GraphView, BlockView, const int* __restrict__, int, RngParams, int, int*, int*, int*,
                                  unsigned long long*, int, int*, const SweepCtl*, int);
 inline GibbsEvalKernel gibbs_eval_kernel(bool hashed) { return hashed ? k_gibbs_eval_hashed : k_gibbs_eval_dense; }
-// Asynchronous-Gibbs evaluation for dense storage with B <= kSmallB (sbp_eval_small.cu): groups of
-// kSmallGroup lanes per vertex, direct-indexed neighbour-block histograms in shared memory.
+// Asynchronous-Gibbs evaluation of light vertices on dense storage (sbp_eval_small.cu): groups of
+// kSmallGroup lanes per vertex; neighbour-block histograms direct-indexed (B <= kSmallB) or in
+// per-group hash tables of `cap` slots (hashed_table), in dynamic shared memory of
+// gibbs_eval_group_smem bytes.
 constexpr int kSmallB = 128;
 constexpr int kSmallThreads = 256;
 constexpr int kSmallGroup = 8;
-using GibbsEvalSmallKernel = void (*)(GraphView, BlockView, const int* __restrict__, int, RngParams, int, int*, int*,
-                                      int*, unsigned long long*, int*, const SweepCtl*, int);
-GibbsEvalSmallKernel gibbs_eval_small_kernel();
+using GibbsEvalGroupKernel = void (*)(GraphView, BlockView, const int* __restrict__, int, RngParams, int, int*, int*,
+                                      int*, unsigned long long*, int, int*, const SweepCtl*, int);
+GibbsEvalGroupKernel gibbs_eval_group_kernel(bool hashed_table);
+size_t gibbs_eval_group_smem(bool hashed_table, int cap);
 __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, const int* n_moved, const int* prop,
                               int* qr, int* qs, unsigned long long* last, unsigned gen, const SweepCtl* ctl, int batch);
 __global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved, int* prop,

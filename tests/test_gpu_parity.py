@@ -302,23 +302,23 @@ def test_graph_run_sweeps_equal_host_driven_sweeps(S, O, batches, seed):
     assert s1["sweeps"] == ost["sweeps"]
 
 
-@pytest.mark.parametrize("B,seed", [(7, 1), (64, 2), (128, 3)])
+@pytest.mark.parametrize("B,seed", [(7, 1), (64, 2), (128, 3), (129, 4), (700, 5), (2500, 6)])
 def test_group_kernel_equals_warp_kernel(S, O, B, seed):
-    """The small-B evaluation kernel (groups of lanes per vertex, direct-indexed histograms) and
-    the warp-per-vertex kernel give the same chain: same proposals, accept decisions and state,
-    and both equal the oracle."""
+    """The group evaluation kernel (groups of lanes per vertex; direct-indexed histograms up to
+    128 blocks, per-group hash tables and a chunked walk above) and the warp-per-vertex kernel
+    give the same chain: same proposals, accept decisions and state, and both equal the oracle."""
     V, s, d, _ = random_graph(4000, 10, 90 + seed, kmin=4, kmax=60)
     a = random_assignment(V, B, seed)
     g = S.Graph(V, s, d)
     states = []
     for small in (1, 0):
-        S.set_option("small_b_kernel", small)
+        S.set_option("group_kernel", small)
         try:
             bm = S.Blockmodel(g, B, a)
             st = S.finetune.asynchronous_gibbs(bm, batches=5, seed=seed, call=3, max_sweeps=4)
             states.append((bm, st))
         finally:
-            S.set_option("small_b_kernel", 1)
+            S.set_option("group_kernel", 1)
     (b1, s1), (b2, s2) = states
     assert np.array_equal(b1.block_assignment(), b2.block_assignment())
     assert np.array_equal(b1.blockmatrix(), b2.blockmatrix())
