@@ -80,11 +80,42 @@ static void rebuild_hashed_side(SbpBlockmodel& bm, long long E, unsigned long lo
   SBP_CHECK_LAUNCH();
 }
 
-// Sparse Blockmodel::initialize_edge_counts: rows of M and MT from sorted (b_src, b_dst) keys.
-static void rebuild_sparse(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_d) {
+// Compressed rows of M (or of MT, keys of the transposed edges) from the sorted (b_src, b_dst)
+// keys of the edges, ascending by column: the merge step's outgoing / incoming edge views of a
+// dense blockmodel too large to scan cell by cell.
+static void sorted_rows(const SbpBlockmodel& bm, long long E, unsigned long long* keys, DevBuf<int>& cptr,
+                        DevBuf<int>& cidx, DevBuf<int>& cval) {
   Context& c = Context::get();
-  const long long E = g.E;
   const int B = bm.B;
+  long long nu = 0;
+  if (E > 0) {
+    unsigned long long* sorted = keys;
+    radix_sort_u64(keys, g_sort.tmp.p, E, key_bits(B), g_sort.hist.p, g_sort.partial.p, c.num_sms, c.stream, &sorted);
+    rle(sorted, E, g_sort.flags.p, g_sort.pos.p, g_sort.ukeys.p, g_sort.heads.p, g_sort.partial.p, c.num_sms, c.stream);
+    long long lastpos = 0;
+    unsigned lastflag = 0;
+    SBP_CUDA(SBP_COPY_ASYNC(&lastpos, g_sort.pos.p + E - 1, sizeof(long long), cudaMemcpyDeviceToHost, c.stream));
+    SBP_CUDA(SBP_COPY_ASYNC(&lastflag, g_sort.flags.p + E - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream));
+    SBP_CHECK_LAUNCH();
+    c.sync();
+    nu = lastpos + lastflag;
+  }
+  SBP_CUDA(cudaMemsetAsync(g_sort.rowcnt.p, 0, B * sizeof(unsigned), c.stream));
+  if (nu > 0) {
+    k_unique_rows<<<grid_for(nu, 256, 8 * c.num_sms), 256, 0, c.stream>>>(g_sort.ukeys.p, nu, B, g_sort.rowcnt.p);
+    SBP_CHECK_LAUNCH();
+  }
+  exclusive_scan_u32(g_sort.rowcnt.p, g_sort.rowptr.p, B, g_sort.partial.p, c.num_sms, c.stream);
+  cptr.reserve(B + 1);
+  cidx.reserve(std::max(nu, 1LL));
+  cval.reserve(std::max(nu, 1LL));
+  k_fill_csr<<<grid_for(B, 128, 16 * c.num_sms), 128, 0, c.stream>>>(g_sort.rowptr.p, g_sort.ukeys.p, g_sort.heads.p,
+                                                                    nu, E, B, cptr.p, cidx.p, cval.p);
+  SBP_CHECK_LAUNCH();
+}
+
+static void reserve_sort_scratch(long long E, int B) {
+  Context& c = Context::get();
   g_sort.keys.reserve(std::max(E, 1LL));
   g_sort.keysT.reserve(std::max(E, 1LL));
   g_sort.tmp.reserve(std::max(E, 1LL));
@@ -97,6 +128,14 @@ static void rebuild_sparse(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_
   g_sort.rowcnt.reserve(B);
   g_sort.caps.reserve(B);
   g_sort.rowptr.reserve(B);
+}
+
+// Sparse Blockmodel::initialize_edge_counts: rows of M and MT from sorted (b_src, b_dst) keys.
+static void rebuild_sparse(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_d) {
+  Context& c = Context::get();
+  const long long E = g.E;
+  const int B = bm.B;
+  reserve_sort_scratch(E, B);
   SBP_CUDA(cudaMemsetAsync(bm.d_out.p, 0, B * sizeof(int), c.stream));
   SBP_CUDA(cudaMemsetAsync(bm.d_in.p, 0, B * sizeof(int), c.stream));
   SBP_CUDA(cudaMemsetAsync(bm.overflow.p, 0, (1 + 2 * (size_t)B) * sizeof(int), c.stream));
@@ -660,6 +699,17 @@ void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& opt, co
     rebuild(bm, g, true);
     rows = Csr{bm.csr_rptr.p, bm.csr_ridx.p, bm.csr_rval.p};
     cols = Csr{bm.csr_cptr.p, bm.csr_cidx.p, bm.csr_cval.p};
+  } else if ((long long)B * bm.ld > 8LL * g.E) {
+    // compressed rows from the sorted edge keys: fewer bytes than scanning B x ld cells twice
+    reserve_sort_scratch(g.E, B);
+    if (g.E > 0)
+      k_edge_keys<<<grid_for(g.E, 256, 16 * c.num_sms), 256, 0, c.stream>>>(g.view(), bm.b.p, g.out_src.p, B,
+                                                                            g_sort.keys.p, g_sort.keysT.p);
+    SBP_CHECK_LAUNCH();
+    sorted_rows(bm, g.E, g_sort.keys.p, ms.rptr, ms.ridx, ms.rval);
+    sorted_rows(bm, g.E, g_sort.keysT.p, ms.cptr, ms.cidx, ms.cval);
+    rows = Csr{ms.rptr.p, ms.ridx.p, ms.rval.p};
+    cols = Csr{ms.cptr.p, ms.cidx.p, ms.cval.p};
   } else {
   // compressed rows of M and of MT (outgoing_edges / incoming_edges views)
   ms.rcnt.reserve(B);

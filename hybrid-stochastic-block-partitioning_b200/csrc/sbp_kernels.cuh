@@ -94,6 +94,9 @@ __global__ void k_fill_rows(const long long* __restrict__ rowptr, const unsigned
                             const long long* __restrict__ base, const int* __restrict__ mask, int2* slot,
                             int* csr_ptr, int* csr_idx, int* csr_val);
 __global__ void k_block_degrees(GraphView g, const int* __restrict__ b, int* d_out, int* d_in);
+__global__ void k_fill_csr(const long long* __restrict__ rowptr, const unsigned long long* __restrict__ ukeys,
+                           const long long* __restrict__ heads, long long nu, long long nedges, int B, int* csr_ptr,
+                           int* csr_idx, int* csr_val);
 __global__ void k_recover_assign(int* b, const int* moved, const int* n_moved, const int* prop, int* old_block);
 __global__ void k_regrow_alloc(const int* __restrict__ full, const int* __restrict__ deg, int B, long long top,
                                long long limit, unsigned long long* used, unsigned long long* nrows, long long* base,

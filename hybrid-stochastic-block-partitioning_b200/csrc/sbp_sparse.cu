@@ -65,6 +65,22 @@ __global__ void k_fill_rows(const long long* __restrict__ rowptr, const unsigned
   }
 }
 
+// Compressed rows only (no hashed slots): the merge step of a large dense blockmodel, whose B x B
+// matrix is too large to scan for its non-zero cells.
+__global__ void k_fill_csr(const long long* __restrict__ rowptr, const unsigned long long* __restrict__ ukeys,
+                           const long long* __restrict__ heads, long long nu, long long nedges, int B, int* csr_ptr,
+                           int* csr_idx, int* csr_val) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < B; r += gridDim.x * blockDim.x) {
+    const long long j0 = rowptr[r], j1 = (r + 1 < B) ? rowptr[r + 1] : nu;
+    csr_ptr[r] = (int)j0;
+    if (r == B - 1) csr_ptr[B] = (int)nu;
+    for (long long j = j0; j < j1; ++j) {
+      csr_idx[j] = (int)(ukeys[j] % (unsigned long long)B);
+      csr_val[j] = (int)(((j + 1 < nu) ? heads[j + 1] : nedges) - heads[j]);
+    }
+  }
+}
+
 // Regrowth of the hashed rows that ran out of room (one side: rows of M or of MT).  A flagged
 // row x gets a region of the power of two at least twice its old room and at least
 // 2 min(deg[x], B) + 16 slots, taken after the `top` slots in use; with no room left below
