@@ -272,6 +272,26 @@ MhResult mh_pass(SbpBlockmodel& bm, const SbpGraph& g, const int* verts, int n, 
   Context& c = Context::get();
   MhResult res;
   if (n == 0) return res;
+  if (g_group_kernel && !bm.sparse && 2 * max_k <= g.light_cap) {
+    // rounds of one vertex per lane group (every vertex of the list fits the group tables)
+    const bool hashed_table = bm.B > kSmallB;
+    const int cap = g.light_cap;
+    const size_t smem = mh_group_smem(hashed_table, cap);
+    if (smem <= kSmemBudget) {
+      const MhGroupKernel k = mh_group_kernel(hashed_table);
+      set_smem_limit((const void*)k, smem);
+      k<<<1, kMhGroupThreads, smem, c.stream>>>(g.view(), bm.view(), verts, n, rng, sweep, cap, c.mh_out, c.status);
+      SBP_CHECK_LAUNCH();
+      double out[4];
+      SBP_CUDA(SBP_COPY_ASYNC(out, c.mh_out, sizeof(out), cudaMemcpyDeviceToHost, c.stream));
+      c.sync();
+      res.visits = (long long)out[0];
+      res.moved = (long long)out[1];
+      res.accepted = (long long)out[2];
+      res.sum_dS = out[3];
+      return res;
+    }
+  }
   const int cap = mh_cap(max_k);
   const size_t per_warp = (size_t)table_ints(cap) * sizeof(int);
   int W = (int)std::min<size_t>(16, kSmemBudget / per_warp);

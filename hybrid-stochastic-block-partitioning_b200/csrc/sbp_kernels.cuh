@@ -62,6 +62,11 @@ using GibbsEvalGroupKernel = void (*)(GraphView, BlockView, const int* __restric
                                       int*, unsigned long long*, int, int*, const SweepCtl*, int);
 GibbsEvalGroupKernel gibbs_eval_group_kernel(bool hashed_table);
 size_t gibbs_eval_group_smem(bool hashed_table, int cap);
+// Metropolis-Hastings rounds of kMhGroupThreads / kSmallGroup vertices (one CTA, dense storage).
+constexpr int kMhGroupThreads = 512;
+using MhGroupKernel = void (*)(GraphView, BlockView, const int* __restrict__, int, RngParams, int, int, double*, int*);
+MhGroupKernel mh_group_kernel(bool hashed_table);
+size_t mh_group_smem(bool hashed_table, int cap);
 __global__ void k_apply_edges(GraphView g, BlockView bm, const int* moved_list, const int* n_moved, const int* prop,
                               int* qr, int* qs, unsigned long long* last, unsigned gen, const SweepCtl* ctl, int batch);
 __global__ void k_apply_finish(BlockView bm, const int* moved_list, const int* n_moved, int* next_n_moved, int* prop,

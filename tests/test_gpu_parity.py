@@ -302,11 +302,13 @@ def test_graph_run_sweeps_equal_host_driven_sweeps(S, O, batches, seed):
     assert s1["sweeps"] == ost["sweeps"]
 
 
+@pytest.mark.parametrize("algo", [0, 1, 2])
 @pytest.mark.parametrize("B,seed", [(7, 1), (64, 2), (128, 3), (129, 4), (700, 5), (2500, 6)])
-def test_group_kernel_equals_warp_kernel(S, O, B, seed):
-    """The group evaluation kernel (groups of lanes per vertex; direct-indexed histograms up to
-    128 blocks, per-group hash tables and a chunked walk above) and the warp-per-vertex kernel
-    give the same chain: same proposals, accept decisions and state, and both equal the oracle."""
+def test_group_kernel_equals_warp_kernel(S, O, B, seed, algo):
+    """The group kernels (groups of lanes per vertex; direct-indexed histograms up to 128 blocks,
+    per-group hash tables and a chunked walk above; asynchronous-Gibbs batches and the
+    Metropolis-Hastings rounds, hybrid using both) and the warp-per-vertex kernels give the same
+    chain: same proposals, accept decisions and state, and both equal the oracle."""
     V, s, d, _ = random_graph(4000, 10, 90 + seed, kmin=4, kmax=60)
     a = random_assignment(V, B, seed)
     g = S.Graph(V, s, d)
@@ -315,7 +317,7 @@ def test_group_kernel_equals_warp_kernel(S, O, B, seed):
         S.set_option("group_kernel", small)
         try:
             bm = S.Blockmodel(g, B, a)
-            st = S.finetune.asynchronous_gibbs(bm, batches=5, seed=seed, call=3, max_sweeps=4)
+            st = S.finetune.run(bm, algo, batches=5, seed=seed, call=3, max_sweeps=4)
             states.append((bm, st))
         finally:
             S.set_option("group_kernel", 1)
@@ -324,5 +326,5 @@ def test_group_kernel_equals_warp_kernel(S, O, B, seed):
     assert np.array_equal(b1.blockmatrix(), b2.blockmatrix())
     assert s1["accepted"] == s2["accepted"] and s1["visits"] == s2["visits"]
     obm = O.Blockmodel(O.Graph(V, s, d), B, a)
-    obm.finetune(O.GIBBS, batches=5, seed=seed, call=3, max_sweeps=4)
+    obm.finetune(algo, batches=5, seed=seed, call=3, max_sweeps=4)
     assert_same_state(b1, obm)
