@@ -1119,6 +1119,9 @@ SbpStatus sbp_set_option(const char* name, int64_t value) {
   } else if (n == "graph_sweeps") {
     SBP_REQUIRE(value == 0 || value == 1, "graph_sweeps must be 0 or 1");
     g_graph_sweeps = (int)value;
+  } else if (n == "dense_max_memory_pct") {
+    SBP_REQUIRE(value >= 1 && value <= 90, "dense_max_memory_pct must be in [1, 90]");
+    g_dense_max_memory_pct = (int)value;
   } else if (n == "group_kernel") {
     SBP_REQUIRE(value == 0 || value == 1, "group_kernel must be 0 or 1");
     g_group_kernel = (int)value;

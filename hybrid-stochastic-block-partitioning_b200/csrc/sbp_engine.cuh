@@ -286,8 +286,10 @@ constexpr int kMaxCap = 8192;         // largest per-warp table
 constexpr size_t kSmemBudget = 200 * 1024;
 constexpr int kSmemRebuildMaxB = 100;
 
-// Blocks above which the block matrix is row-hashed instead of dense (sbp_set_option).
+// Blocks above which the block matrix is row-hashed instead of dense, and the largest share of the
+// free device memory (percent) a dense matrix may take (sbp_set_option).
 inline int g_dense_max_blocks = 65536;
+inline int g_dense_max_memory_pct = 40;
 // Hashed row capacity = power of two >= factor * (cells after a rebuild) + 4 * factor.
 inline int g_hashed_row_factor = 4;
 // 1: an asynchronous-Gibbs finetune on dense storage runs as one CUDA graph launch with the
@@ -467,7 +469,7 @@ struct SbpBlockmodel {
       size_t free_b = 0, total_b = 0;
       if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
         const size_t have = M.n * sizeof(int) * 2;   // a buffer this blockmodel already holds counts as free
-        if (dense_bytes > 0.4 * (double)(free_b + have)) sparse = true;
+        if (dense_bytes > 0.01 * g_dense_max_memory_pct * (double)(free_b + have)) sparse = true;
       } else {
         cudaGetLastError();
       }
