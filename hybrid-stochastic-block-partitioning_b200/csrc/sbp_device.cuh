@@ -670,13 +670,14 @@ __device__ __forceinline__ double move_delta(const GraphView& g, const BlockView
       M_us = bm_getT<ST>(bm, s, u);
       const bool is_r = (u == r), is_s = (u == s), corner = is_r || is_s;
       const double c = (double)(co + ci + (is_r ? self : 0));
-      fwd += c * (M_su + M_us + 1.0) / ((double)du + (double)B);
+      const double inv_u = 1.0 / ((double)du + (double)B);   // a non-corner block's degree is unchanged
+      fwd += c * (M_su + M_us + 1.0) * inv_u;
       const double bw = is_r ? (double)(M_rr + d_rr) + (double)(M_rr + d_rr) + 1.0
                       : is_s ? (double)(M_rs + d_rs) + (double)(M_sr + d_sr) + 1.0
                              : (double)(M_ru - co) + (double)(M_ur - ci) + 1.0;
       const int nd = is_r ? (dout_r - k_out) + (din_r - k_in) - (M_rr + d_rr)
                    : is_s ? (dout_s + k_out) + (din_s + k_in) - (M_ss + d_ss) : du;
-      bwd += c * bw / ((double)nd + (double)B);
+      bwd += c * bw * (corner ? 1.0 / ((double)nd + (double)B) : inv_u);
       // changed non-corner cells (r,u) (s,u) (u,r) (u,s); corner cells are terms 0-3 below
       co_c = corner ? 0 : co;
       ci_c = corner ? 0 : ci;

@@ -272,7 +272,7 @@ MhResult mh_pass(SbpBlockmodel& bm, const SbpGraph& g, const int* verts, int n, 
   Context& c = Context::get();
   MhResult res;
   if (n == 0) return res;
-  if (g_group_kernel && !bm.sparse && 2 * max_k <= g.light_cap) {
+  if (use_group_kernel(bm) && (bm.B <= kSmallB || 2 * max_k <= g.light_cap)) {
     // rounds of one vertex per lane group (every vertex of the list fits the group tables)
     const bool hashed_table = bm.B > kSmallB;
     const int cap = g.light_cap;
@@ -1123,7 +1123,7 @@ SbpStatus sbp_set_option(const char* name, int64_t value) {
     SBP_REQUIRE(value >= 1 && value <= 90, "dense_max_memory_pct must be in [1, 90]");
     g_dense_max_memory_pct = (int)value;
   } else if (n == "group_kernel") {
-    SBP_REQUIRE(value == 0 || value == 1, "group_kernel must be 0 or 1");
+    SBP_REQUIRE(value >= 0 && value <= 2, "group_kernel must be 0, 1 or 2");
     g_group_kernel = (int)value;
   } else if (n == "batched_wait_limit") {
     SBP_REQUIRE(value >= 16 && value <= (1LL << 30), "batched_wait_limit must be in [16, 2^30]");

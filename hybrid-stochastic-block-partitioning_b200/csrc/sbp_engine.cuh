@@ -296,8 +296,11 @@ inline int g_hashed_row_factor = 4;
 // sweep loop decided on the GPU; 0: one host-driven launch sequence per sweep (sbp_set_option).
 inline int g_graph_sweeps = 1;
 inline long long g_overflow_rebuilds = 0;   // rebuilds forced by a full hashed row
-// Light vertices of dense blockmodels: 1 evaluated by the group kernel (sbp_eval_small.cu), 0 by
-// the warp-per-vertex kernel (sbp_set_option "group_kernel").
+// Light vertices of dense blockmodels (sbp_set_option "group_kernel"): 1 (default) evaluated by the
+// group kernels (sbp_eval_small.cu) when B <= kSmallB (direct-indexed group tables), by the warp-
+// per-vertex kernels above; 2 by the group kernels at every B (hashed group tables above kSmallB:
+// half the occupancy of the warp kernel at the light-table size of the 200,000-vertex graph,
+// measured slower there); 0 by the warp-per-vertex kernels always.
 inline int g_group_kernel = 1;
 // Batched partitioner: idle claim attempts of a persistent CTA before the launch gives up with an
 // error (each attempt sleeps ~0.25 us), and the fault injection of the failure-detection test
@@ -499,7 +502,9 @@ struct SbpBlockmodel {
 
 namespace sbpb {
 
-inline bool use_group_kernel(const SbpBlockmodel& bm) { return g_group_kernel && !bm.sparse; }
+inline bool use_group_kernel(const SbpBlockmodel& bm) {
+  return !bm.sparse && (g_group_kernel == 2 || (g_group_kernel == 1 && bm.B <= kSmallB));
+}
 
 // Launch of the group kernel over n light vertices (dense storage).
 inline void launch_group_eval(const SbpGraph& g, SbpBlockmodel& bm, const int* verts, int n, const RngParams& rng,

@@ -352,16 +352,17 @@ __device__ __forceinline__ GroupEval group_evaluate(const GraphView& g, const Bl
       const int M_su = ldb<kFrozen>(bm.M + (size_t)s * ld + u);
       const int M_us = ldb<kFrozen>(bm.MT + (size_t)s * ld + u);
       const int du = ldb<kFrozen>(bm.d + u);
-      const bool is_r = u == r, is_s = u == s;
+      const bool is_r = u == r, is_s = u == s, corner = is_r || is_s;
       const double c = (double)(co + ci + (is_r ? self : 0));
-      fwd += c * (M_su + M_us + 1.0) / ((double)du + (double)B);
+      const double inv_u = 1.0 / ((double)du + (double)B);   // a non-corner block's degree is unchanged
+      fwd += c * (M_su + M_us + 1.0) * inv_u;
       const double bw = is_r ? (double)(M_rr + d_rr) + (double)(M_rr + d_rr) + 1.0
                       : is_s ? (double)(M_rs + d_rs) + (double)(M_sr + d_sr) + 1.0
                              : (double)(M_ru - co) + (double)(M_ur - ci) + 1.0;
       const int nd = is_r ? (dout_r - k_out) + (din_r - k_in) - (M_rr + d_rr)
                    : is_s ? (dout_s + k_out) + (din_s + k_in) - (M_ss + d_ss) : du;
-      bwd += c * bw / ((double)nd + (double)B);
-      if (!is_r && !is_s) {   // cells (r,u) (s,u) for out-edges to u, (u,r) (u,s) for in-edges
+      bwd += c * bw * (corner ? 1.0 / ((double)nd + (double)B) : inv_u);
+      if (!corner) {   // cells (r,u) (s,u) for out-edges to u, (u,r) (u,s) for in-edges
         if (co) {
           dS += dxlogx_int(bm.logt, M_ru, M_ru - co) + dxlogx_int(bm.logt, M_su, M_su + co);
           Tz += 2LL * (M_ru + M_su);

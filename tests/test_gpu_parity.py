@@ -313,7 +313,7 @@ def test_group_kernel_equals_warp_kernel(S, O, B, seed, algo):
     a = random_assignment(V, B, seed)
     g = S.Graph(V, s, d)
     states = []
-    for small in (1, 0):
+    for small in (2, 0):   # the group kernels at every B, then the warp kernels
         S.set_option("group_kernel", small)
         try:
             bm = S.Blockmodel(g, B, a)
