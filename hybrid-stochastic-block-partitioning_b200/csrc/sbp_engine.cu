@@ -331,7 +331,7 @@ void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, in
   if (nl > 0) {
     const bool small = use_group_kernel(bm);
     const size_t smem = (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps;
-    if (!small) set_smem_limit((const void*)k_eval, smem);
+    set_smem_limit((const void*)k_eval, smem);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (g_prof.on) {
       e0 = g_prof.get();
@@ -339,7 +339,15 @@ void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, in
       SBP_CUDA(cudaEventRecord(e0, c.stream));
     }
     if (small) {
-      launch_group_eval(g, bm, plan.order.p + plan.light_begin[bt], nl, rng, sweep, n_cur, nullptr, 0, c.stream);
+      // direct-indexed tables take every light vertex; hashed ones those of k <= kGroupMaxK, the
+      // warp kernel the rest
+      const int ng = bm.B <= kSmallB ? nl : plan.group_n[bt];
+      if (ng > 0)
+        launch_group_eval(g, bm, plan.order.p + plan.light_begin[bt], ng, rng, sweep, n_cur, nullptr, 0, c.stream);
+      if (nl > ng)
+        k_eval<<<grid_for(nl - ng, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem, c.stream>>>(
+            g.view(), bm.view(), plan.order.p + plan.light_begin[bt] + ng, nl - ng, rng, sweep, bm.prop.p,
+            bm.moved.p, n_cur, c.counters, g.light_cap, c.status, nullptr, 0);
     } else {
       k_eval<<<grid_for(nl, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem, c.stream>>>(
           g.view(), bm.view(), plan.order.p + plan.light_begin[bt], nl, rng, sweep, bm.prop.p, bm.moved.p, n_cur,
@@ -457,13 +465,17 @@ static int gibbs_sweeps_graph(SbpBlockmodel& bm, const SbpGraph& g, const BatchP
   for (int bt = 0; bt < nb; ++bt) {
     const int nl = plan.light_n[bt], nh = plan.heavy_n[bt];
     if (nl > 0) {
-      if (use_group_kernel(bm))
-        launch_group_eval(g, bm, plan.order.p + plan.light_begin[bt], nl, rng, 0, nullptr, g_ctl.p, bt, c.stream);
-      else
-        k_eval<<<grid_for(nl, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem_light, c.stream>>>(
-            g.view(), bm.view(), plan.order.p + plan.light_begin[bt], nl, rng, 0, bm.prop.p, bm.moved.p, nullptr,
-            c.counters, g.light_cap, c.status, g_ctl.p, bt);
-      ++launches;
+      const int ng = !use_group_kernel(bm) ? 0 : bm.B <= kSmallB ? nl : plan.group_n[bt];
+      if (ng > 0) {
+        launch_group_eval(g, bm, plan.order.p + plan.light_begin[bt], ng, rng, 0, nullptr, g_ctl.p, bt, c.stream);
+        ++launches;
+      }
+      if (nl > ng) {
+        k_eval<<<grid_for(nl - ng, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem_light, c.stream>>>(
+            g.view(), bm.view(), plan.order.p + plan.light_begin[bt] + ng, nl - ng, rng, 0, bm.prop.p, bm.moved.p,
+            nullptr, c.counters, g.light_cap, c.status, g_ctl.p, bt);
+        ++launches;
+      }
     }
     if (nh > 0) {
       k_eval<<<grid_for(nh, 1, 64 * c.num_sms), 32, smem_heavy, c.stream>>>(

@@ -318,6 +318,7 @@ using namespace sbpb;
 struct BatchPlan {
   DevBuf<int> order;                       // per batch: light vertices then heavy vertices
   std::vector<int> light_begin, light_n, heavy_begin, heavy_n;
+  std::vector<int> group_n;                // light vertices of k <= kGroupMaxK, at the front of each light list
   std::vector<double> light_bytes;         // algorithmic bytes of each light evaluation launch
   int max_batch = 0;
 };
@@ -375,8 +376,11 @@ struct SbpGraph {
       for (int bt = 0; bt < n / batch_size; ++bt) {
         const int start = bt * batch_size, end = std::min(n, (bt + 1) * batch_size);
         p->light_begin.push_back((int)order.size());
+        for (int i = start; i < end; ++i)   // vertices that fit the group tables first
+          if (h_k[list[i]] <= std::min(kGroupMaxK, light_cap / 2)) order.push_back(list[i]);
+        p->group_n.push_back((int)order.size() - p->light_begin.back());
         for (int i = start; i < end; ++i)
-          if (h_k[list[i]] <= light_cap / 2) order.push_back(list[i]);
+          if (h_k[list[i]] > kGroupMaxK && h_k[list[i]] <= light_cap / 2) order.push_back(list[i]);
         p->light_n.push_back((int)order.size() - p->light_begin.back());
         double lb = 0.0;   // 12 B (CSR offsets + b[v]) + 8 B per neighbour (id + block gather)
         for (int i = p->light_begin.back(); i < (int)order.size(); ++i) lb += 12.0 + 8.0 * h_k[order[i]];
@@ -506,12 +510,13 @@ inline bool use_group_kernel(const SbpBlockmodel& bm) {
   return !bm.sparse && (g_group_kernel == 2 || (g_group_kernel == 1 && bm.B <= kSmallB));
 }
 
-// Launch of the group kernel over n light vertices (dense storage).
+// Launch of the group kernel over n light vertices (dense storage); with hashed group tables
+// (B > kSmallB) every vertex must have k <= kGroupMaxK.
 inline void launch_group_eval(const SbpGraph& g, SbpBlockmodel& bm, const int* verts, int n, const RngParams& rng,
                               int sweep, int* n_moved, const SweepCtl* ctl, int batch, cudaStream_t stream) {
   Context& c = Context::get();
   const bool hashed_table = bm.B > kSmallB;
-  const int cap = g.light_cap;
+  const int cap = std::min(g.light_cap, 2 * kGroupMaxK);
   const size_t smem = gibbs_eval_group_smem(hashed_table, cap);
   const GibbsEvalGroupKernel k = gibbs_eval_group_kernel(hashed_table);
   static size_t set_for[2] = {0, 0};

@@ -58,6 +58,7 @@ inline GibbsEvalKernel gibbs_eval_kernel(bool hashed) { return hashed ? k_gibbs_
 constexpr int kSmallB = 128;
 constexpr int kSmallThreads = 256;
 constexpr int kSmallGroup = 8;
+constexpr int kGroupMaxK = 128;   // largest degree of a vertex on hashed group tables (256 slots)
 using GibbsEvalGroupKernel = void (*)(GraphView, BlockView, const int* __restrict__, int, RngParams, int, int*, int*,
                                       int*, unsigned long long*, int, int*, const SweepCtl*, int);
 GibbsEvalGroupKernel gibbs_eval_group_kernel(bool hashed_table);
