@@ -309,9 +309,47 @@ __device__ __forceinline__ int warp_select_hashed(const long long* base, const i
 __device__ __forceinline__ int select_in_chunk(int4 q, int chunk, long long target, int lane);
 
 // Two-level walk: find the chunk through the chunk sums, then the column inside the chunk
-// with one 16-byte load per lane.  Same result as warp_select_dense on the full row.
+// with one 16-byte load per lane.  Same result as warp_select_dense on the full row.  Up to
+// kWideChunks chunks, lane i loads the sums of chunks [16 i, 16 i + 16) at once (one memory
+// round trip instead of one per 32 chunks), scans its lane total across the warp and walks its
+// sixteen sums; longer rows take 32 chunks per step.
+constexpr int kWideChunks = 16 * kWarp;
 __device__ __forceinline__ int warp_select_chunked(const int* row, const int* csum, int nch, long long target,
                                                    int lane) {
+  if (nch <= kWideChunks) {
+    int cs[16];
+    long long lsum = 0;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int c = lane * 16 + q;
+      cs[q] = c < nch ? csum[c] : 0;
+      lsum += cs[q];
+    }
+    const long long incl = warp_incl_scan(lsum, lane);
+    const unsigned hit = __ballot_sync(kFull, incl > target);
+    if (!hit) return -1;
+    const int src = __ffs(hit) - 1;
+    int chunk = -1;
+    long long before = 0;
+    if (lane == src) {
+      long long run = incl - lsum;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        if (chunk < 0) {
+          if (target < run + cs[q]) {
+            chunk = lane * 16 + q;
+            before = run;
+          } else {
+            run += cs[q];
+          }
+        }
+      }
+    }
+    chunk = __shfl_sync(kFull, chunk, src);
+    before = __shfl_sync(kFull, before, src);
+    const int4 q4 = *reinterpret_cast<const int4*>(row + chunk * kChunk + 4 * lane);
+    return select_in_chunk(q4, chunk, target - before, lane);
+  }
   int chunk = -1;
   for (int base = 0; base < nch; base += kWarp) {
     const int c = base + lane;
