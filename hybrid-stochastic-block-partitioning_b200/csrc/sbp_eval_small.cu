@@ -11,7 +11,7 @@
 //    B <= kSmallB a direct-indexed array of B words (out count | in count << 15 | presence << 30),
 //    above it an open-addressing table of twice the light-vertex degree bound; plus the list of
 //    entries present;
-//  * the multinomial walk finds the chunk through the chunk sums, four per lane per step, then
+//  * the multinomial walk finds the chunk through the chunk sums, sixteen per lane per step, then
 //    the column inside it, sixteen counts per lane;
 //  * the frozen state of the batch (assignment, block matrix, degrees, log table) is read through
 //    the read-only data cache;
@@ -128,9 +128,12 @@ __device__ __forceinline__ int4 ldb4(const int4* p) {
 }
 
 // The multinomial walk of evaluate_vertex over a dense row (or column) of M: the first column
-// whose running count exceeds tg.  Chunk sums (kChunk columns each) locate the chunk, four per
-// lane per step; the chunk's counts are then scanned sixteen per lane.  Every lane of the warp
+// whose running count exceeds tg.  Chunk sums (kChunk columns each) locate the chunk, sixteen per
+// lane per step (one memory round trip per 16 G chunks); the chunk's counts are then scanned
+// sixteen per lane.  Every lane of the warp
 // takes part (loop bounds are warp-uniform); groups with walk == false get -1.
+constexpr int kSumsPerLane = 16;
+
 template <int G, bool kFrozen>
 __device__ __forceinline__ int group_walk(const int* row, const int* csum, int nch, long long tg, bool walk, int gl,
                                           int gbase) {
@@ -141,12 +144,12 @@ __device__ __forceinline__ int group_walk(const int* row, const int* csum, int n
     bool found = !walk;
     chunk = -1;
     long long acc = 0;
-    for (int c0 = 0; c0 < nch; c0 += 4 * G) {
-      int cs[4];
+    for (int c0 = 0; c0 < nch; c0 += kSumsPerLane * G) {
+      int cs[kSumsPerLane];
       long long lsum = 0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int c = c0 + gl * 4 + q;
+      for (int q = 0; q < kSumsPerLane; ++q) {
+        const int c = c0 + gl * kSumsPerLane + q;
         cs[q] = (walk && c < nch) ? ldb<kFrozen>(csum + c) : 0;
         lsum += cs[q];
       }
@@ -163,10 +166,10 @@ __device__ __forceinline__ int group_walk(const int* row, const int* csum, int n
       if (hit && gl == __ffs(hit) - 1 - gbase) {
         long long run = acc + incl - lsum;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < kSumsPerLane; ++q) {
           if (pick < 0) {
             if (tg < run + cs[q]) {
-              pick = c0 + gl * 4 + q;
+              pick = c0 + gl * kSumsPerLane + q;
               pb = run;
             } else {
               run += cs[q];
