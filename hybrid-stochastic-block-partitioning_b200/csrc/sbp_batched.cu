@@ -312,7 +312,7 @@ std::vector<int4> sweep_stages(const BatchPlan& p, int chunk, int mdl_ctas) {
   return st;
 }
 
-enum SlotState { kNeedMerge, kFinetuning, kDone };
+enum SlotState { kNeedMerge, kFinetuning, kEnded, kDone };   // kEnded: finetune over, not yet wrapped up
 
 struct Slot {
   int index = 0;
@@ -405,6 +405,7 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
   };
 
   auto start_finetune = [&](Slot& s) {
+    Context& c = Context::get();   // primary, or secondary beside a sweep launch
     SbpBlockmodel& bm = s.ps->bm;
     std::memset(&s.fs, 0, sizeof s.fs);
     s.fs.num_blocks = bm.B;
@@ -429,6 +430,7 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
     s.state = kFinetuning;
   };
   auto end_finetune = [&](Slot& s) {
+    Context& c = Context::get();
     SbpBlockmodel& bm = s.ps->bm;
     bm.overall_entropy = (float)mdl(bm, *s.g);
     unsigned long long cnt[3];
@@ -444,31 +446,42 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
     s.state = s.ps->done ? kDone : kNeedMerge;
   };
 
-  for (;;) {
-    // graphs between finetunes: merge step, then the batched finetune or the single-graph round
-    for (auto& sp : slots) {
-      Slot& s = *sp;
-      if (s.state != kNeedMerge) continue;
-      const int algo = partition_merge(*s.ps, *s.g, opt, &s.fo);
-      if (algo == SBP_ASYNC_GIBBS && batchable(s.ps->bm, *s.g)) {
-        start_finetune(s);
-        info.batched_finetunes++;
-      } else {
-        SbpStats fs;
-        finetune(s.ps->bm, *s.g, algo, s.fo, nullptr, fs);
-        info.fallback_finetunes++;
-        partition_finish_round(*s.ps, *s.g, fs, s.out);
-        s.state = s.ps->done ? kDone : kNeedMerge;
-      }
+  // The steps of one graph between two finetunes: the end of the last one, the golden-section
+  // step, the merge, and the start of the next finetune (batched) or a whole single-graph one.
+  auto between = [&](Slot& s) {
+    if (s.state == kEnded) end_finetune(s);
+    if (s.state != kNeedMerge) return;
+    const int algo = partition_merge(*s.ps, *s.g, opt, &s.fo);
+    if (algo == SBP_ASYNC_GIBBS && batchable(s.ps->bm, *s.g)) {
+      start_finetune(s);
+      info.batched_finetunes++;
+    } else {
+      SbpStats fs;
+      finetune(s.ps->bm, *s.g, algo, s.fo, nullptr, fs);
+      info.fallback_finetunes++;
+      partition_finish_round(*s.ps, *s.g, fs, s.out);
+      s.state = s.ps->done ? kDone : kNeedMerge;
     }
+  };
+  // While a sweep launch runs on the primary stream, the graphs between finetunes are processed
+  // on the secondary context; they touch none of the buffers of the graphs in the launch.
+  // Buffers in the device cache carry no pending work of the primary stream: every launch
+  // follows a synchronisation of that stream with only its own set-up copies after it.
+  Context* side = g_batched_overlap > 0 ? &Context::secondary() : nullptr;
+
+  for (;;) {
     std::vector<Slot*> act;
-    bool all_done = true;
+    bool all_done = true, waiting = false;
     for (auto& sp : slots) {
       if (sp->state == kFinetuning) act.push_back(sp.get());
+      if (sp->state == kNeedMerge || sp->state == kEnded) waiting = true;
       if (sp->state != kDone) all_done = false;
     }
     if (all_done) break;
-    if (act.empty()) continue;
+    if (act.empty()) {   // nothing to sweep: the graphs between finetunes, on the primary stream
+      for (auto& sp : slots) between(*sp);
+      continue;
+    }
 
     // one sweep of every finetuning graph
     const Shape shape = current_shape();
@@ -517,7 +530,8 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
       std::memset(&q, 0, sizeof q);
       if (g_batched_stall_graph == s->index) q.ctr = 1ull << 20;   // stage 0, item 2^20: beyond every stage
     }
-    const int grid = shape.ctas_per_sm * c.num_sms;
+    const int reserve = (side && waiting) ? std::min(g_batched_overlap, shape.ctas_per_sm * c.num_sms / 2) : 0;
+    const int grid = shape.ctas_per_sm * c.num_sms - reserve;
     auto ex = cl.execs.find(grid);
     if (ex == cl.execs.end()) {
       cudaGraph_t graph;
@@ -544,6 +558,17 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
     ++g_launches;
     g_h2d += (long long)(n * (sizeof(BGraph) + sizeof(int) + sizeof(Queue)) + sizeof(SweepParams));
     g_d2h += (long long)(n * sizeof(double) + sizeof(int));
+    if (waiting) {
+      try {
+        ContextScope scope(side);
+        for (auto& sp : slots)
+          if (sp->state != kFinetuning) between(*sp);
+        if (side) side->sync();
+      } catch (...) {
+        cudaStreamSynchronize(c.stream);   // no launch outlives the call
+        throw;
+      }
+    }
     c.sync();
     info.sweep_launches++;
     if (*hStatus) c.check_status();
@@ -567,7 +592,7 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
       s->fs.sweeps++;
       const int it = s->sweep++;
       if (early_stop(it, s->fo.bracket_established != 0, s->initial, s->deltas) || s->sweep >= kMaxIterations)
-        end_finetune(*s);
+        s->state = kEnded;
     }
   }
   if (tuning && g_tuned.find(key) == g_tuned.end() && ncand > 0) {

@@ -1143,6 +1143,9 @@ SbpStatus sbp_set_option(const char* name, int64_t value) {
   } else if (n == "batched_stall_graph") {
     SBP_REQUIRE(value >= -1 && value < (1LL << 30), "batched_stall_graph must be -1 or a graph index");
     g_batched_stall_graph = (int)value;
+  } else if (n == "batched_overlap") {
+    SBP_REQUIRE(value >= 0 && value <= 1024, "batched_overlap must be in [0, 1024]");
+    g_batched_overlap = (int)value;
   } else {
     throw Error(SBP_ERR_INVALID_ARGUMENT, "unknown option: " + n);
   }

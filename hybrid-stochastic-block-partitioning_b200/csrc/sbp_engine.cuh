@@ -184,7 +184,29 @@ struct Context {
   int npartial = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
-  static Context& get() {
+  // A context: its own stream and scratch; the log table is shared when given.
+  static Context* create(double2* logt) {
+    auto* c = new Context();
+    SBP_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    int dev = 0;
+    SBP_CUDA(cudaGetDevice(&dev));
+    SBP_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
+    c->npartial = 4 * c->num_sms;
+    SBP_CUDA(cudaMalloc(&c->status, 8 * sizeof(int)));
+    SBP_CUDA(cudaMalloc(&c->counters, 8 * sizeof(unsigned long long)));
+    SBP_CUDA(cudaMalloc(&c->partial, c->npartial * sizeof(double)));
+    SBP_CUDA(cudaMalloc(&c->scalar, sizeof(double)));
+    SBP_CUDA(cudaMalloc(&c->mh_out, 16 * sizeof(double)));
+    SBP_CUDA(cudaMalloc(&c->done, sizeof(unsigned)));
+    SBP_CUDA(cudaMemset(c->status, 0, 8 * sizeof(int)));
+    SBP_CUDA(cudaMemset(c->done, 0, sizeof(unsigned)));
+    SBP_CUDA(cudaEventCreate(&c->ev0));
+    SBP_CUDA(cudaEventCreate(&c->ev1));
+    c->logt = logt ? logt : make_log_table();
+    return c;
+  }
+  // The process's context: every entry point runs on it.
+  static Context& primary() {
     static Context* ctx = nullptr;
     if (!ctx) {
       int n = 0;
@@ -192,26 +214,25 @@ struct Context {
         cudaGetLastError();
         throw Error(SBP_ERR_CUDA, "no CUDA device available (the engine has no CPU fallback)");
       }
-      auto* c = new Context();
-      SBP_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-      int dev = 0;
-      SBP_CUDA(cudaGetDevice(&dev));
-      SBP_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
-      c->npartial = 4 * c->num_sms;
-      SBP_CUDA(cudaMalloc(&c->status, 8 * sizeof(int)));
-      SBP_CUDA(cudaMalloc(&c->counters, 8 * sizeof(unsigned long long)));
-      SBP_CUDA(cudaMalloc(&c->partial, c->npartial * sizeof(double)));
-      SBP_CUDA(cudaMalloc(&c->scalar, sizeof(double)));
-      SBP_CUDA(cudaMalloc(&c->mh_out, 16 * sizeof(double)));
-      SBP_CUDA(cudaMalloc(&c->done, sizeof(unsigned)));
-      SBP_CUDA(cudaMemset(c->status, 0, 8 * sizeof(int)));
-      SBP_CUDA(cudaMemset(c->done, 0, sizeof(unsigned)));
-      SBP_CUDA(cudaEventCreate(&c->ev0));
-      SBP_CUDA(cudaEventCreate(&c->ev1));
-      c->logt = make_log_table();
-      ctx = c;
+      ctx = create(nullptr);
     }
     return *ctx;
+  }
+  // A second context, for work that runs beside the primary stream's kernels (the batched
+  // partitioner's merges while its sweep kernel runs).
+  static Context& secondary() {
+    static Context* ctx = nullptr;
+    if (!ctx) ctx = create(primary().logt);
+    return *ctx;
+  }
+  // The calling thread's current context: the primary one unless a ContextScope is open.
+  static Context*& current() {
+    static thread_local Context* cur = nullptr;
+    return cur;
+  }
+  static Context& get() {
+    Context* c = current();
+    return c ? *c : primary();
   }
   void sync() { SBP_CUDA(cudaStreamSynchronize(stream)); }
   // Read and clear the device status word; throw on any error bit.
@@ -233,6 +254,17 @@ struct Context {
 };
 
 inline cudaStream_t engine_stream() { return Context::get().stream; }
+
+// Makes a context current on the calling thread for the scope's lifetime (null: no change).
+struct ContextScope {
+  Context* prev;
+  explicit ContextScope(Context* c) : prev(Context::current()) {
+    if (c) Context::current() = c;
+  }
+  ~ContextScope() { Context::current() = prev; }
+  ContextScope(const ContextScope&) = delete;
+  ContextScope& operator=(const ContextScope&) = delete;
+};
 
 // Optional timing of the vertex-evaluation kernel: CUDA events around every light-vertex
 // evaluation launch on the launching stream, resolved when the profile is read.
@@ -307,6 +339,9 @@ inline int g_group_kernel = 1;
 // (index of a graph whose sweep queue never opens; -1: none).  sbp_set_option.
 inline long long g_batched_wait_limit = 1LL << 22;
 inline int g_batched_stall_graph = -1;
+// CTA slots the batched sweep kernel leaves free while the merges of the graphs between two
+// finetunes run beside it on the secondary context (0: merges run after each sweep launch).
+inline int g_batched_overlap = 0;
 
 }  // namespace sbpb
 

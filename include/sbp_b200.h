@@ -122,7 +122,11 @@ int32_t sbp_device_count(void);
  * persistent CTA of sbp_partition_batched before its launch gives up and the call fails with
  * SBP_ERR_DEVICE.  "batched_stall_graph" (default -1): fault injection for failure-detection
  * tests -- the sweep queue of that graph of a batched launch starts with its first stage taken,
- * so no stage of it ever opens and the launch must end by its wait limit. */
+ * so no stage of it ever opens and the launch must end by its wait limit.  "batched_overlap"
+ * (default 16, range 0-1024): while a sweep launch of sbp_partition_batched runs, the graphs
+ * between two finetunes (merge, golden-section step, the next finetune's set-up) are processed
+ * on a second stream, and the launch leaves this many CTA slots free for their kernels; 0 runs
+ * them after each launch instead (same results either way). */
 SbpStatus sbp_set_option(const char *name, int64_t value);
 
 /* The CUDA stream every call of this library runs on (cudaStream_t), for interop and timing.

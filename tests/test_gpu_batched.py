@@ -125,3 +125,23 @@ def test_batched_wait_runs_out_and_the_library_stays_usable(S):
     for g, out in zip(graphs, outs):
         single, _ = S.sbp.stochastic_block_partition(g, batches=4, seed=3)
         assert np.array_equal(out, single)
+
+
+@pytest.mark.parametrize("overlap", [0, 16, 1024])
+def test_batched_overlapped_merges_are_identical(S, overlap):
+    """The graphs between finetunes are processed on a second stream while a sweep launch runs
+    (sbp_set_option "batched_overlap" = CTA slots left free for them; 1024 leaves half the grid,
+    0 runs them after the launch): the partitions are the single-graph ones either way,
+    including rounds on row-hashed storage with the single-graph finetune."""
+    specs = uneven_graphs(500, [700, 2100, 350, 1500, 900, 3000, 1200, 500])
+    graphs = [S.Graph(V, s, d) for V, s, d, _ in specs]
+    S.set_option("batched_overlap", overlap)
+    S.set_option("dense_max_blocks", 256)
+    try:
+        outs, stats, info = S.batched.stochastic_block_partition(graphs, batches=10, seed=21)
+        assert info["batched_finetunes"] > 0 and info["fallback_finetunes"] > 0
+        for g, out, st in zip(graphs, outs, stats):
+            assert_same(out, st, *single(S, g, 21))
+    finally:
+        S.set_option("dense_max_blocks", 65536)
+        S.set_option("batched_overlap", 16)
