@@ -625,7 +625,9 @@ __global__ void __launch_bounds__(kMhGroupThreads)
           chunk_add(bm.CST, bm.nch, s, u, ci);
         }
       }
-      __syncwarp();
+      // only this group's lanes are here (the other groups of the warp may not commit): a
+      // full-warp barrier would wait for lanes that never arrive
+      __syncwarp(G == 32 ? kFull : ((1u << G) - 1u) << gbase);
       if (gl == 0) {
         const int self = e.self;
         const int d_rr = -co_r - ci_r - self, d_rs = -co_s + ci_r;
