@@ -327,7 +327,7 @@ void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, in
   Context& c = Context::get();
   const int nl = plan.light_n[bt], nh = plan.heavy_n[bt];
   int* n_cur = bm.n_moved.p + (bm.gen & 1);
-  const GibbsEvalKernel k_eval = gibbs_eval_kernel(bm.sparse);
+  const GibbsEvalKernel k_eval = gibbs_eval_kernel(bm.sparse, bm.B);
   if (nl > 0) {
     const bool small = use_group_kernel(bm);
     const size_t smem = (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps;
@@ -432,7 +432,7 @@ static int gibbs_sweeps_graph(SbpBlockmodel& bm, const SbpGraph& g, const BatchP
   SBP_CUDA(SBP_COPY_ASYNC(g_ctl.p, &h, sizeof h, cudaMemcpyHostToDevice, c.stream));
   const size_t smem_light = (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps;
   const size_t smem_heavy = (size_t)table_ints(g.heavy_cap) * sizeof(int);
-  const GibbsEvalKernel k_eval = k_gibbs_eval_dense;   // the graph runs dense storage only
+  const GibbsEvalKernel k_eval = gibbs_eval_kernel(false, bm.B);   // the graph runs dense storage only
   set_smem_limit((const void*)k_eval, std::max(smem_light, smem_heavy));
   const bool cells = (long long)bm.B * bm.B <= 4LL * g.E;
   const int mdl_grid = c.npartial;

@@ -1037,7 +1037,7 @@ SbpStatus sbp_collect_moves(SbpBlockmodel* bm, const SbpGraph* cg, SbpDataset* d
       // plain evaluation (gibbs_batch without its apply), record, then apply
       const int nl = plan.light_n[bt], nh = plan.heavy_n[bt];
       int* n_cur = bm->n_moved.p + (bm->gen & 1);
-      const GibbsEvalKernel k_eval = gibbs_eval_kernel(bm->sparse);
+      const GibbsEvalKernel k_eval = gibbs_eval_kernel(bm->sparse, bm->B);
       if (nl > 0) {
         const size_t smem = (size_t)table_ints(g.light_cap) * sizeof(int) * kLightWarps;
         set_smem_limit((const void*)k_eval, smem);
