@@ -479,7 +479,9 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
     }
     if (all_done) break;
     if (act.empty()) {   // nothing to sweep: the graphs between finetunes, on the primary stream
+      const auto h0 = std::chrono::steady_clock::now();
       for (auto& sp : slots) between(*sp);
+      info.serial_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - h0).count();
       continue;
     }
 
@@ -559,11 +561,14 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
     g_h2d += (long long)(n * (sizeof(BGraph) + sizeof(int) + sizeof(Queue)) + sizeof(SweepParams));
     g_d2h += (long long)(n * sizeof(double) + sizeof(int));
     if (waiting) {
+      const auto h0 = std::chrono::steady_clock::now();
       try {
         ContextScope scope(side);
         for (auto& sp : slots)
           if (sp->state != kFinetuning) between(*sp);
         if (side) side->sync();
+        (side ? info.overlapped_seconds : info.serial_seconds) +=
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - h0).count();
       } catch (...) {
         cudaStreamSynchronize(c.stream);   // no launch outlives the call
         throw;

@@ -341,7 +341,7 @@ inline long long g_batched_wait_limit = 1LL << 22;
 inline int g_batched_stall_graph = -1;
 // CTA slots the batched sweep kernel leaves free while the merges of the graphs between two
 // finetunes run beside it on the secondary context (0: merges run after each sweep launch).
-inline int g_batched_overlap = 0;
+inline int g_batched_overlap = 64;
 
 }  // namespace sbpb
 

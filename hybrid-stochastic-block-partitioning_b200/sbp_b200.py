@@ -129,7 +129,8 @@ class BatchInfo(ctypes.Structure):
     _fields_ = [("rounds", ctypes.c_int32), ("batched_finetunes", ctypes.c_int32),
                 ("fallback_finetunes", ctypes.c_int32), ("sweep_launches", ctypes.c_int32), ("chunk", ctypes.c_int32),
                 ("ctas_per_sm", ctypes.c_int32), ("tuned", ctypes.c_int32), ("candidates", ctypes.c_int32),
-                ("candidate_ms", ctypes.c_double * 8), ("sweep_seconds", ctypes.c_double), ("seconds", ctypes.c_double)]
+                ("candidate_ms", ctypes.c_double * 8), ("sweep_seconds", ctypes.c_double), ("seconds", ctypes.c_double),
+                ("overlapped_seconds", ctypes.c_double), ("serial_seconds", ctypes.c_double)]
 
 
 class Trace(ctypes.Structure):

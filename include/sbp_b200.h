@@ -123,7 +123,7 @@ int32_t sbp_device_count(void);
  * SBP_ERR_DEVICE.  "batched_stall_graph" (default -1): fault injection for failure-detection
  * tests -- the sweep queue of that graph of a batched launch starts with its first stage taken,
  * so no stage of it ever opens and the launch must end by its wait limit.  "batched_overlap"
- * (default 16, range 0-1024): while a sweep launch of sbp_partition_batched runs, the graphs
+ * (default 64, range 0-1024): while a sweep launch of sbp_partition_batched runs, the graphs
  * between two finetunes (merge, golden-section step, the next finetune's set-up) are processed
  * on a second stream, and the launch leaves this many CTA slots free for their kernels; 0 runs
  * them after each launch instead (same results either way). */
@@ -442,6 +442,9 @@ typedef struct {
     double candidate_ms[8];     /* their sweep times, per graph swept */
     double sweep_seconds;       /* device time of the persistent sweep launches */
     double seconds;             /* device-clock time of the whole call */
+    double overlapped_seconds;  /* host time of the steps between finetunes (merges and the rest)
+                                   that ran beside a sweep launch */
+    double serial_seconds;      /* host time of those steps while no sweep launch ran */
 } SbpBatchInfo;
 
 /* graphs[n] -> out_assignments[i][V_i]; stats[i] per graph (optional; total_seconds is the

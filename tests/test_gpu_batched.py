@@ -144,4 +144,4 @@ def test_batched_overlapped_merges_are_identical(S, overlap):
             assert_same(out, st, *single(S, g, 21))
     finally:
         S.set_option("dense_max_blocks", 65536)
-        S.set_option("batched_overlap", 16)
+        S.set_option("batched_overlap", 64)
