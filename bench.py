@@ -63,7 +63,27 @@ def args_parse():
                     help="drive every finetune sweep from the host (same kernels and results) instead of one CUDA "
                          "graph per finetune call; for kernel profilers, which do not profile the kernel nodes of a "
                          "graph with conditional nodes")
+    ap.add_argument("--eval-case", type=int, default=0, metavar="PARTS",
+                    help="a small case for kernel profilers instead of the bench: three host-driven asynchronous-"
+                         "Gibbs sweeps from the planted partition split PARTS ways")
     return ap.parse_args()
+
+
+def eval_case(a, V, src, dst, truth):
+    """Kernel-profiler case: the planted partition with each block split into `a.eval_case` random
+    parts, three asynchronous-Gibbs sweeps driven from the host, so that every evaluation launch is
+    a plain kernel launch (ncu does not profile the kernel nodes of the graph-run finetune)."""
+    import numpy as np
+    import sbp_b200 as S
+    S.load()
+    g = S.Graph(V, src, dst)
+    rng = np.random.default_rng(0)
+    b = truth.astype(np.int64) * a.eval_case + rng.integers(0, a.eval_case, V)
+    b = np.unique(b, return_inverse=True)[1].astype(np.int32)
+    S.set_option("graph_sweeps", 0)
+    bm = S.Blockmodel(g, int(b.max()) + 1, b)
+    st = S.finetune.asynchronous_gibbs(bm, batches=a.batches, seed=3, max_sweeps=3)
+    print(json.dumps({"eval_case": a.eval_case, "B": bm.B, "visits": st["visits"], "accepted": st["accepted"]}))
 
 
 def peaks():
@@ -264,21 +284,30 @@ def learned_vs_plain(S, O, dcsbm, np):
             "target": "learned reaches the plain final MDL within 0.5 % in at least 2x less wall time"}
 
 
-def mh_and_hybrid(S, O, dcsbm):
+def mh_and_hybrid(S, O, dcsbm, big):
     """Full partitions with Metropolis-Hastings and with the hybrid schedule (batches 10) on the
-    20,000-vertex / 32-block graph, second of two runs timed on the device clock."""
+    20,000-vertex / 32-block graph, second of two runs timed on the device clock; and one hybrid
+    partition of the bench graph (`big`: V, src, dst, truth), timed on its first run."""
+    def entry(a, st, truth):
+        return {"seconds": st["total_seconds"], "mcmc_seconds": st["mcmc_seconds"], "sweeps": st["sweeps"],
+                "visits": st["visits"], "visits_per_s": st["visits"] / st["total_seconds"], "mdl": st["mdl"],
+                "blocks": st["num_blocks"], "nmi_vs_planted": float(O.nmi(a, truth))}
     V, s, d, truth = dcsbm.config_graph(2)
     g = S.Graph(V, s, d)
     out = {"workload": WORKLOADS[2]}
     for algo in ("metropolis_hastings", "hybrid_mcmc"):
         S.sbp.stochastic_block_partition(g, algorithm=algo, batches=10, seed=2)
         a, st = S.sbp.stochastic_block_partition(g, algorithm=algo, batches=10, seed=2)
-        out[algo] = {"seconds": st["total_seconds"], "mcmc_seconds": st["mcmc_seconds"], "sweeps": st["sweeps"],
-                     "visits": st["visits"], "visits_per_s": st["visits"] / st["total_seconds"], "mdl": st["mdl"],
-                     "blocks": st["num_blocks"], "nmi_vs_planted": float(O.nmi(a, truth))}
+        out[algo] = entry(a, st, truth)
     anchor = reference_anchor(2)
     if anchor:
         out["reference_full_partition_async_gibbs"] = anchor
+    V, s, d, truth = big
+    g = S.Graph(V, s, d)
+    a, st = S.sbp.stochastic_block_partition(g, algorithm="hybrid_mcmc", batches=10, seed=2)
+    out["hybrid_mcmc_bench_graph"] = dict(
+        entry(a, st, truth), workload="hybrid SBP: Metropolis-Hastings over the highest-degree 15 % of vertices, "
+        "async Gibbs (batches 10) over the rest, approximate block merge; " + WORKLOADS[4].split("merge, ")[1])
     return out
 
 
@@ -324,6 +353,9 @@ def main():
               "merge": "approximate", "step": "one full stochastic_block_partition (B = V -> final B)",
               "l2": "256 MB buffer written before every timed step (L2 flush)", "parallelism": f"replicas x{world}",
               "sweep_driver": "host loop" if a.host_sweeps else "one CUDA graph per finetune call"}
+    if a.eval_case:
+        eval_case(a, V, src, dst, truth)
+        return
 
     if a.impl == "reference":
         if rank != 0:
@@ -486,7 +518,7 @@ def main():
         if world == 1 and not a.no_batched:
             line["batched"] = batched_vs_sequential(S, dcsbm, np)
         if world == 1 and not a.no_mh:
-            line["mh_and_hybrid"] = mh_and_hybrid(S, O, dcsbm)
+            line["mh_and_hybrid"] = mh_and_hybrid(S, O, dcsbm, (V, src, dst, truth))
         print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()

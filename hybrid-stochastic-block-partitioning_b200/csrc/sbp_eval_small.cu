@@ -133,10 +133,6 @@ __device__ __forceinline__ int4 ldb4(const int4* p) {
 // sixteen per lane.  Every lane of the warp
 // takes part (loop bounds are warp-uniform); groups with walk == false get -1.
 constexpr int kSumsPerLane = 16;
-// Steps of the neighbour gather, and table entries of the delta-MDL sum, whose loads are issued
-// together (memory-level parallelism inside one lane group).
-constexpr int kGatherBatch = 4;
-constexpr int kEntryBatch = 4;
 
 template <int G, bool kFrozen>
 __device__ __forceinline__ int group_walk(const int* row, const int* csum, int nch, long long tg, bool walk, int gl,
@@ -268,30 +264,19 @@ __device__ __forceinline__ GroupEval group_evaluate(const GraphView& g, const Bl
   const int idx = (valid && k > 0 && !given) ? (int)scale32(x.x, k) : -1;
   // 1. neighbour-block histogram and the proposal's neighbour block
   int tblk = -1;
-  // kGatherBatch steps at a time: every neighbour id of the steps, then every block, then the
-  // table inserts and the proposal's pick in step order (two memory round trips per batch of
-  // steps instead of two per step; the same inserts in the same order)
   const int gather_iters = warp_max_int((k + G - 1) / G);
-  for (int it0 = 0; it0 < gather_iters; it0 += kGatherBatch) {
-    int uu[kGatherBatch], bu[kGatherBatch];
-#pragma unroll
-    for (int q = 0; q < kGatherBatch; ++q) {
-      const int e = (it0 + q) * G + gl;
-      uu[q] = e < k ? (e < k_out ? __ldg(g.out_idx + o0 + e) : __ldg(g.in_idx + i0 + (e - k_out))) : -1;
+  for (int it = 0; it < gather_iters; ++it) {
+    const int e = it * G + gl;
+    int bu = -1;
+    if (e < k) {
+      const bool out = e < k_out;
+      const int u = out ? __ldg(g.out_idx + o0 + e) : __ldg(g.in_idx + i0 + (e - k_out));
+      bu = ldb<kFrozen>(bm.b + u);
+      if (!(out && u == v)) T.add(bu, out ? 1u : (1u << kInShift));   // the self loop only marks r present
     }
-#pragma unroll
-    for (int q = 0; q < kGatherBatch; ++q) bu[q] = uu[q] >= 0 ? ldb<kFrozen>(bm.b + uu[q]) : -1;
-#pragma unroll
-    for (int q = 0; q < kGatherBatch; ++q) {
-      if (it0 + q < gather_iters) {   // warp-uniform
-        const int e = (it0 + q) * G + gl;
-        const bool out = e < k_out;
-        if (e < k && !(out && uu[q] == v)) T.add(bu[q], out ? 1u : (1u << kInShift));   // a self loop only marks r
-        const int src = idx - (it0 + q) * G;
-        const int pick = __shfl_sync(kFull, bu[q], (src >= 0 && src < G) ? src : 0, G);
-        if (src >= 0 && src < G) tblk = pick;
-      }
-    }
+    const int src = idx - it * G;
+    const int pick = __shfl_sync(kFull, bu, (src >= 0 && src < G) ? src : 0, G);
+    if (src >= 0 && src < G) tblk = pick;
   }
   if (valid && self && gl == 0) T.add(r, kPresent);
   __syncwarp();
@@ -357,34 +342,19 @@ __device__ __forceinline__ GroupEval group_evaluate(const GraphView& g, const Bl
   const int d_ss = co_s + ci_s + self;
   const int kin_self = k_in + self;
   const int nent = active ? *T.n : 0;
-  // each lane takes entries gl, gl + G, ... in that order, kEntryBatch at a time: the batch's
-  // cells and degrees are loaded first (one memory round trip), then its terms are added in order
-  for (int j0 = gl; j0 < nent; j0 += kEntryBatch * G) {
-    int uu[kEntryBatch], cw[kEntryBatch], m_ru[kEntryBatch], m_ur[kEntryBatch], m_su[kEntryBatch],
-        m_us[kEntryBatch], dd[kEntryBatch];
-#pragma unroll
-    for (int q = 0; q < kEntryBatch; ++q) {
-      const int j = j0 + q * G;
-      uu[q] = -1;
-      if (j < nent) {
-        const int slot = T.list[j];
-        const int u = T.key_of(slot);
-        uu[q] = u;
-        cw[q] = (int)T.w[slot];
-        m_ru[q] = ldb<kFrozen>(bm.M + (size_t)r * ld + u);
-        m_ur[q] = ldb<kFrozen>(bm.MT + (size_t)r * ld + u);
-        m_su[q] = ldb<kFrozen>(bm.M + (size_t)s * ld + u);
-        m_us[q] = ldb<kFrozen>(bm.MT + (size_t)s * ld + u);
-        dd[q] = ldb<kFrozen>(bm.d + u);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < kEntryBatch; ++q) {
-      if (uu[q] < 0) continue;
-      const int u = uu[q];
-      const unsigned wu = (unsigned)cw[q];
+  const int ent_iters = warp_max_int((nent + G - 1) / G);
+  for (int it = 0; it < ent_iters; ++it) {
+    const int j = it * G + gl;
+    if (j < nent) {
+      const int slot = T.list[j];
+      const int u = T.key_of(slot);
+      const unsigned wu = T.w[slot];
       const int co = wu & kCountMask, ci = (wu >> kInShift) & kCountMask;
-      const int M_ru = m_ru[q], M_ur = m_ur[q], M_su = m_su[q], M_us = m_us[q], du = dd[q];
+      const int M_ru = ldb<kFrozen>(bm.M + (size_t)r * ld + u);
+      const int M_ur = ldb<kFrozen>(bm.MT + (size_t)r * ld + u);
+      const int M_su = ldb<kFrozen>(bm.M + (size_t)s * ld + u);
+      const int M_us = ldb<kFrozen>(bm.MT + (size_t)s * ld + u);
+      const int du = ldb<kFrozen>(bm.d + u);
       const bool is_r = u == r, is_s = u == s, corner = is_r || is_s;
       const double c = (double)(co + ci + (is_r ? self : 0));
       const double inv_u = 1.0 / ((double)du + (double)B);   // a non-corner block's degree is unchanged
@@ -475,7 +445,8 @@ __device__ __forceinline__ void group_table_clear(const GroupTable<kHash>& T, in
 
 // Direct-indexed tables (33 KB of shared memory per CTA): registers capped for three CTAs per SM
 // (measured 17 % shorter launches than at two CTAs per SM on 71 blocks).  Hashed tables of 256
-// slots take 98 KB per CTA, two CTAs per SM whatever the registers.
+// slots take 98 KB per CTA, two CTAs per SM whatever the registers.  (Issuing the loads of four
+// gather steps, or of four delta-MDL entries, together was measured 3-8 % slower.)
 template <int G, bool kHash>
 __global__ void __launch_bounds__(kSmallThreads, kHash ? 2 : 3)
     k_gibbs_eval_group(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
