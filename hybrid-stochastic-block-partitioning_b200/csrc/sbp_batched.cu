@@ -24,6 +24,11 @@
 // A graph whose round cannot use the kernel (row-hashed storage at large B, Metropolis-
 // Hastings or hybrid finetunes, degrees beyond the kernel's tables) runs that round's
 // finetune on the single-graph path, between two sweep launches of the others.
+//
+// The steps of the graphs between two finetunes (end of the finetune, golden-section step,
+// merge, set-up of the next finetune) run on a pool of host threads, each with its own context,
+// while the next sweep launch of the other graphs runs; the launch leaves a few CTA slots free
+// for their kernels.
 #include <chrono>
 #include <map>
 
@@ -334,6 +339,84 @@ struct Slot {
   DevBuf<double> partial;
 };
 
+// Host threads for the steps of several graphs between their finetunes.  Each thread has its
+// own context (stream, status word, MDL scratch), so the small kernels and the host
+// synchronisations of different graphs' merges overlap one another.  Created once, never
+// destroyed (its threads wait for work until the process exits).
+class StepPool {
+ public:
+  static StepPool& get() {
+    static StepPool* pool = new StepPool(kMaxThreads);
+    return *pool;
+  }
+  // fn(item) for every item, spread over `threads` of the pool's threads (each item handled by
+  // one thread, its device work finished on return); rethrows the first exception.
+  void run(const std::vector<Slot*>& items, int threads, const std::function<void(Slot&)>& fn) {
+    threads = std::max(1, std::min({threads, kMaxThreads, (int)items.size()}));
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      items_ = &items;
+      fn_ = &fn;
+      next_ = 0;
+      active_ = threads;
+      busy_ = threads;
+      err_ = nullptr;
+      ++gen_;
+    }
+    cv_work_.notify_all();
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_done_.wait(lk, [&] { return busy_ == 0; });
+    if (err_) std::rethrow_exception(err_);
+  }
+
+ private:
+  static constexpr int kMaxThreads = 64;
+  explicit StepPool(int n) {
+    int dev = 0;
+    SBP_CUDA(cudaGetDevice(&dev));
+    double2* logt = Context::primary().logt;
+    for (int i = 0; i < n; ++i) std::thread([this, i, dev, logt] { worker(i, dev, logt); }).detach();
+  }
+  void worker(int i, int dev, double2* logt) {
+    Context* ctx = nullptr;
+    unsigned long long seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_work_.wait(lk, [&] { return gen_ != seen; });
+        seen = gen_;
+        if (i >= active_) continue;   // not one of this round's threads
+      }
+      try {
+        if (!ctx) {
+          SBP_CUDA(cudaSetDevice(dev));
+          ctx = Context::create(logt);
+          Context::current() = ctx;
+        }
+        for (;;) {
+          const int k = next_.fetch_add(1);
+          if (k >= (int)items_->size()) break;
+          (*fn_)(*(*items_)[k]);
+          ctx->sync();
+        }
+      } catch (...) {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (!err_) err_ = std::current_exception();
+      }
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--busy_ == 0) cv_done_.notify_all();
+    }
+  }
+  std::mutex mu_;
+  std::condition_variable cv_work_, cv_done_;
+  const std::vector<Slot*>* items_ = nullptr;
+  const std::function<void(Slot&)>* fn_ = nullptr;
+  std::atomic<int> next_{0};
+  int active_ = 0, busy_ = 0;
+  unsigned long long gen_ = 0;
+  std::exception_ptr err_;
+};
+
 }  // namespace
 
 // The batched driver: per-graph state machines, one persistent launch per sweep of the
@@ -448,26 +531,46 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
 
   // The steps of one graph between two finetunes: the end of the last one, the golden-section
   // step, the merge, and the start of the next finetune (batched) or a whole single-graph one.
-  auto between = [&](Slot& s) {
+  // Runs on any host thread, on that thread's current context.
+  std::atomic<int> n_batched{0}, n_fallback{0};
+  const std::function<void(Slot&)> between = [&](Slot& s) {
     if (s.state == kEnded) end_finetune(s);
     if (s.state != kNeedMerge) return;
     const int algo = partition_merge(*s.ps, *s.g, opt, &s.fo);
     if (algo == SBP_ASYNC_GIBBS && batchable(s.ps->bm, *s.g)) {
       start_finetune(s);
-      info.batched_finetunes++;
+      n_batched++;
     } else {
       SbpStats fs;
       finetune(s.ps->bm, *s.g, algo, s.fo, nullptr, fs);
-      info.fallback_finetunes++;
+      n_fallback++;
       partition_finish_round(*s.ps, *s.g, fs, s.out);
       s.state = s.ps->done ? kDone : kNeedMerge;
     }
   };
-  // While a sweep launch runs on the primary stream, the graphs between finetunes are processed
-  // on the secondary context; they touch none of the buffers of the graphs in the launch.
-  // Buffers in the device cache carry no pending work of the primary stream: every launch
-  // follows a synchronisation of that stream with only its own set-up copies after it.
-  Context* side = g_batched_overlap > 0 ? &Context::secondary() : nullptr;
+  // The graphs between finetunes, each once: on the step pool's threads (each with its own
+  // context), or with batched_threads 1 on this thread -- beside a sweep launch on the secondary
+  // context, else on the primary one.  Beside a launch they touch none of the buffers of the
+  // graphs in it, and buffers released to the device cache carry their stream's event.
+  const int threads = g_batched_threads;
+  const bool overlap = g_batched_overlap > 0;
+  Context* side = (overlap && threads == 1) ? &Context::secondary() : nullptr;
+  auto run_between = [&](bool beside_launch) {
+    std::vector<Slot*> v;
+    for (auto& sp : slots)
+      if (sp->state == kEnded || sp->state == kNeedMerge) v.push_back(sp.get());
+    if (v.empty()) return;
+    const auto h0 = std::chrono::steady_clock::now();
+    if (threads > 1) {
+      StepPool::get().run(v, threads, between);
+    } else {
+      ContextScope scope(beside_launch ? side : nullptr);
+      for (Slot* sp : v) between(*sp);
+      if (beside_launch) side->sync();
+    }
+    (beside_launch ? info.overlapped_seconds : info.serial_seconds) +=
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - h0).count();
+  };
 
   for (;;) {
     std::vector<Slot*> act;
@@ -478,11 +581,13 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
       if (sp->state != kDone) all_done = false;
     }
     if (all_done) break;
-    if (act.empty()) {   // nothing to sweep: the graphs between finetunes, on the primary stream
-      const auto h0 = std::chrono::steady_clock::now();
-      for (auto& sp : slots) between(*sp);
-      info.serial_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - h0).count();
-      continue;
+    if (act.empty() || (waiting && !overlap)) {   // no launch to run beside: the steps first
+      run_between(false);
+      act.clear();
+      for (auto& sp : slots)
+        if (sp->state == kFinetuning) act.push_back(sp.get());
+      waiting = false;
+      if (act.empty()) continue;
     }
 
     // one sweep of every finetuning graph
@@ -532,7 +637,7 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
       std::memset(&q, 0, sizeof q);
       if (g_batched_stall_graph == s->index) q.ctr = 1ull << 20;   // stage 0, item 2^20: beyond every stage
     }
-    const int reserve = (side && waiting) ? std::min(g_batched_overlap, shape.ctas_per_sm * c.num_sms / 2) : 0;
+    const int reserve = waiting ? std::min(g_batched_overlap, shape.ctas_per_sm * c.num_sms / 2) : 0;
     const int grid = shape.ctas_per_sm * c.num_sms - reserve;
     auto ex = cl.execs.find(grid);
     if (ex == cl.execs.end()) {
@@ -560,15 +665,9 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
     ++g_launches;
     g_h2d += (long long)(n * (sizeof(BGraph) + sizeof(int) + sizeof(Queue)) + sizeof(SweepParams));
     g_d2h += (long long)(n * sizeof(double) + sizeof(int));
-    if (waiting) {
-      const auto h0 = std::chrono::steady_clock::now();
+    if (waiting) {   // beside the launch
       try {
-        ContextScope scope(side);
-        for (auto& sp : slots)
-          if (sp->state != kFinetuning) between(*sp);
-        if (side) side->sync();
-        (side ? info.overlapped_seconds : info.serial_seconds) +=
-            std::chrono::duration<double>(std::chrono::steady_clock::now() - h0).count();
+        run_between(true);
       } catch (...) {
         cudaStreamSynchronize(c.stream);   // no launch outlives the call
         throw;
@@ -614,6 +713,8 @@ static void partition_batched(std::vector<std::unique_ptr<Slot>>& slots, const S
     info.chunk = g_tuned[key].chunk;
     info.ctas_per_sm = std::min(g_tuned[key].ctas_per_sm, max_per_sm);
   }
+  info.batched_finetunes = n_batched;
+  info.fallback_finetunes = n_fallback;
   c.check_status();
 }
 

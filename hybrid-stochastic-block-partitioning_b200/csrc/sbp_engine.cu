@@ -22,7 +22,7 @@ struct SortScratch {
   DevBuf<unsigned> hist, flags, rowcnt, caps;
   DevBuf<long long> pos, heads, rowptr;
 };
-static SortScratch g_sort;
+static thread_local SortScratch g_sort;   // per host thread (the batched partitioner merges on several)
 
 static int key_bits(int B) {
   const unsigned long long maxkey = (unsigned long long)B * (unsigned long long)B;
@@ -188,8 +188,8 @@ void rebuild(SbpBlockmodel& bm, const SbpGraph& g, bool recompute_d) {
 // assignment, which already carries the batch's moves.  Rows that did not run out of room took
 // every update of the batch and stay as they are.  Costs one pass over the edges instead of a
 // full rebuild; returns false (and changes nothing) when the slot arrays have no room left.
-static DevBuf<int> g_regrow_list;
-static DevBuf<unsigned long long> g_regrow_ctr;   // [0, 1] slots taken per side, [2, 3] rows per side, [4] no room
+static thread_local DevBuf<int> g_regrow_list;
+static thread_local DevBuf<unsigned long long> g_regrow_ctr;   // [0, 1] slots taken per side, [2, 3] rows per side, [4] no room
 
 static bool regrow_hashed(SbpBlockmodel& bm, const SbpGraph& g) {
   Context& c = Context::get();
@@ -262,8 +262,16 @@ static int mh_cap(int max_k) {
   return cap;
 }
 
+// Raise a kernel's dynamic shared-memory limit to at least `bytes` (never lowers it: another host
+// thread may be about to launch the kernel with a larger request).
 void set_smem_limit(const void* fn, size_t bytes) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, size_t> limit;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = limit[fn];
+  if (bytes <= cur) return;
   SBP_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  cur = bytes;
 }
 
 // One sequential Metropolis-Hastings pass over verts (device list of n vertices).
@@ -356,10 +364,7 @@ void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, in
     SBP_CHECK_LAUNCH();
     if (g_prof.on) {
       SBP_CUDA(cudaEventRecord(e1, c.stream));
-      g_prof.pending.push_back({e0, e1});
-      g_prof.launches++;
-      g_prof.visits += nl;
-      g_prof.bytes += plan.light_bytes[bt];
+      g_prof.add(e0, e1, nl, plan.light_bytes[bt]);
     }
   }
   if (nh > 0) {
@@ -412,7 +417,7 @@ void gibbs_apply(SbpBlockmodel& bm, const SbpGraph& g, int batch) {
 // whose last CTA applies the early stop on the GPU and sets the loop condition).
 // Same kernels, same order and the same early-stop arithmetic as the host loop, so the chain
 // and the sweep count are the host loop's.  Returns the sweeps run.
-static DevBuf<SweepCtl> g_ctl;
+static thread_local DevBuf<SweepCtl> g_ctl;
 
 static int gibbs_sweeps_graph(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, RngParams rng,
                               int max_sweeps, bool bracket, double initial_entropy) {
@@ -1143,6 +1148,9 @@ SbpStatus sbp_set_option(const char* name, int64_t value) {
   } else if (n == "batched_stall_graph") {
     SBP_REQUIRE(value >= -1 && value < (1LL << 30), "batched_stall_graph must be -1 or a graph index");
     g_batched_stall_graph = (int)value;
+  } else if (n == "batched_threads") {
+    SBP_REQUIRE(value >= 1 && value <= 64, "batched_threads must be in [1, 64]");
+    g_batched_threads = (int)value;
   } else if (n == "batched_overlap") {
     SBP_REQUIRE(value >= 0 && value <= 1024, "batched_overlap must be in [0, 1024]");
     g_batched_overlap = (int)value;

@@ -2,6 +2,8 @@
 // (sbp_engine.cu: graph, blockmodel, finetune, merge, partition and the C ABI;
 // sbp_learned.cu: the learned proposal).  Not part of the public C ABI.
 #pragma once
+#include <atomic>
+#include <condition_variable>
 #include <functional>
 #include <map>
 #include <algorithm>
@@ -9,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -41,8 +44,9 @@ struct Error : std::runtime_error {
     }                                                                                                   \
   } while (0)
 
-inline long long g_launches = 0;   // kernels launched by this library (all entry points)
-inline long long g_h2d = 0, g_d2h = 0;   // bytes copied host->device / device->host
+// Counters shared by every host thread that calls the library.
+inline std::atomic<long long> g_launches{0};   // kernels launched by this library (all entry points)
+inline std::atomic<long long> g_h2d{0}, g_d2h{0};   // bytes copied host->device / device->host
 
 #define SBP_CHECK_LAUNCH() \
   do {                     \
@@ -74,50 +78,116 @@ inline size_t device_memory_bytes() {
 
 // Released device buffers are kept for reuse instead of being freed: cudaFree synchronizes
 // the whole device, and every partition round releases and reallocates its blockmodel's
-// buffers.  A reused buffer is handed out only after the engine's stream has drained, so no
-// queued kernel still reads it.  At most kDeviceCacheBytes stay cached.
+// buffers.  A released buffer carries an event recorded on the releasing thread's stream, and
+// it is handed out again only after that event has completed, so no queued kernel of any
+// stream still uses it.  Thread-safe.  At most kDeviceCacheBytes stay cached.
 cudaStream_t engine_stream();
 
 struct DeviceCache {
   static constexpr size_t kDeviceCacheBytes = 32ull << 30;
-  std::multimap<size_t, void*> blocks;   // bytes -> buffer
+  struct Block {
+    void* p;
+    cudaEvent_t released;   // null: released while its stream was being captured (wait for the stream)
+  };
+  std::multimap<size_t, Block> blocks;   // bytes -> buffer
+  std::vector<cudaEvent_t> spare;        // events for reuse
   size_t cached = 0;
+  std::mutex mu;
   static DeviceCache& get() {
     static DeviceCache* c = new DeviceCache();   // never destroyed: buffers live until exit
     return *c;
   }
+  static void wait(const Block& b) {
+    SBP_CUDA(b.released ? cudaEventSynchronize(b.released) : cudaStreamSynchronize(engine_stream()));
+  }
   void* take(size_t bytes, size_t* got) {
-    auto it = blocks.lower_bound(bytes);
-    if (it != blocks.end() && it->first <= bytes + bytes / 4 + (1u << 20)) {
-      void* p = it->second;
-      *got = it->first;
-      cached -= it->first;
-      blocks.erase(it);
-      SBP_CUDA(cudaStreamSynchronize(engine_stream()));
-      return p;
+    Block b{nullptr, nullptr};
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      auto it = blocks.lower_bound(bytes);
+      if (it != blocks.end() && it->first <= bytes + bytes / 4 + (1u << 20)) {
+        b = it->second;
+        *got = it->first;
+        cached -= it->first;
+        blocks.erase(it);
+      }
+    }
+    if (b.p) {
+      wait(b);
+      recycle(b.released);
+      return b.p;
     }
     void* p = nullptr;
     cudaError_t e = cudaMalloc(&p, bytes);
-    if (e == cudaErrorMemoryAllocation && !blocks.empty()) {   // give the cache back and retry
+    if (e == cudaErrorMemoryAllocation) {   // give the cache back and retry
       cudaGetLastError();
-      SBP_CUDA(cudaStreamSynchronize(engine_stream()));
-      for (auto& kv : blocks) cudaFree(kv.second);
-      blocks.clear();
-      cached = 0;
-      e = cudaMalloc(&p, bytes);
+      std::multimap<size_t, Block> all;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        all.swap(blocks);
+        cached = 0;
+      }
+      for (auto& kv : all) {
+        wait(kv.second);
+        cudaFree(kv.second.p);
+        recycle(kv.second.released);
+      }
+      if (!all.empty()) e = cudaMalloc(&p, bytes);
     }
     if (e == cudaErrorMemoryAllocation) throw Error(SBP_ERR_OUT_OF_MEMORY, "cudaMalloc: out of device memory");
     SBP_CUDA(e);
     *got = bytes;
     return p;
   }
-  void give(void* p, size_t bytes) {
-    if (cached + bytes > kDeviceCacheBytes) {
-      cudaFree(p);
-      return;
+  // Called from destructors: never throws.
+  void give(void* p, size_t bytes) noexcept {
+    cudaEvent_t ev = nullptr;
+    try {
+      const cudaStream_t st = engine_stream();
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+        ev = event();
+        if (ev && cudaEventRecord(ev, st) != cudaSuccess) {
+          cudaGetLastError();
+          cudaStreamSynchronize(st);
+          recycle(ev);
+          ev = nullptr;
+        }
+      }
+    } catch (...) {
+      ev = nullptr;
     }
-    blocks.emplace(bytes, p);
-    cached += bytes;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (cached + bytes <= kDeviceCacheBytes) {
+        blocks.emplace(bytes, Block{p, ev});
+        cached += bytes;
+        return;
+      }
+    }
+    cudaFree(p);   // synchronizes the device first
+    recycle(ev);
+  }
+  cudaEvent_t event() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (!spare.empty()) {
+        cudaEvent_t e = spare.back();
+        spare.pop_back();
+        return e;
+      }
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return e;
+  }
+  void recycle(cudaEvent_t e) {
+    if (!e) return;
+    std::lock_guard<std::mutex> lk(mu);
+    spare.push_back(e);
   }
 };
 
@@ -270,11 +340,20 @@ struct ContextScope {
 // evaluation launch on the launching stream, resolved when the profile is read.
 struct EvalProfiler {
   bool on = false;
+  std::mutex mu;   // launches may come from several host threads (the batched partitioner's merges)
   std::vector<cudaEvent_t> pool;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
   double ms = 0.0, bytes = 0.0;
   long long launches = 0, visits = 0;
+  void add(cudaEvent_t e0, cudaEvent_t e1, long long n, double b) {
+    std::lock_guard<std::mutex> lk(mu);
+    pending.push_back({e0, e1});
+    launches++;
+    visits += n;
+    bytes += b;
+  }
   cudaEvent_t get() {
+    std::lock_guard<std::mutex> lk(mu);
     if (!pool.empty()) {
       cudaEvent_t e = pool.back();
       pool.pop_back();
@@ -285,6 +364,7 @@ struct EvalProfiler {
     return e;
   }
   void resolve() {
+    std::lock_guard<std::mutex> lk(mu);
     for (auto& pr : pending) {
       SBP_CUDA(cudaEventSynchronize(pr.second));
       float t = 0.f;
@@ -327,7 +407,7 @@ inline int g_hashed_row_factor = 4;
 // 1: an asynchronous-Gibbs finetune on dense storage runs as one CUDA graph launch with the
 // sweep loop decided on the GPU; 0: one host-driven launch sequence per sweep (sbp_set_option).
 inline int g_graph_sweeps = 1;
-inline long long g_overflow_rebuilds = 0;   // rebuilds forced by a full hashed row
+inline thread_local long long g_overflow_rebuilds = 0;   // rebuilds forced by a full hashed row (calling thread)
 // Light vertices of dense blockmodels (sbp_set_option "group_kernel"): 1 (default) evaluated by the
 // group kernels (sbp_eval_small.cu) when B <= kSmallB (direct-indexed group tables), by the warp-
 // per-vertex kernels above; 2 by the group kernels at every B (hashed group tables above kSmallB:
@@ -342,6 +422,9 @@ inline int g_batched_stall_graph = -1;
 // CTA slots the batched sweep kernel leaves free while the merges of the graphs between two
 // finetunes run beside it on the secondary context (0: merges run after each sweep launch).
 inline int g_batched_overlap = 64;
+// Host threads (each with its own context) that run the steps between finetunes of several
+// graphs of a batched partition at once; 1: the calling thread alone.
+inline int g_batched_threads = 8;
 
 }  // namespace sbpb
 
@@ -545,6 +628,8 @@ inline bool use_group_kernel(const SbpBlockmodel& bm) {
   return !bm.sparse && (g_group_kernel == 2 || (g_group_kernel == 1 && bm.B <= kSmallB));
 }
 
+void set_smem_limit(const void* fn, size_t bytes);
+
 // Launch of the group kernel over n light vertices (dense storage); with hashed group tables
 // (B > kSmallB) every vertex must have k <= kGroupMaxK.
 inline void launch_group_eval(const SbpGraph& g, SbpBlockmodel& bm, const int* verts, int n, const RngParams& rng,
@@ -554,11 +639,7 @@ inline void launch_group_eval(const SbpGraph& g, SbpBlockmodel& bm, const int* v
   const int cap = std::min(g.light_cap, 2 * kGroupMaxK);
   const size_t smem = gibbs_eval_group_smem(hashed_table, cap);
   const GibbsEvalGroupKernel k = gibbs_eval_group_kernel(hashed_table);
-  static size_t set_for[2] = {0, 0};
-  if (set_for[hashed_table] < smem) {
-    SBP_CUDA(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    set_for[hashed_table] = smem;
-  }
+  set_smem_limit((const void*)k, smem);
   k<<<grid_for(n, kSmallThreads / kSmallGroup, 64 * c.num_sms), kSmallThreads, smem, stream>>>(
       g.view(), bm.view(), verts, n, rng, sweep, bm.prop.p, bm.moved.p, n_moved, c.counters, cap, c.status, ctl,
       batch);
@@ -673,8 +754,8 @@ struct PartitionState {
 
 // Process-wide finetune counters (finetune::MCMC_iterations / MCMC_time, src/finetune.cpp:15-16)
 // and intermediate records of partitions (sbp::intermediate_results, src/sbp.cpp:16-20).
-inline long long g_mcmc_iterations = 0;
-inline double g_mcmc_time = 0.0;
+inline thread_local long long g_mcmc_iterations = 0;   // the calling thread's finetune sweeps so far
+inline thread_local double g_mcmc_time = 0.0;
 inline std::vector<SbpIntermediate> g_intermediates;
 // Record one intermediate of a partition in progress (modularity only when asked: the reference
 // computes it for the final record alone).

@@ -126,7 +126,9 @@ int32_t sbp_device_count(void);
  * (default 64, range 0-1024): while a sweep launch of sbp_partition_batched runs, the graphs
  * between two finetunes (merge, golden-section step, the next finetune's set-up) are processed
  * on a second stream, and the launch leaves this many CTA slots free for their kernels; 0 runs
- * them after each launch instead (same results either way). */
+ * them before the next launch instead (same results either way).  "batched_threads" (default 8,
+ * range 1-64): host threads, each with its own stream and scratch, that run those steps for
+ * several graphs at once; 1: the calling thread alone. */
 SbpStatus sbp_set_option(const char *name, int64_t value);
 
 /* The CUDA stream every call of this library runs on (cudaStream_t), for interop and timing.

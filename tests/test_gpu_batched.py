@@ -127,21 +127,26 @@ def test_batched_wait_runs_out_and_the_library_stays_usable(S):
         assert np.array_equal(out, single)
 
 
-@pytest.mark.parametrize("overlap", [0, 16, 1024])
-def test_batched_overlapped_merges_are_identical(S, overlap):
-    """The graphs between finetunes are processed on a second stream while a sweep launch runs
-    (sbp_set_option "batched_overlap" = CTA slots left free for them; 1024 leaves half the grid,
-    0 runs them after the launch): the partitions are the single-graph ones either way,
-    including rounds on row-hashed storage with the single-graph finetune."""
+@pytest.mark.parametrize("overlap,threads", [(0, 1), (16, 1), (1024, 1), (0, 8), (64, 8), (64, 3)])
+def test_batched_overlapped_merges_are_identical(S, overlap, threads):
+    """The graphs between finetunes are processed while a sweep launch runs (sbp_set_option
+    "batched_overlap" = CTA slots left free for them; 1024 leaves half the grid, 0 runs them
+    before the next launch instead), on a pool of host threads with a context each
+    ("batched_threads"; 1: the calling thread on a second context): the partitions are the
+    single-graph ones either way, including rounds on row-hashed storage with the single-graph
+    finetune."""
     specs = uneven_graphs(500, [700, 2100, 350, 1500, 900, 3000, 1200, 500])
     graphs = [S.Graph(V, s, d) for V, s, d, _ in specs]
     S.set_option("batched_overlap", overlap)
+    S.set_option("batched_threads", threads)
     S.set_option("dense_max_blocks", 256)
     try:
         outs, stats, info = S.batched.stochastic_block_partition(graphs, batches=10, seed=21)
         assert info["batched_finetunes"] > 0 and info["fallback_finetunes"] > 0
+        assert info["serial_seconds"] > 0 and (overlap == 0) == (info["overlapped_seconds"] == 0)
         for g, out, st in zip(graphs, outs, stats):
             assert_same(out, st, *single(S, g, 21))
     finally:
         S.set_option("dense_max_blocks", 65536)
         S.set_option("batched_overlap", 64)
+        S.set_option("batched_threads", 8)
