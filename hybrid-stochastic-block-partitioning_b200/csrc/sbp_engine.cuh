@@ -400,8 +400,8 @@ constexpr int kSmemRebuildMaxB = 100;
 
 // Blocks above which the block matrix is row-hashed instead of dense, and the largest share of the
 // free device memory (percent) a dense matrix may take (sbp_set_option).
-inline int g_dense_max_blocks = 65536;
-inline int g_dense_max_memory_pct = 40;
+inline int g_dense_max_blocks = 131072;
+inline int g_dense_max_memory_pct = 60;
 // Hashed row capacity = power of two >= factor * (cells after a rebuild) + 4 * factor.
 inline int g_hashed_row_factor = 4;
 // 1: an asynchronous-Gibbs finetune on dense storage runs as one CUDA graph launch with the
@@ -587,7 +587,7 @@ struct SbpBlockmodel {
     B = nb;
     sparse = B > g_dense_max_blocks;
     const double dense_bytes = 2.0 * (double)B * (double)(((B + kChunk - 1) / kChunk) * kChunk) * sizeof(int);
-    // dense only while it takes at most 40 % of the free device memory; cudaMemGetInfo can
+    // dense only while it takes at most 60 % of the free device memory; cudaMemGetInfo can
     // stall the host for tens of milliseconds, so it is asked only for a matrix above 5 % of
     // the device's memory
     if (!sparse && dense_bytes > 0.05 * (double)device_memory_bytes()) {

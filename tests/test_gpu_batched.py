@@ -83,7 +83,7 @@ def test_batched_fallback_rounds_are_identical(S):
             out_s, st_s = S.sbp.stochastic_block_partition(g, algorithm="async_gibbs", batches=8, seed=11)
             assert_same(out, st, out_s, st_s)
     finally:
-        S.set_option("dense_max_blocks", 65536)
+        S.set_option("dense_max_blocks", 131072)
 
 
 def test_batched_other_algorithms_fall_back(S):
@@ -147,6 +147,6 @@ def test_batched_overlapped_merges_are_identical(S, overlap, threads):
         for g, out, st in zip(graphs, outs, stats):
             assert_same(out, st, *single(S, g, 21))
     finally:
-        S.set_option("dense_max_blocks", 65536)
+        S.set_option("dense_max_blocks", 131072)
         S.set_option("batched_overlap", 64)
         S.set_option("batched_threads", 8)

@@ -16,9 +16,9 @@ RTOL_MDL = 1e-9
 @pytest.fixture(params=["dense", "hashed"])
 def storage(request, S):
     """Run the test with dense B x B counts and again with the row-hashed block matrix."""
-    S.set_option("dense_max_blocks", 65536 if request.param == "dense" else 1)
+    S.set_option("dense_max_blocks", 131072 if request.param == "dense" else 1)
     yield request.param
-    S.set_option("dense_max_blocks", 65536)
+    S.set_option("dense_max_blocks", 131072)
 
 
 def pair(S, O, V, s, d, B, a):
@@ -248,7 +248,7 @@ def test_hashed_rows_grow_and_stay_exact(S, O):
             total += st["overflow_rebuilds"]
         assert total > 0, "the test no longer drives the rows past their capacity"
     finally:
-        S.set_option("dense_max_blocks", 65536)
+        S.set_option("dense_max_blocks", 131072)
         S.set_option("hashed_row_factor", 4)
 
 

@@ -27,9 +27,9 @@ def cfg2():
 
 @pytest.fixture(params=["dense", "hashed"])
 def storage(request, S):
-    S.set_option("dense_max_blocks", 65536 if request.param == "dense" else 1)
+    S.set_option("dense_max_blocks", 131072 if request.param == "dense" else 1)
     yield request.param
-    S.set_option("dense_max_blocks", 65536)
+    S.set_option("dense_max_blocks", 131072)
 
 
 def perturbed(truth, frac, seed, K=None):
@@ -123,5 +123,5 @@ def test_hashed_rows_overflow_again_and_again_at_20k(S, O, cfg2):
             total += st["overflow_rebuilds"]
         assert total >= 3, "the rows no longer overflow repeatedly"
     finally:
-        S.set_option("dense_max_blocks", 65536)
+        S.set_option("dense_max_blocks", 131072)
         S.set_option("hashed_row_factor", 4)
