@@ -1098,6 +1098,12 @@ SbpStatus sbp_get_stream(void** out) {
   SBP_API_END
 }
 
+SbpStatus sbp_release_cached_memory(void) {
+  SBP_API_BEGIN
+  DeviceCache::get().release_all();
+  SBP_API_END
+}
+
 SbpStatus sbp_profile_enable(int32_t on) {
   SBP_API_BEGIN
   Context::get();

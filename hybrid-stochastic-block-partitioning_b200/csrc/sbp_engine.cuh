@@ -80,11 +80,17 @@ inline size_t device_memory_bytes() {
 // the whole device, and every partition round releases and reallocates its blockmodel's
 // buffers.  A released buffer carries an event recorded on the releasing thread's stream, and
 // it is handed out again only after that event has completed, so no queued kernel of any
-// stream still uses it.  Thread-safe.  At most kDeviceCacheBytes stay cached.
+// stream still uses it.  Thread-safe.
 cudaStream_t engine_stream();
 
 struct DeviceCache {
-  static constexpr size_t kDeviceCacheBytes = 32ull << 30;
+  // at most half the device's memory (at least 32 GB) stays cached: the dense block matrix of a
+  // 100,000-block finetune (two 40 GB buffers) is reused by the next partition instead of being
+  // freed and allocated again
+  static size_t cap_bytes() {
+    static const size_t cap = std::max<size_t>(32ull << 30, device_memory_bytes() / 2);
+    return cap;
+  }
   struct Block {
     void* p;
     cudaEvent_t released;   // null: released while its stream was being captured (wait for the stream)
@@ -159,7 +165,7 @@ struct DeviceCache {
     }
     {
       std::lock_guard<std::mutex> lk(mu);
-      if (cached + bytes <= kDeviceCacheBytes) {
+      if (cached + bytes <= cap_bytes()) {
         blocks.emplace(bytes, Block{p, ev});
         cached += bytes;
         return;
@@ -167,6 +173,20 @@ struct DeviceCache {
     }
     cudaFree(p);   // synchronizes the device first
     recycle(ev);
+  }
+  // Free every cached buffer (after the work that released it).
+  void release_all() {
+    std::multimap<size_t, Block> all;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      all.swap(blocks);
+      cached = 0;
+    }
+    for (auto& kv : all) {
+      wait(kv.second);
+      cudaFree(kv.second.p);
+      recycle(kv.second.released);
+    }
   }
   cudaEvent_t event() {
     {

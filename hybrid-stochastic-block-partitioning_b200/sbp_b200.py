@@ -24,7 +24,8 @@ STATUS = {0: "SBP_OK", 1: "SBP_ERR_INVALID_ARGUMENT", 2: "SBP_ERR_CUDA", 3: "SBP
           4: "SBP_ERR_REPLAY", 5: "SBP_ERR_DEVICE", 6: "SBP_ERR_OUT_OF_MEMORY"}
 
 EXPORTED = [
-    "sbp_last_error", "sbp_device_count", "sbp_set_option", "sbp_get_stream", "sbp_profile_enable", "sbp_profile_read",
+    "sbp_last_error", "sbp_device_count", "sbp_set_option", "sbp_get_stream", "sbp_release_cached_memory",
+    "sbp_profile_enable", "sbp_profile_read",
     "sbp_graph_create", "sbp_graph_destroy", "sbp_graph_num_edges",
     "sbp_graph_get_split", "sbp_graph_set_split", "sbp_blockmodel_create", "sbp_blockmodel_copy",
     "sbp_blockmodel_destroy", "sbp_blockmodel_num_blocks", "sbp_blockmodel_set_num_blocks_to_merge",
@@ -259,6 +260,11 @@ def device_count():
 def set_option(name, value):
     """Engine option, e.g. set_option("dense_max_blocks", 65536) (include/sbp_b200.h lists them)."""
     _check(load().sbp_set_option(name.encode(), int(value)))
+
+
+def release_cached_memory():
+    """Free the device buffers the library keeps cached for reuse."""
+    _check(load().sbp_release_cached_memory())
 
 
 def stream_handle():

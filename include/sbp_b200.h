@@ -134,6 +134,11 @@ SbpStatus sbp_set_option(const char *name, int64_t value);
 /* The CUDA stream every call of this library runs on (cudaStream_t), for interop and timing.
  * No reference counterpart (the reference is CPU-only). */
 SbpStatus sbp_get_stream(void **out);
+
+/* Released device buffers stay cached for reuse (up to half the device's memory, at least 32 GB;
+ * a new allocation that does not fit frees them first).  This frees them now, once the work that
+ * used them has finished.  No reference counterpart. */
+SbpStatus sbp_release_cached_memory(void);
 /* Enable CUDA-event timing of the vertex-evaluation kernel launches (off by default), and read
  * the counters.  No reference counterpart. */
 SbpStatus sbp_profile_enable(int32_t on);
