@@ -111,9 +111,12 @@ int32_t sbp_device_count(void);
 /* Engine options (no reference counterpart).  "dense_max_blocks": blockmodels with more blocks
  * than this keep their block matrix as row-hashed regions (a sparse device-resident matrix with
  * integer counts updated by atomics) instead of dense B x B arrays; default 131072 (dense storage
- * is faster wherever it fits; it also falls back to row-hashed when the dense matrix would take
- * more than dense_max_memory_pct, default 60, percent of the free device memory).  Applies to blockmodels whose block count is set
- * after the call.  "hashed_row_factor" (default 4, range 2-64): a rebuilt hashed row gets room
+ * is faster wherever it fits).  "dense_max_memory_pct" (default 60, range 1-90): a dense matrix
+ * that would take more than this percentage of the free device memory is row-hashed instead.
+ * Both apply to blockmodels whose block count is set after the call.  "group_kernel" (default
+ * 1): asynchronous-Gibbs and Metropolis-Hastings evaluation with a group of 8 lanes per vertex
+ * on dense blockmodels of at most 128 blocks; 2: at every block count (vertices of degree up to
+ * 128); 0: one warp per vertex everywhere (same results).  "hashed_row_factor" (default 4, range 2-64): a rebuilt hashed row gets room
  * for factor x its cells, at most 2 x for rows of more than 128 cells (larger: rows fill up and
  * are regrown less often; smaller: less memory and a cheaper walk of the row).  "graph_sweeps" (default 1): an
  * asynchronous-Gibbs finetune on dense storage runs as one CUDA graph launch whose sweep loop and

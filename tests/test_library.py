@@ -64,3 +64,27 @@ def test_batched_configs():
     assert min(sizes) >= 1000 and max(sizes) <= 50000
     c = dcsbm.batched_config(0)
     assert c["K"] == round(1.2 * c["V"] ** 0.35)
+
+
+def test_engine_options_are_checked_on_the_host():
+    """sbp_set_option validates names and ranges without a device; every option documented in
+    the header is accepted at its default."""
+    import sbp_b200 as S
+    defaults = {"dense_max_blocks": 131072, "dense_max_memory_pct": 60, "hashed_row_factor": 4, "graph_sweeps": 1,
+                "group_kernel": 1, "batched_wait_limit": 1 << 22, "batched_stall_graph": -1,
+                "batched_overlap": 64, "batched_threads": 8}
+    header = open(os.path.join(ROOT, "include", "sbp_b200.h")).read()
+    for name, value in defaults.items():
+        assert f'"{name}"' in header, name
+        S.set_option(name, value)
+    for name, bad in (("batched_threads", 0), ("batched_threads", 65), ("batched_overlap", -1),
+                      ("group_kernel", 3), ("dense_max_memory_pct", 91), ("no_such_option", 1)):
+        with pytest.raises(S.SbpError) as e:
+            S.set_option(name, bad)
+        assert e.value.code == 1
+        assert name in S.last_error() or "option" in S.last_error()
+
+
+def test_release_cached_memory_needs_no_device():
+    import sbp_b200 as S
+    S.release_cached_memory()   # nothing cached: no CUDA call
