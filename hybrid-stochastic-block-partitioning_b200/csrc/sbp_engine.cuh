@@ -174,6 +174,10 @@ struct DeviceCache {
     cudaFree(p);   // synchronizes the device first
     recycle(ev);
   }
+  size_t cached_bytes() {
+    std::lock_guard<std::mutex> lk(mu);
+    return cached;
+  }
   // Free every cached buffer (after the work that released it).
   void release_all() {
     std::multimap<size_t, Block> all;
@@ -613,7 +617,9 @@ struct SbpBlockmodel {
     if (!sparse && dense_bytes > 0.05 * (double)device_memory_bytes()) {
       size_t free_b = 0, total_b = 0;
       if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-        const size_t have = M.n * sizeof(int) * 2;   // a buffer this blockmodel already holds counts as free
+        // buffers this blockmodel already holds, and those the device cache keeps for reuse,
+        // count as free
+        const size_t have = M.n * sizeof(int) * 2 + DeviceCache::get().cached_bytes();
         if (dense_bytes > 0.01 * g_dense_max_memory_pct * (double)(free_b + have)) sparse = true;
       } else {
         cudaGetLastError();
