@@ -314,41 +314,55 @@ __device__ __forceinline__ int select_in_chunk(int4 q, int chunk, long long targ
 // round trip instead of one per 32 chunks), scans its lane total across the warp and walks its
 // sixteen sums; longer rows take 32 chunks per step.
 constexpr int kWideChunks = 16 * kWarp;
+// Rows of up to kWideChunks chunks: load the chunk sums of row t of M and of MT in the round trip
+// of t's degrees (before the walk knows which one it needs) instead of after it.
+#ifndef SBP_CHUNK_SUMS_WITH_DEGREES
+#define SBP_CHUNK_SUMS_WITH_DEGREES 0
+#endif
+constexpr bool kChunkSumsWithDegrees = SBP_CHUNK_SUMS_WITH_DEGREES != 0;
+// The wide walk over chunk sums already loaded: lane i holds the sums of chunks [16 i, 16 i + 16)
+// (0 beyond the row).
+__device__ __forceinline__ int walk_loaded_chunk_sums(const int* row, const int (&cs)[16], long long target,
+                                                      int lane) {
+  long long lsum = 0;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) lsum += cs[q];
+  const long long incl = warp_incl_scan(lsum, lane);
+  const unsigned hit = __ballot_sync(kFull, incl > target);
+  if (!hit) return -1;
+  const int src = __ffs(hit) - 1;
+  int chunk = -1;
+  long long before = 0;
+  if (lane == src) {
+    long long run = incl - lsum;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      if (chunk < 0) {
+        if (target < run + cs[q]) {
+          chunk = lane * 16 + q;
+          before = run;
+        } else {
+          run += cs[q];
+        }
+      }
+    }
+  }
+  chunk = __shfl_sync(kFull, chunk, src);
+  before = __shfl_sync(kFull, before, src);
+  const int4 q4 = *reinterpret_cast<const int4*>(row + chunk * kChunk + 4 * lane);
+  return select_in_chunk(q4, chunk, target - before, lane);
+}
+
 __device__ __forceinline__ int warp_select_chunked(const int* row, const int* csum, int nch, long long target,
                                                    int lane) {
   if (nch <= kWideChunks) {
     int cs[16];
-    long long lsum = 0;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
       const int c = lane * 16 + q;
       cs[q] = c < nch ? csum[c] : 0;
-      lsum += cs[q];
     }
-    const long long incl = warp_incl_scan(lsum, lane);
-    const unsigned hit = __ballot_sync(kFull, incl > target);
-    if (!hit) return -1;
-    const int src = __ffs(hit) - 1;
-    int chunk = -1;
-    long long before = 0;
-    if (lane == src) {
-      long long run = incl - lsum;
-#pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        if (chunk < 0) {
-          if (target < run + cs[q]) {
-            chunk = lane * 16 + q;
-            before = run;
-          } else {
-            run += cs[q];
-          }
-        }
-      }
-    }
-    chunk = __shfl_sync(kFull, chunk, src);
-    before = __shfl_sync(kFull, before, src);
-    const int4 q4 = *reinterpret_cast<const int4*>(row + chunk * kChunk + 4 * lane);
-    return select_in_chunk(q4, chunk, target - before, lane);
+    return walk_loaded_chunk_sums(row, cs, target, lane);
   }
   int chunk = -1;
   for (int base = 0; base < nch; base += kWarp) {
@@ -840,6 +854,16 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
       const size_t ro = (size_t)tblk * bm.ld, co = (size_t)tblk * bm.nch;
       int4 qa = make_int4(0, 0, 0, 0), qb = make_int4(0, 0, 0, 0);
       int ca = 0, cb = 0;
+      int wa[16], wb[16];
+      const bool wide = kChunkSumsWithDegrees && bm.nch > kWarp && bm.nch <= kWideChunks;
+      if (wide) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int c = lane * 16 + q;
+          wa[q] = c < bm.nch ? ldi<ST>(bm.CS + co + c) : 0;
+          wb[q] = c < bm.nch ? ldi<ST>(bm.CST + co + c) : 0;
+        }
+      }
       if (bm.nch == 1) {
         if constexpr (ST == Store::kDenseFrozen) {
           qa = __ldg(reinterpret_cast<const int4*>(bm.M + ro) + lane);
@@ -857,7 +881,12 @@ __device__ __forceinline__ EvalResult evaluate_vertex(const GraphView& g, const 
       const long long tg = in_row ? target : target - dot;
       if (bm.nch == 1) s = select_in_chunk(in_row ? qa : qb, 0, tg, lane);
       else if (bm.nch <= kWarp) s = select_chunk_then_column(in_row ? bm.M + ro : bm.MT + ro, in_row ? ca : cb, tg, lane);
-      else s = warp_select_chunked(in_row ? bm.M + ro : bm.MT + ro, in_row ? bm.CS + co : bm.CST + co, bm.nch, tg, lane);
+      else if (wide) {
+        int w[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) w[q] = in_row ? wa[q] : wb[q];
+        s = walk_loaded_chunk_sums(in_row ? bm.M + ro : bm.MT + ro, w, tg, lane);
+      } else s = warp_select_chunked(in_row ? bm.M + ro : bm.MT + ro, in_row ? bm.CS + co : bm.CST + co, bm.nch, tg, lane);
     } else {
       s = -1;
     }
