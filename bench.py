@@ -364,7 +364,8 @@ def main():
         K = int(truth.max()) + 1
         ref_config = dict(config, step="one reference finetune::asynchronous_gibbs call capped at 1 sweep (batches "
                           f"{a.batches}, --transpose) at B = the step's level of the partition's halving schedule "
-                          "(V/2, V/4, ... the planted B), from the planted partition split into B/K sub-blocks",
+                          "(V/2, V/4, ... the planted B, taken in spread order: V/2, then the middle level, ...), "
+                          "from the planted partition split into B/K sub-blocks",
                           sweep_driver="reference host loop (OpenMP, every host core)",
                           l2="not applicable (host CPU; each step reloads the graph in a fresh process)")
         if not rb.capped_built():
@@ -374,6 +375,7 @@ def main():
             for _ in range(a.warmup):   # untimed: one capped sweep at the planted B
                 rb.time_reference_level(V, src, dst, truth, K, a.batches)
             levels = rb.halving_levels(V, K)
+            levels = [levels[i] for i in rb.spread_order(len(levels))]
             visits, secs, used = 0, 0.0, []
             for k in range(a.steps):
                 r = rb.time_reference_level(V, src, dst, truth, levels[k % len(levels)], a.batches)

@@ -319,6 +319,20 @@ def halving_levels(V, K):
     return levels + [K]
 
 
+def spread_order(n):
+    """0..n-1 in van der Corput order (0, n/2, n/4, 3n/4, ...): every prefix samples the whole
+    range evenly, so a sample of the halving levels cut short by a time budget is not biased
+    towards the largest or the smallest block counts."""
+    out, seen = [], set()
+    bits = max(1, (n - 1).bit_length())
+    for i in range(1 << bits):
+        j = int(format(i, f"0{bits}b")[::-1], 2)
+        if j < n and j not in seen:
+            seen.add(j)
+            out.append(j)
+    return out
+
+
 def time_reference_level(V, src, dst, truth, B, batches=10, threads=None, algo="async_gibbs"):
     """One capped (1-sweep) reference finetune call at about B blocks: the planted partition split
     into B / K sub-blocks per block."""
@@ -331,10 +345,13 @@ def time_reference_level(V, src, dst, truth, B, batches=10, threads=None, algo="
 
 def time_reference(V, src, dst, truth, budget_s=20.0, batches=10, threads=None):
     """Vertex visits/s of the reference's asynchronous Gibbs on every host core, over 1-sweep
-    calls at the partition's block-count levels (halving_levels), taken from the smallest B up
-    until `budget_s` of sweep time: the bounded CPU baseline."""
+    calls at the partition's block-count levels (halving_levels) in spread order, until
+    `budget_s` of sweep time: the bounded CPU baseline.  Every level of the partition's first
+    descent runs the same number of sweeps, so visits over seconds across evenly spread levels
+    estimates the whole descent's rate."""
     K = int(truth.max()) + 1
-    levels = halving_levels(V, K)[::-1]
+    all_levels = halving_levels(V, K)
+    levels = [all_levels[i] for i in spread_order(len(all_levels))]
     visits, secs, done = 0, 0.0, []
     for B in levels:
         r = time_reference_level(V, src, dst, truth, B, batches, threads)
@@ -346,7 +363,7 @@ def time_reference(V, src, dst, truth, budget_s=20.0, batches=10, threads=None):
     return {"value": visits / secs, "unit": "vertex visits/s", "cores": threads or os.cpu_count(), "kind": "reference",
             "sample": f"reference finetune::asynchronous_gibbs (batches {batches}, --transpose; the build's only change "
                       f"is a sweep cap) for 1 sweep at each of B = {done} (the planted partition split into B/K "
-                      f"sub-blocks; the partition's halving schedule from the planted K upwards): {visits} visits "
+                      f"sub-blocks; levels of the partition's halving schedule in spread order): {visits} visits "
                       f"in {secs:.2f} s"}
 
 
