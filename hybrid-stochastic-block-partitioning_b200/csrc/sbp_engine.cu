@@ -24,6 +24,48 @@ struct SortScratch {
 };
 static thread_local SortScratch g_sort;   // per host thread (the batched partitioner merges on several)
 
+// 0..n-1 ordered by key ascending, equal keys by index: the order of std::stable_sort on the
+// indices with `key[a] < key[b]`, from an LSD radix sort (16-bit digits) of order-preserving
+// 64-bit images of the keys (-0.0 taken as +0.0, which compares equal).  With a NaN key (no
+// strict weak order) it is std::stable_sort itself.  A 200,000-key sort takes a few ms instead
+// of about 20.
+static std::vector<int> stable_order_by(const std::vector<double>& key) {
+  const size_t n = key.size();
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::vector<unsigned long long> img(n);
+  for (size_t i = 0; i < n; ++i) {
+    double x = key[i];
+    if (std::isnan(x)) {
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
+      return order;
+    }
+    if (x == 0.0) x = 0.0;
+    unsigned long long bits;
+    std::memcpy(&bits, &x, sizeof bits);
+    img[i] = (bits >> 63) ? ~bits : (bits | (1ull << 63));
+  }
+  std::vector<int> tmp(n);
+  std::vector<unsigned> count(1u << 16);
+  for (int shift = 0; shift < 64; shift += 16) {
+    std::fill(count.begin(), count.end(), 0u);
+    for (size_t i = 0; i < n; ++i) count[(img[i] >> shift) & 0xffff]++;
+    if (n > 0 && count[(img[0] >> shift) & 0xffff] == n) continue;   // one digit value: order unchanged
+    unsigned run = 0;
+    for (auto& c : count) {
+      const unsigned k = c;
+      c = run;
+      run += k;
+    }
+    for (size_t i = 0; i < n; ++i) {
+      const int o = order[i];
+      tmp[count[(img[o] >> shift) & 0xffff]++] = o;
+    }
+    order.swap(tmp);
+  }
+  return order;
+}
+
 static int key_bits(int B) {
   const unsigned long long maxkey = (unsigned long long)B * (unsigned long long)B;
   int bits = 1;
@@ -807,9 +849,7 @@ void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& opt, co
   const int to_merge = bm.num_blocks_to_merge;
   if (opt.approximate) {
     // Blockmodel::carry_out_best_merges (src/blockmodel/blockmodel.cpp:50-78); sort ties by index
-    std::vector<int> order(B);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b2) { return dS[a] < dS[b2]; });
+    const std::vector<int> order = stable_order_by(dS);
     GroupMap gm(B);
     int merged = 0, counter = 0;
     while (merged < to_merge) {
