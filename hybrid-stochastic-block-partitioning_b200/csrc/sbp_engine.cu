@@ -399,13 +399,9 @@ void gibbs_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, in
             g.view(), bm.view(), plan.order.p + plan.light_begin[bt] + ng, nl - ng, rng, sweep, bm.prop.p,
             bm.moved.p, n_cur, c.counters, g.light_cap, c.status, nullptr, 0);
     } else {
-      const int ns = eval_small_tier(bm, g, plan, bt);
-      if (ns > 0)
-        launch_small_tier(g, bm, plan.order.p + plan.light_begin[bt], ns, rng, sweep, n_cur, nullptr, 0, c.stream);
-      if (nl > ns)
-        k_eval<<<grid_for(nl - ns, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem, c.stream>>>(
-            g.view(), bm.view(), plan.order.p + plan.light_begin[bt] + ns, nl - ns, rng, sweep, bm.prop.p,
-            bm.moved.p, n_cur, c.counters, g.light_cap, c.status, nullptr, 0);
+      k_eval<<<grid_for(nl, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem, c.stream>>>(
+          g.view(), bm.view(), plan.order.p + plan.light_begin[bt], nl, rng, sweep, bm.prop.p, bm.moved.p, n_cur,
+          c.counters, g.light_cap, c.status, nullptr, 0);
     }
     SBP_CHECK_LAUNCH();
     if (g_prof.on) {
@@ -516,13 +512,9 @@ static int gibbs_sweeps_graph(SbpBlockmodel& bm, const SbpGraph& g, const BatchP
   for (int bt = 0; bt < nb; ++bt) {
     const int nl = plan.light_n[bt], nh = plan.heavy_n[bt];
     if (nl > 0) {
-      const int ng = !use_group_kernel(bm) ? eval_small_tier(bm, g, plan, bt)
-                     : bm.B <= kSmallB ? nl : plan.group_n[bt];
+      const int ng = !use_group_kernel(bm) ? 0 : bm.B <= kSmallB ? nl : plan.group_n[bt];
       if (ng > 0) {
-        if (use_group_kernel(bm))
-          launch_group_eval(g, bm, plan.order.p + plan.light_begin[bt], ng, rng, 0, nullptr, g_ctl.p, bt, c.stream);
-        else
-          launch_small_tier(g, bm, plan.order.p + plan.light_begin[bt], ng, rng, 0, nullptr, g_ctl.p, bt, c.stream);
+        launch_group_eval(g, bm, plan.order.p + plan.light_begin[bt], ng, rng, 0, nullptr, g_ctl.p, bt, c.stream);
         ++launches;
       }
       if (nl > ng) {
@@ -1202,9 +1194,6 @@ SbpStatus sbp_set_option(const char* name, int64_t value) {
   } else if (n == "batched_stall_graph") {
     SBP_REQUIRE(value >= -1 && value < (1LL << 30), "batched_stall_graph must be -1 or a graph index");
     g_batched_stall_graph = (int)value;
-  } else if (n == "eval_tiers") {
-    SBP_REQUIRE(value == 0 || value == 1, "eval_tiers must be 0 or 1");
-    g_eval_tiers = (int)value;
   } else if (n == "batched_threads") {
     SBP_REQUIRE(value >= 1 && value <= 64, "batched_threads must be in [1, 64]");
     g_batched_threads = (int)value;

@@ -417,8 +417,6 @@ inline int pow2_at_least(int x) {
 
 constexpr int kLightCap = 256;        // per-warp table slots for light vertices
 constexpr int kLightCapMax = 512;     // largest per-warp table of the 8-warp evaluation CTA
-constexpr int kSmallTierK = 64;       // light vertices of at most this degree ...
-constexpr int kSmallTierCap = 128;    // ... fit tables of this many slots (evaluated apart, option eval_tiers)
 constexpr int kLightWarps = 8;
 constexpr int kMaxCap = 8192;         // largest per-warp table
 constexpr size_t kSmemBudget = 200 * 1024;
@@ -440,9 +438,6 @@ inline thread_local long long g_overflow_rebuilds = 0;   // rebuilds forced by a
 // half the occupancy of the warp kernel at the light-table size of the 200,000-vertex graph,
 // measured slower there); 0 by the warp-per-vertex kernels always.
 inline int g_group_kernel = 1;
-// 1: the light vertices of k <= kSmallTierK are evaluated by a launch of their own, with tables
-// of kSmallTierCap slots and registers capped for four CTAs per SM (dense storage, warp kernel)
-inline int g_eval_tiers = 0;
 // Batched partitioner: idle claim attempts of a persistent CTA before the launch gives up with an
 // error (each attempt sleeps ~0.25 us), and the fault injection of the failure-detection test
 // (index of a graph whose sweep queue never opens; -1: none).  sbp_set_option.
@@ -466,7 +461,6 @@ struct BatchPlan {
   DevBuf<int> order;                       // per batch: light vertices then heavy vertices
   std::vector<int> light_begin, light_n, heavy_begin, heavy_n;
   std::vector<int> group_n;                // light vertices of k <= kGroupMaxK, at the front of each light list
-  std::vector<int> small_n;                // of those, the vertices of k <= kSmallTierK, at the very front
   std::vector<double> light_bytes;         // algorithmic bytes of each light evaluation launch
   int max_batch = 0;
 };
@@ -524,15 +518,8 @@ struct SbpGraph {
       for (int bt = 0; bt < n / batch_size; ++bt) {
         const int start = bt * batch_size, end = std::min(n, (bt + 1) * batch_size);
         p->light_begin.push_back((int)order.size());
-        // the light list in three tiers: k <= kSmallTierK (small tables), then the rest of the
-        // vertices that fit the group tables, then the other light vertices (the order inside a
-        // batch does not change its result)
-        for (int i = start; i < end; ++i)
-          if (h_k[list[i]] <= std::min(kSmallTierK, light_cap / 2)) order.push_back(list[i]);
-        p->small_n.push_back((int)order.size() - p->light_begin.back());
-        for (int i = start; i < end; ++i)
-          if (h_k[list[i]] > kSmallTierK && h_k[list[i]] <= std::min(kGroupMaxK, light_cap / 2))
-            order.push_back(list[i]);
+        for (int i = start; i < end; ++i)   // vertices that fit the group tables first
+          if (h_k[list[i]] <= std::min(kGroupMaxK, light_cap / 2)) order.push_back(list[i]);
         p->group_n.push_back((int)order.size() - p->light_begin.back());
         for (int i = start; i < end; ++i)
           if (h_k[list[i]] > kGroupMaxK && h_k[list[i]] <= light_cap / 2) order.push_back(list[i]);
@@ -682,21 +669,6 @@ inline void launch_group_eval(const SbpGraph& g, SbpBlockmodel& bm, const int* v
   k<<<grid_for(n, kSmallThreads / kSmallGroup, 64 * c.num_sms), kSmallThreads, smem, stream>>>(
       g.view(), bm.view(), verts, n, rng, sweep, bm.prop.p, bm.moved.p, n_moved, c.counters, cap, c.status, ctl,
       batch);
-}
-
-// Light vertices of batch bt evaluated by the low-degree tier's own launch (option eval_tiers;
-// dense storage, warp kernel): the front of the batch's light list.
-inline int eval_small_tier(const SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, int bt) {
-  return (g_eval_tiers && !bm.sparse && g.light_cap > kSmallTierCap) ? plan.small_n[bt] : 0;
-}
-inline void launch_small_tier(const SbpGraph& g, SbpBlockmodel& bm, const int* verts, int n, const RngParams& rng,
-                              int sweep, int* n_moved, const SweepCtl* ctl, int batch, cudaStream_t stream) {
-  Context& c = Context::get();
-  const size_t smem = (size_t)table_ints(kSmallTierCap) * sizeof(int) * kLightWarps;
-  set_smem_limit((const void*)k_gibbs_eval_dense_occ4, smem);
-  k_gibbs_eval_dense_occ4<<<grid_for(n, kLightWarps, 64 * c.num_sms), kLightWarps * 32, smem, stream>>>(
-      g.view(), bm.view(), verts, n, rng, sweep, bm.prop.p, bm.moved.p, n_moved, c.counters, kSmallTierCap, c.status,
-      ctl, batch);
 }
 
 struct MhResult {

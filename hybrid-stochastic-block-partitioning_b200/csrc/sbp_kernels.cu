@@ -114,15 +114,6 @@ __global__ void __launch_bounds__(256, 2)
   gibbs_eval_body<Store::kDenseFrozen>(g, bm, verts, n, rng, sweep, prop, moved_list, n_moved, counters, cap, status,
                                        ctl, batch);
 }
-// Registers capped for four CTAs per SM: the launch of the low-degree tier, whose tables of 128
-// slots (18 KB per CTA) leave room for them.
-__global__ void __launch_bounds__(256, 4)
-    k_gibbs_eval_dense_occ4(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
-                            int* prop, int* moved_list, int* n_moved, unsigned long long* counters, int cap,
-                            int* status, const SweepCtl* ctl, int batch) {
-  gibbs_eval_body<Store::kDenseFrozen>(g, bm, verts, n, rng, sweep, prop, moved_list, n_moved, counters, cap, status,
-                                       ctl, batch);
-}
 // The same with registers capped for three CTAs per SM (a few spilled values): more vertices in
 // flight, which pays while the block matrix is small enough for its cells to hit in L2.
 __global__ void __launch_bounds__(256, 3)

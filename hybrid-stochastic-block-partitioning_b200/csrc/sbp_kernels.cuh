@@ -48,10 +48,6 @@ __global__ void __launch_bounds__(256, 2)
     k_gibbs_eval_hashed(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
                         int* prop, int* moved_list, int* n_moved, unsigned long long* counters, int cap, int* status,
                         const SweepCtl* ctl, int batch);
-__global__ void __launch_bounds__(256, 4)
-    k_gibbs_eval_dense_occ4(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
-                            int* prop, int* moved_list, int* n_moved, unsigned long long* counters, int cap,
-                            int* status, const SweepCtl* ctl, int batch);
 __global__ void __launch_bounds__(256, 3)
     k_gibbs_eval_dense_occ3(GraphView g, BlockView bm, const int* __restrict__ verts, int n, RngParams rng, int sweep,
                             int* prop, int* moved_list, int* n_moved, unsigned long long* counters, int cap,
