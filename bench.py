@@ -18,7 +18,8 @@ device time (merges included) is the denominator.  `--config 2` runs the 20,000-
 --impl reference times the reference's own CPU implementation on every host core: the reference
 built from its sources (oracle/_ref; the timing build's only change is a cap on the sweeps of a
 finetune call), one 1-sweep asynchronous-Gibbs call per step at the block counts the partition
-passes through (V/2, V/4, ... down to the planted B, cycled over the steps).  The reference's
+passes through (V/2, V/4, ... down to the planted B), taken in spread order (V/2, the middle
+level, the quarter levels, ...) and cycled over the steps.  The reference's
 full-partition wall time on the same graph, measured once, is carried beside it (oracle/
 reference_anchors.json).
 Multi-GPU: the path does not shard; every rank runs its own replica partitions ("replicas
