@@ -298,7 +298,7 @@ bool early_stop(int iteration, bool bracket, double initial_entropy, const std::
   return average < threshold;
 }
 
-static int mh_cap(int max_k) {
+int mh_cap(int max_k) {
   int cap = pow2_at_least(std::max(2 * max_k, kLightCap));
   if (cap > kMaxCap) throw Error(SBP_ERR_UNSUPPORTED, "vertex degree too large for the Metropolis-Hastings kernel");
   return cap;

@@ -827,6 +827,8 @@ void merge_blocks(SbpBlockmodel& bm, SbpGraph& g, const SbpMergeOptions& opt, co
                   int* best_out, double* dS_out, SbpStats& st, const SbpMoveReplay* moves = nullptr);
 Snapshot snapshot(SbpBlockmodel& bm);
 void restore(SbpBlockmodel& bm, SbpGraph& g, const Snapshot& x);
+// Per-warp table slots of the Metropolis-Hastings kernels for vertices of degree up to max_k.
+int mh_cap(int max_k);
 // One sequential Metropolis-Hastings pass over a device list of n vertices.
 MhResult mh_pass(SbpBlockmodel& bm, const SbpGraph& g, const int* verts, int n, int max_k, RngParams rng, int sweep);
 

@@ -132,20 +132,6 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 
-// Same for a dense cell owned by one thread (plain update of M/MT, atomic chunk sums, which
-// lanes share); hashed rows are always updated atomically (lanes share their slots).
-__device__ __forceinline__ void cell_add_owned(const BlockView& bm, int row, int col, int delta) {
-  if (!delta) return;
-  if (bm.sparse) {
-    cell_add(bm, row, col, delta);
-    return;
-  }
-  bm.M[(size_t)row * bm.ld + col] += delta;
-  bm.MT[(size_t)col * bm.ld + row] += delta;
-  chunk_add(bm.CS, bm.nch, row, col, delta);
-  chunk_add(bm.CST, bm.nch, col, row, delta);
-}
-
 // Apply accepted moves of one batch.  Every edge incident to a moved vertex moves once from
 // its old cell to its new cell; the result equals the reference's one-by-one application.
 // qr/qs keep the reference's diagonal delta of each move as seen at its turn in vertex order,
@@ -269,7 +255,7 @@ __global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, i
   extern __shared__ int smem[];
   __shared__ int s_acc[32], s_moved[32], s_r[32], s_s[32], s_t[32], s_commit[32];
   __shared__ double s_dS[32];
-  __shared__ int s_first, s_stop, s_upto;
+  __shared__ int s_stop, s_upto;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int W = blockDim.x >> 5;
   WarpTable t = carve_table(smem, cap, warp);
@@ -305,97 +291,14 @@ __global__ void k_mh(GraphView g, BlockView bm, const int* __restrict__ verts, i
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      const int avail = min(W, n - pos);
-      int first = -1;
-      for (int w = 0; w < avail; ++w)
-        if (s_acc[w]) { first = w; break; }
-      int upto = first >= 0 ? first + 1 : avail;
-      if (first >= 0) s_commit[first] = 1;
-      if (first >= 0 && !bm.sparse) {
-        // later vertices whose evaluation no commit of this round could have touched keep their
-        // result: a commit c changes cells in rows / columns r_c, s_c towards its neighbour
-        // blocks, and the degrees and d of r_c and s_c.  Vertex w read its neighbours' blocks
-        // (a neighbour that moved puts r_c among them), the row and column of its proposal's
-        // block t_w, cells towards r_w, s_w and its neighbour blocks, and their degrees.
-        int ncommit = 1;
-        int cw[32];
-        cw[0] = first;
-        for (int w = first + 1; w < avail; ++w) {
-          const WarpTable tw = carve_table(smem, cap, w);
-          bool indep = true;
-          for (int q = 0; q < ncommit && indep; ++q) {
-            const int c = cw[q];
-            const WarpTable tc = carve_table(smem, cap, c);
-            const int rc = s_r[c], sc = s_s[c];
-            const int rw = s_r[w], sw = s_s[w], tb = s_t[w];
-            if (rc == rw || rc == sw || rc == tb || sc == rw || sc == sw || sc == tb) indep = false;
-            else if (table_find(tw, rc) >= 0 || table_find(tw, sc) >= 0) indep = false;
-            else if ((tb >= 0 && table_find(tc, tb) >= 0) || table_find(tc, rw) >= 0 || table_find(tc, sw) >= 0)
-              indep = false;
-          }
-          if (!indep) break;
-          upto = w + 1;
-          if (s_acc[w]) {
-            s_commit[w] = 1;
-            cw[ncommit++] = w;
-          }
-        }
-      }
-      s_first = first;
-      s_upto = upto;
+      int first;
+      s_upto = mh_round_commits(bm, smem, cap, min(W, n - pos), s_acc, s_r, s_s, s_t, s_commit, &first);
     }
     __syncthreads();
-    const int first = s_first;
     const int upto_round = s_upto;
-    if (s_commit[warp]) {
-      // apply the move of v from r to s with the counts still in this warp's table; lanes own
-      // distinct non-corner cells, lane 0 owns the four corner cells (r,r) (r,s) (s,r) (s,s)
-      const int s = res.s;
-      const int self = g.self[v];
-      const MoveCounts mc = corner_counts(t, r, s);
-      const int nl = *t.nlist;
-      for (int j = lane; j < nl; j += kWarp) {
-        const int h = t.list[j];
-        const int u = t.keys[h], co = t.cout[h], ci = t.cin[h];
-        if (u == r || u == s) continue;
-        cell_add_owned(bm, r, u, -co);
-        cell_add_owned(bm, s, u, co);
-        cell_add_owned(bm, u, r, -ci);
-        cell_add_owned(bm, u, s, ci);
-      }
-      __syncwarp();
-      if (lane == 0) {
-        const int d_rr = -mc.co_r - mc.ci_r - self;
-        const int d_rs = -mc.co_s + mc.ci_r;
-        const int d_sr = mc.co_r - mc.ci_s;
-        const int d_ss = mc.co_s + mc.ci_s + self;
-        cell_add_owned(bm, r, r, d_rr);
-        cell_add_owned(bm, r, s, d_rs);
-        cell_add_owned(bm, s, r, d_sr);
-        cell_add_owned(bm, s, s, d_ss);
-        bm.b[v] = s;
-        bm.d_out[r] -= k_out;
-        bm.d_out[s] += k_out;
-        bm.d_in[r] -= k_in + self;
-        bm.d_in[s] += k_in + self;
-        __threadfence_block();
-        if (*bm.overflow) {
-          // a hashed row is full: stop here; the host rebuilds the rows with more room, sets
-          // d[r], d[s] from the rebuilt diagonal and these deltas, and resumes at pos+first+1
-          s_stop = 1;
-          out[4] = 1.0;
-          out[5] = (double)(pos + first);
-          out[6] = (double)r;
-          out[7] = (double)s;
-          out[8] = (double)d_rr;
-          out[9] = (double)d_ss;
-        } else {
-          // Blockmodel::move_vertex reads the already-updated diagonal and adds the delta again
-          bm.d[r] = bm.d_out[r] + bm.d_in[r] - (bm_get(bm, r, r) + d_rr);
-          bm.d[s] = bm.d_out[s] + bm.d_in[s] - (bm_get(bm, s, s) + d_ss);
-        }
-      }
-    }
+    // a hashed row can run out of room only on row-hashed storage, where the round commits its
+    // first accepted vertex alone: the stop position is pos + first
+    if (s_commit[warp]) mh_apply_move(g, bm, t, v, r, res.s, k_out, k_in, lane, pos + warp, out, &s_stop);
     if (threadIdx.x == 0) {
       for (int w = 0; w < upto_round; ++w) {
         moved += s_moved[w];

@@ -29,6 +29,7 @@
 
 #include "sbp_engine.cuh"
 #include "sbp_mlp.cuh"
+#include "sbp_steps.cuh"
 
 using namespace sbpb;
 
@@ -174,6 +175,21 @@ struct BatchBufs {
   float* L2;      // [n][16]
 };
 
+// Features of vertex v against the current state into row `row` of the batch buffers (one
+// warp; the table is left filled, the caller resets it).
+__device__ __forceinline__ void features_row(const GraphView& g, const BlockView& bm, int v, int row, BatchBufs bb,
+                                             LearnedParams lp, const WarpTable& t, int lane, int* status) {
+  const int r = bm.b[v];
+  const int o0 = g.out_ptr[v], k_out = g.out_ptr[v + 1] - o0;
+  const int i0 = g.in_ptr[v], k_in = g.in_ptr[v + 1] - i0;
+  const int self = g.self[v];
+  gather_neighbour_blocks(g, bm, v, r, o0, k_out, i0, k_out + k_in, self, -1, t, lane, status);
+  __syncwarp();
+  int blk, nv;
+  vertex_features(bm, t, r, k_out, k_in, self, lp, lane, bb.F1 + (size_t)row * kMlpIn,
+                  bb.slot + (size_t)row * kFeatSlots, bb.info + row, &blk, &nv);
+}
+
 // Features of the batch's vertices (rows row0 .. row0 + n - 1 of the batch buffers).
 __global__ void k_learn_features(GraphView g, BlockView bm, const int* __restrict__ verts, int n, int row0,
                                  BatchBufs bb, LearnedParams lp, int cap, int* status) {
@@ -183,17 +199,7 @@ __global__ void k_learn_features(GraphView g, BlockView bm, const int* __restric
   WarpTable t = carve_table(smem, cap, warp);
   init_table(t, lane);
   for (int i = blockIdx.x * wpb + warp; i < n; i += gridDim.x * wpb) {
-    const int v = verts[i];
-    const int r = bm.b[v];
-    const int o0 = g.out_ptr[v], k_out = g.out_ptr[v + 1] - o0;
-    const int i0 = g.in_ptr[v], k_in = g.in_ptr[v + 1] - i0;
-    const int self = g.self[v];
-    gather_neighbour_blocks(g, bm, v, r, o0, k_out, i0, k_out + k_in, self, -1, t, lane, status);
-    __syncwarp();
-    const int row = row0 + i;
-    int blk, nv;
-    vertex_features(bm, t, r, k_out, k_in, self, lp, lane, bb.F1 + (size_t)row * kMlpIn,
-                    bb.slot + (size_t)row * kFeatSlots, bb.info + row, &blk, &nv);
+    features_row(g, bm, verts[i], row0 + i, bb, lp, t, lane, status);
     table_reset(t, lane);
   }
 }
@@ -211,12 +217,10 @@ __device__ __forceinline__ double learned_q(const float* L, int nvalid, int slot
   return q;
 }
 
-// Draw s from the forward logits, store q(s), and build the reverse-state features.
-__global__ void k_learn_propose(const int* __restrict__ verts, int n, BlockView bm, BatchBufs bb, LearnedParams lp,
-                                RngParams rng, int sweep, long long V, int* status) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int v = verts[i];
+// Draw s for vertex v (row i) from the forward logits, store q(s), and build the reverse-state
+// features.  One thread.
+__device__ __forceinline__ void propose_row(int i, int v, const BlockView& bm, BatchBufs bb, LearnedParams lp,
+                                            const RngParams& rng, int sweep, long long V, int* status) {
   const uint4 x = draw_record(rng, (uint32_t)v, (uint32_t)sweep, 0u, (long long)sweep * V + v, status);
   const int4 inf = bb.info[i];
   const int r = inf.x, k_out = inf.y, k_in = inf.z, self = inf.w & 1, nvalid = inf.w >> 1;
@@ -268,6 +272,14 @@ __global__ void k_learn_propose(const int* __restrict__ verts, int n, BlockView 
   f2[56 + 6] = __float2bfloat16_rn(g[6]);
 }
 
+// Draw s from the forward logits, store q(s), and build the reverse-state features.
+__global__ void k_learn_propose(const int* __restrict__ verts, int n, BlockView bm, BatchBufs bb, LearnedParams lp,
+                                RngParams rng, int sweep, long long V, int* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  propose_row(i, verts[i], bm, bb, lp, rng, sweep, V, status);
+}
+
 // Delta-MDL of the drawn move, the exact Hastings factor from the reverse logits, accept.
 __global__ void k_learn_eval(GraphView g, BlockView bm, const int* __restrict__ verts, int n, int row0,
                              BatchBufs bb, LearnedParams lp, RngParams rng, int sweep, int* prop, int* moved_list,
@@ -317,6 +329,129 @@ __global__ void k_learn_eval(GraphView g, BlockView bm, const int* __restrict__ 
     atomicAdd(counters + 0, c_visit);
     atomicAdd(counters + 1, c_moved);
     atomicAdd(counters + 2, c_acc);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Sequential Metropolis-Hastings with the learned proposal (finetune::metropolis_hastings,
+// src/finetune.cpp:412-444, with the proposal of :488-501 replaced).  A pass over a vertex list
+// is a sequence of rounds over a window of list positions pos .. pos + W - 1, pos kept on the
+// device so that rounds queue on the stream without the host:
+//   k_learn_mh_features  features of the window's vertices against the current state (rows 0..W-1)
+//   network              forward logits
+//   k_learn_mh_propose   draw, q(s | v, state), reverse-state features
+//   network              reverse logits
+//   k_learn_mh_round     delta-MDL, exact Hastings factor and accept of every window vertex against
+//                        the same state, then the commit rule of k_mh (mh_round_commits): the first
+//                        accepted vertex and later ones no commit could have touched are applied,
+//                        pos advances past the positions decided.
+// The features read v's neighbour blocks, the degrees of those blocks and of v's own block, B and
+// v's degrees; the reverse features the degrees of r and s.  A commit touches only the degrees of
+// its own r and s, and a vertex whose neighbour moved holds that neighbour's old block, so the
+// commit rule's independence test covers the learned draw as it covers the plain one: a vertex
+// kept in a round was proposed, corrected and accepted exactly as the sequential chain would.
+// out (doubles): [0] visits [1] proposals moved [2] accepted [3] sum of accepted dS, [4..9] the
+// stop record of a hashed row that ran out of room (mh_apply_move).
+// ------------------------------------------------------------------------------------------
+constexpr int kMhRoundMaxWarps = 16;
+
+__global__ void k_learn_mh_features(GraphView g, BlockView bm, const int* __restrict__ verts, int n,
+                                    const int* __restrict__ pos_ptr, int W, BatchBufs bb, LearnedParams lp, int cap,
+                                    int* status) {
+  extern __shared__ int smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int w = blockIdx.x * (blockDim.x >> 5) + warp;
+  const int i = *pos_ptr + w;
+  if (w >= W || i >= n) return;   // warp-uniform
+  WarpTable t = carve_table(smem, cap, warp);
+  init_table(t, lane);
+  features_row(g, bm, verts[i], w, bb, lp, t, lane, status);
+}
+
+__global__ void k_learn_mh_propose(const int* __restrict__ verts, int n, const int* __restrict__ pos_ptr, int W,
+                                   BlockView bm, BatchBufs bb, LearnedParams lp, RngParams rng, int sweep,
+                                   long long V, int* status) {
+  const int w = threadIdx.x;
+  const int i = *pos_ptr + w;
+  if (w >= W || i >= n) return;
+  propose_row(w, verts[i], bm, bb, lp, rng, sweep, V, status);
+}
+
+__global__ void __launch_bounds__(kMhRoundMaxWarps * 32)
+    k_learn_mh_round(GraphView g, BlockView bm, const int* __restrict__ verts, int n, int* pos_ptr, BatchBufs bb,
+                     LearnedParams lp, RngParams rng, int sweep, int cap, double* out, int* status) {
+  extern __shared__ int smem[];
+  __shared__ int s_acc[32], s_moved[32], s_r[32], s_s[32], s_t[32], s_commit[32];
+  __shared__ double s_dS[32];
+  __shared__ int s_stop, s_upto;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int W = blockDim.x >> 5;
+  const int pos = *pos_ptr;
+  // the list is done, or a hashed row ran out of room in an earlier round and the host has not
+  // yet rebuilt the rows: nothing to do (the same for every thread)
+  if (pos >= n || out[4] != 0.0) return;
+  WarpTable t = carve_table(smem, cap, warp);
+  init_table(t, lane);
+  const int i = pos + warp;
+  int v = -1, r = -1, s = -1, k_out = 0, k_in = 0, acc = 0;
+  double dS = 0.0;
+  if (i < n) {
+    v = verts[i];
+    const int4 inf = bb.info[warp];
+    r = inf.x;
+    k_out = inf.y;
+    k_in = inf.z;
+    const int self = inf.w & 1, nvalid = inf.w >> 1;
+    s = bb.s_prop[warp];
+    gather_neighbour_blocks(g, bm, v, r, g.out_ptr[v], k_out, g.in_ptr[v], k_out + k_in, self, -1, t, lane, status);
+    if (s != r) {
+      const uint4 x = draw_record(rng, (uint32_t)v, (uint32_t)sweep, 0u, (long long)sweep * g.V + v, status);
+      double Hp;
+      dS = move_delta(g, bm, r, s, k_out, k_in, self, t, lane, &Hp);
+      int slot_r = -1;
+      const int2* sl = bb.slot + (size_t)warp * kFeatSlots;
+      for (int j = 0; j < nvalid; ++j)
+        if (sl[j].x == r) slot_r = j;
+      const double qr = learned_q(bb.L2 + (size_t)warp * kMlpOut, nvalid, slot_r, lp.eps, bm.B);
+      const double H = qr / bb.qf[warp];
+      double ap = exp(-3.0 * dS) * H;
+      ap = ap >= 1.0 ? 1.0 : ap;
+      acc = (u53(x.z, x.w) <= ap) ? 1 : 0;
+    }
+  }
+  if (lane == 0) {
+    s_acc[warp] = acc;
+    s_moved[warp] = (i < n && s != r) ? 1 : 0;
+    s_dS[warp] = dS;
+    s_r[warp] = r;
+    s_s[warp] = s;
+    s_t[warp] = -1;   // the learned draw reads no row of a proposal block
+    s_commit[warp] = 0;
+  }
+  if (threadIdx.x == 0) s_stop = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int first;
+    s_upto = mh_round_commits(bm, smem, cap, min(W, n - pos), s_acc, s_r, s_s, s_t, s_commit, &first);
+  }
+  __syncthreads();
+  if (s_commit[warp]) mh_apply_move(g, bm, t, v, r, s, k_out, k_in, lane, pos + warp, out, &s_stop);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int upto = s_upto;
+    double moved = out[1], accepted = out[2], sum_dS = out[3];
+    for (int w = 0; w < upto; ++w) {
+      moved += s_moved[w];
+      if (s_commit[w]) {   // accepted moves in vertex order, summed in that order over the pass
+        accepted += 1.0;
+        sum_dS += s_dS[w];
+      }
+    }
+    out[0] += (double)upto;
+    out[1] = moved;
+    out[2] = accepted;
+    out[3] = sum_dS;
+    *pos_ptr = pos + upto;
   }
 }
 
@@ -395,6 +530,7 @@ struct LearnScratch {
   DevBuf<int> s_prop;
   DevBuf<double> qf;
   DevBuf<float> L1, L2;
+  DevBuf<int> mh_pos;   // list position of the learned Metropolis-Hastings pass
   void reserve(size_t n) {
     const size_t rows = ((n + kMlpTile - 1) / kMlpTile) * kMlpTile;
     F1.reserve(rows * kMlpIn);
@@ -450,6 +586,72 @@ static void check_tensor_status() {
   c.check_status();
 }
 
+// One sequential Metropolis-Hastings pass over verts (device list of n vertices) with the
+// learned proposal: rounds of k_learn_mh_* launches queued in chunks, the host reading the list
+// position back between chunks (and rebuilding hashed rows that ran out of room, as mh_pass).
+static MhResult learned_mh_pass(SbpBlockmodel& bm, const SbpGraph& g, const int* verts, int n, int max_k,
+                                const SbpMlp& mlp, LearnedParams lp, RngParams rng, int sweep) {
+  Context& c = Context::get();
+  MhResult res;
+  if (n == 0) return res;
+  const int cap = mh_cap(max_k);
+  const size_t per_warp = (size_t)table_ints(cap) * sizeof(int);
+  const int W = (int)std::min<size_t>(kMhRoundMaxWarps, kSmemBudget / per_warp);
+  if (W < 1) throw Error(SBP_ERR_UNSUPPORTED, "vertex degree too large for the Metropolis-Hastings kernel");
+  const int fw = std::min(W, 4);   // warps per CTA of the features launch
+  set_smem_limit((const void*)k_learn_mh_features, per_warp * fw);
+  set_smem_limit((const void*)k_learn_mh_round, per_warp * W);
+  g_learn.reserve(W);
+  g_learn.mh_pos.reserve(1);
+  const BatchBufs bb = g_learn.view();
+  int* pos = g_learn.mh_pos.p;
+  SBP_CUDA(cudaMemsetAsync(pos, 0, sizeof(int), c.stream));
+  SBP_CUDA(cudaMemsetAsync(c.mh_out, 0, 10 * sizeof(double), c.stream));
+  int at = 0, rounds = 8;
+  double out[10];
+  while (at < n) {
+    for (int k = 0; k < rounds; ++k) {
+      k_learn_mh_features<<<(W + fw - 1) / fw, fw * 32, per_warp * fw, c.stream>>>(g.view(), bm.view(), verts, n,
+                                                                                 pos, W, bb, lp, cap, c.status);
+      SBP_CHECK_LAUNCH();
+      mlp_forward(bb.F1, W, mlp.weights(), bb.L1, c.status, c.num_sms, c.stream);
+      SBP_CHECK_LAUNCH();
+      k_learn_mh_propose<<<1, 32, 0, c.stream>>>(verts, n, pos, W, bm.view(), bb, lp, rng, sweep, g.V, c.status);
+      SBP_CHECK_LAUNCH();
+      mlp_forward(bb.F2, W, mlp.weights(), bb.L2, c.status, c.num_sms, c.stream);
+      SBP_CHECK_LAUNCH();
+      k_learn_mh_round<<<1, W * 32, per_warp * W, c.stream>>>(g.view(), bm.view(), verts, n, pos, bb, lp, rng, sweep,
+                                                              cap, c.mh_out, c.status);
+      SBP_CHECK_LAUNCH();
+    }
+    int now = 0;
+    SBP_CUDA(SBP_COPY_ASYNC(&now, pos, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    SBP_CUDA(SBP_COPY_ASYNC(out, c.mh_out, sizeof(out), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    // every round decides at least one position, so a chunk that decided none means the rounds
+    // did not run as designed
+    if (now <= at) throw Error(SBP_ERR_DEVICE, "learned Metropolis-Hastings rounds made no progress");
+    if (out[4] != 0.0) {
+      // a hashed row ran out of room: rebuild the rows with more room (keeping d), finish that
+      // move's d[r], d[s]; pos is already past the move
+      rebuild(bm, g, false);
+      ++g_overflow_rebuilds;
+      k_fix_move_degrees<<<1, 1, 0, c.stream>>>(bm.view(), (int)out[6], (int)out[7], (int)out[8], (int)out[9]);
+      SBP_CHECK_LAUNCH();
+      SBP_CUDA(cudaMemsetAsync(c.mh_out + 4, 0, sizeof(double), c.stream));
+    }
+    // queue about as many rounds as the positions left need at the rate of this chunk
+    const double per_round = std::max(1.0, (double)(now - at) / rounds);
+    at = now;
+    rounds = (int)std::min(256.0, std::max(1.0, std::ceil((double)(n - at) / per_round)));
+  }
+  res.visits = (long long)out[0];
+  res.moved = (long long)out[1];
+  res.accepted = (long long)out[2];
+  res.sum_dS = out[3];
+  return res;
+}
+
 // Learned-proposal evaluation of one batch (light then heavy vertices of the plan), then apply.
 static void learned_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan& plan, int bt, const SbpMlp& mlp,
                           LearnedParams lp, RngParams rng, int sweep) {
@@ -484,11 +686,13 @@ static void learned_batch(SbpBlockmodel& bm, const SbpGraph& g, const BatchPlan&
 }
 
 // Finetune with the learned proposal (mlp != NULL) or the plain one (mlp == NULL), recording
-// the MDL after every sweep.  Asynchronous Gibbs or hybrid (the hybrid's high-degree
-// Metropolis-Hastings pass keeps the plain proposal).  A learned sweep whose acceptance rate
-// falls below fallback_acceptance switches the rest of the call to the plain proposal.
-// stop_rule 0: the asynchronous_gibbs early stop (changes measured from the call's first
-// MDL, src/finetune.cpp:40,74); 1: per-sweep MDL changes, as metropolis_hastings.
+// the MDL after every sweep: Metropolis-Hastings (learned_mh_pass over every vertex),
+// asynchronous Gibbs, or hybrid (learned_mh_pass over the high-degree list, then the batches).
+// A learned sweep whose acceptance rate falls below fallback_acceptance switches the rest of the
+// call to the plain proposal.  Early stop of Metropolis-Hastings: its own rule on each sweep's
+// summed accepted delta-MDL (src/finetune.cpp:144-162, 436-440).  Otherwise stop_rule 0: the
+// asynchronous_gibbs early stop (changes measured from the call's first MDL,
+// src/finetune.cpp:40,74); 1: per-sweep MDL changes, as metropolis_hastings.
 static void finetune_learned(SbpBlockmodel& bm, SbpGraph& g, int algorithm, const SbpFinetuneOptions& opt,
                              const SbpMlp* m, float eps, float fallback, int stop_rule, SbpTrace* trace,
                              SbpStats& st) {
@@ -508,7 +712,8 @@ static void finetune_learned(SbpBlockmodel& bm, SbpGraph& g, int algorithm, cons
   const int max_sweeps = (opt.max_sweeps <= 0 || opt.max_sweeps > kMaxIterations) ? kMaxIterations : opt.max_sweeps;
   const bool bracket = opt.bracket_established != 0;
   const LearnedParams lp = learned_params(g, eps);
-  const BatchPlan& plan = g.plan(algorithm, opt.batches);
+  const bool mh = algorithm == SBP_METROPOLIS_HASTINGS;
+  const BatchPlan* plan = mh ? nullptr : &g.plan(algorithm, opt.batches);
   SBP_CUDA(cudaMemsetAsync(c.counters, 0, 8 * sizeof(unsigned long long), c.stream));
   c.sync();
   const auto t0 = std::chrono::steady_clock::now();
@@ -520,20 +725,32 @@ static void finetune_learned(SbpBlockmodel& bm, SbpGraph& g, int algorithm, cons
   bool learned = m != nullptr;
   unsigned long long prev[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int it = 0; it < max_sweeps; ++it) {
-    if (algorithm == SBP_HYBRID_MCMC && !g.high.empty()) {
-      const MhResult r = mh_pass(bm, g, g.high_dev.p, (int)g.high.size(), g.max_k_of(g.high), rng, it);
+    long long pass_visits = 0, pass_acc = 0;   // this sweep's Metropolis-Hastings pass
+    double pass_dS = 0.0;
+    if (mh || (algorithm == SBP_HYBRID_MCMC && !g.high.empty())) {
+      const int* list = mh ? g.identity.p : g.high_dev.p;
+      const int nl = mh ? g.V : (int)g.high.size();
+      const int mk = mh ? g.max_k : g.max_k_of(g.high);
+      const MhResult r = learned ? learned_mh_pass(bm, g, list, nl, mk, *m, lp, rng, it)
+                                 : mh_pass(bm, g, list, nl, mk, rng, it);
       mh_visits += r.visits;
       mh_moved += r.moved;
       mh_acc += r.accepted;
+      pass_visits = r.visits;
+      pass_acc = r.accepted;
+      pass_dS = r.sum_dS;
     }
-    const long long ovf_sweep = g_overflow_rebuilds;
-    for (size_t bt = 0; bt < plan.light_n.size(); ++bt) {
-      if (learned) learned_batch(bm, g, plan, (int)bt, *m, lp, rng, it);
-      else gibbs_batch(bm, g, plan, (int)bt, rng, it);
+    if (!mh) {
+      const long long ovf_sweep = g_overflow_rebuilds;
+      for (size_t bt = 0; bt < plan->light_n.size(); ++bt) {
+        if (learned) learned_batch(bm, g, *plan, (int)bt, *m, lp, rng, it);
+        else gibbs_batch(bm, g, *plan, (int)bt, rng, it);
+      }
+      tidy_hashed(bm, g, ovf_sweep);
     }
-    tidy_hashed(bm, g, ovf_sweep);
     const double entropy = mdl(bm, g);
-    deltas.push_back(stop_rule == 1 ? entropy - last_entropy : entropy - initial_entropy);
+    if (mh) deltas.push_back(pass_dS);
+    else deltas.push_back(stop_rule == 1 ? entropy - last_entropy : entropy - initial_entropy);
     last_entropy = entropy;
     st.sweeps++;
     if (learned) st.learned_sweeps++;
@@ -547,7 +764,7 @@ static void finetune_learned(SbpBlockmodel& bm, SbpGraph& g, int algorithm, cons
       trace->count++;
     }
     if (learned) {
-      const double v = (double)(cnt[0] - prev[0]), a = (double)(cnt[2] - prev[2]);
+      const double v = (double)(cnt[0] - prev[0] + pass_visits), a = (double)(cnt[2] - prev[2] + pass_acc);
       if (v > 0 && a / v < (double)fallback) learned = false;
     }
     std::memcpy(prev, cnt, sizeof cnt);
@@ -1083,9 +1300,8 @@ SbpStatus sbp_finetune_learned(SbpBlockmodel* bm, const SbpGraph* cg, int32_t al
                                SbpTrace* trace, SbpStats* stats) {
   SBP_API_BEGIN
   SBP_REQUIRE(bm && cg && opt, "null argument");
-  SBP_REQUIRE(algorithm == SBP_ASYNC_GIBBS || algorithm == SBP_HYBRID_MCMC,
-              "the learned proposal runs with asynchronous Gibbs or hybrid batches");
-  SBP_REQUIRE(opt->batches >= 1, "batches must be >= 1");
+  SBP_REQUIRE(algorithm >= SBP_METROPOLIS_HASTINGS && algorithm <= SBP_HYBRID_MCMC, "unknown finetune algorithm");
+  SBP_REQUIRE(opt->batches >= 1 || algorithm == SBP_METROPOLIS_HASTINGS, "batches must be >= 1");
   SBP_REQUIRE(!trace || (trace->capacity >= 0 && (trace->capacity == 0 || (trace->seconds && trace->mdl))),
               "invalid trace");
   float eps, fallback;
@@ -1097,15 +1313,15 @@ SbpStatus sbp_finetune_learned(SbpBlockmodel* bm, const SbpGraph* cg, int32_t al
   SBP_API_END
 }
 
-// stochastic_block_partition with the learned proposal in every asynchronous-Gibbs or hybrid
-// finetune (mlp == NULL: the plain proposal with the chosen stop rule).
+// stochastic_block_partition with the learned proposal in every finetune (mlp == NULL: the plain
+// proposal with the chosen stop rule).
 SbpStatus sbp_partition_learned(const SbpGraph* cg, const SbpOptions* opt, const SbpMlp* m,
                                 const SbpLearnedOptions* lopt, int32_t* out_assignment, SbpStats* stats) {
   SBP_API_BEGIN
   SBP_REQUIRE(cg && opt && out_assignment, "null argument");
-  SBP_REQUIRE(opt->algorithm == SBP_ASYNC_GIBBS || opt->algorithm == SBP_HYBRID_MCMC,
-              "the learned proposal runs with asynchronous Gibbs or hybrid batches");
-  SBP_REQUIRE(opt->batches >= 1, "batches must be >= 1");
+  SBP_REQUIRE(opt->algorithm >= SBP_METROPOLIS_HASTINGS && opt->algorithm <= SBP_HYBRID_MCMC,
+              "unknown finetune algorithm");
+  SBP_REQUIRE(opt->batches >= 1 || opt->algorithm == SBP_METROPOLIS_HASTINGS, "batches must be >= 1");
   float eps, fallback;
   int stop_rule;
   check_learned_options(lopt, &eps, &fallback, &stop_rule);
@@ -1113,10 +1329,6 @@ SbpStatus sbp_partition_learned(const SbpGraph* cg, const SbpOptions* opt, const
   long long learned_sweeps = 0;
   const FinetuneStep step = [&](SbpBlockmodel& bm, SbpGraph& gg, int algo, const SbpFinetuneOptions& fo,
                                 SbpStats& fs) {
-    if (algo == SBP_METROPOLIS_HASTINGS) {   // after opt->asynciterations rounds
-      finetune(bm, gg, algo, fo, nullptr, fs);
-      return;
-    }
     finetune_learned(bm, gg, algo, fo, m, eps, fallback, stop_rule, nullptr, fs);
     learned_sweeps += fs.learned_sweeps;
   };

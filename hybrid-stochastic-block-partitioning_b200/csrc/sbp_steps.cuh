@@ -34,6 +34,125 @@ __device__ __forceinline__ void cell_add(const BlockView& bm, int row, int col, 
   chunk_add(bm.CST, bm.nch, col, row, delta);
 }
 
+// Same for a dense cell owned by one thread (plain update of M/MT, atomic chunk sums, which
+// lanes share); hashed rows are always updated atomically (lanes share their slots).
+__device__ __forceinline__ void cell_add_owned(const BlockView& bm, int row, int col, int delta) {
+  if (!delta) return;
+  if (bm.sparse) {
+    cell_add(bm, row, col, delta);
+    return;
+  }
+  bm.M[(size_t)row * bm.ld + col] += delta;
+  bm.MT[(size_t)col * bm.ld + row] += delta;
+  chunk_add(bm.CS, bm.nch, row, col, delta);
+  chunk_add(bm.CST, bm.nch, col, row, delta);
+}
+
+// Commit rule of a sequential Metropolis-Hastings round (finetune::metropolis_hastings,
+// src/finetune.cpp:412-444, run speculatively): warps 0 .. avail-1 of the CTA evaluated list
+// positions pos .. pos+avail-1 against the same state, with warp w's neighbour-block table in
+// the CTA's shared tables.  The first accepted vertex (in list order) commits; everything
+// before it was rejected against the true state.  On dense storage a later vertex keeps its
+// result while no commit of the round could have touched what it read: a commit c changes
+// cells in rows / columns r_c, s_c towards its neighbour blocks, and the degrees and d of r_c
+// and s_c.  Vertex w read its neighbours' blocks (a neighbour that moved puts r_c among them),
+// the row and column of its proposal's block t_w (-1: none), cells towards r_w, s_w and its
+// neighbour blocks, and their degrees.  Marks s_commit; returns the number of positions the
+// round visited.  Called by one thread.
+__device__ __forceinline__ int mh_round_commits(const BlockView& bm, int* smem, int cap, int avail, const int* s_acc,
+                                                const int* s_r, const int* s_s, const int* s_t, int* s_commit,
+                                                int* first_out) {
+  int first = -1;
+  for (int w = 0; w < avail; ++w)
+    if (s_acc[w]) {
+      first = w;
+      break;
+    }
+  int upto = first >= 0 ? first + 1 : avail;
+  if (first >= 0) s_commit[first] = 1;
+  if (first >= 0 && !bm.sparse) {
+    int ncommit = 1;
+    int cw[32];
+    cw[0] = first;
+    for (int w = first + 1; w < avail; ++w) {
+      const WarpTable tw = carve_table(smem, cap, w);
+      bool indep = true;
+      for (int q = 0; q < ncommit && indep; ++q) {
+        const int c = cw[q];
+        const WarpTable tc = carve_table(smem, cap, c);
+        const int rc = s_r[c], sc = s_s[c];
+        const int rw = s_r[w], sw = s_s[w], tb = s_t[w];
+        if (rc == rw || rc == sw || rc == tb || sc == rw || sc == sw || sc == tb) indep = false;
+        else if (table_find(tw, rc) >= 0 || table_find(tw, sc) >= 0) indep = false;
+        else if ((tb >= 0 && table_find(tc, tb) >= 0) || table_find(tc, rw) >= 0 || table_find(tc, sw) >= 0)
+          indep = false;
+      }
+      if (!indep) break;
+      upto = w + 1;
+      if (s_acc[w]) {
+        s_commit[w] = 1;
+        cw[ncommit++] = w;
+      }
+    }
+  }
+  *first_out = first;
+  return upto;
+}
+
+// One warp applies the committed move of v from r to s (Blockmodel::move_vertex,
+// src/blockmodel/blockmodel.cpp:344-360) with the counts still in its table: lanes own distinct
+// non-corner cells, lane 0 the four corner cells (r,r) (r,s) (s,r) (s,s), the assignment and
+// the degrees.  When a hashed row runs out of room, lane 0 sets *stop and records in out[4..9]
+// where the round stopped (list position stop_pos) and the move's diagonal deltas: the host
+// rebuilds the rows with more room, sets d[r], d[s] from the rebuilt diagonal and these deltas,
+// and resumes at stop_pos + 1.
+__device__ __forceinline__ void mh_apply_move(const GraphView& g, const BlockView& bm, const WarpTable& t, int v, int r,
+                                              int s, int k_out, int k_in, int lane, int stop_pos, double* out,
+                                              int* stop) {
+  const int self = g.self[v];
+  const MoveCounts mc = corner_counts(t, r, s);
+  const int nl = *t.nlist;
+  for (int j = lane; j < nl; j += kWarp) {
+    const int h = t.list[j];
+    const int u = t.keys[h], co = t.cout[h], ci = t.cin[h];
+    if (u == r || u == s) continue;
+    cell_add_owned(bm, r, u, -co);
+    cell_add_owned(bm, s, u, co);
+    cell_add_owned(bm, u, r, -ci);
+    cell_add_owned(bm, u, s, ci);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    const int d_rr = -mc.co_r - mc.ci_r - self;
+    const int d_rs = -mc.co_s + mc.ci_r;
+    const int d_sr = mc.co_r - mc.ci_s;
+    const int d_ss = mc.co_s + mc.ci_s + self;
+    cell_add_owned(bm, r, r, d_rr);
+    cell_add_owned(bm, r, s, d_rs);
+    cell_add_owned(bm, s, r, d_sr);
+    cell_add_owned(bm, s, s, d_ss);
+    bm.b[v] = s;
+    bm.d_out[r] -= k_out;
+    bm.d_out[s] += k_out;
+    bm.d_in[r] -= k_in + self;
+    bm.d_in[s] += k_in + self;
+    __threadfence_block();
+    if (*bm.overflow) {
+      *stop = 1;
+      out[4] = 1.0;
+      out[5] = (double)stop_pos;
+      out[6] = (double)r;
+      out[7] = (double)s;
+      out[8] = (double)d_rr;
+      out[9] = (double)d_ss;
+    } else {
+      // Blockmodel::move_vertex reads the already-updated diagonal and adds the delta again
+      bm.d[r] = bm.d_out[r] + bm.d_in[r] - (bm_get(bm, r, r) + d_rr);
+      bm.d[s] = bm.d_out[s] + bm.d_in[s] - (bm_get(bm, s, s) + d_ss);
+    }
+  }
+}
+
 // Apply of one accepted move v: r -> prop[v] (Blockmodel::move_vertex, src/blockmodel/
 // blockmodel.cpp:344-360, for a batch of simultaneous moves): M, MT and the chunk sums by edge,
 // d_out / d_in, the quirk terms qr/qs of d[r], d[s] (the neighbours that are counted in the

@@ -422,12 +422,16 @@ SbpStatus sbp_learned_q(const SbpBlockmodel *bm, const SbpGraph *g, const SbpMlp
  * candidate slot of every accepted move to `data` (samples past its capacity are dropped). */
 SbpStatus sbp_collect_moves(SbpBlockmodel *bm, const SbpGraph *g, SbpDataset *data, const SbpFinetuneOptions *opt,
                             SbpStats *stats);
-/* Asynchronous-Gibbs or hybrid finetune with the learned proposal (mlp != NULL) or the plain one
- * (mlp == NULL), same sweeps as sbp_finetune, early stop per lopt->stop_rule; optional per-sweep
- * MDL trace. */
+/* finetune::{metropolis_hastings, asynchronous_gibbs, hybrid_mcmc} (src/finetune.cpp:412-444,
+ * 31-89, 342-410) with the learned proposal (mlp != NULL) in place of common::propose_new_block
+ * (src/common.cpp:131-182) or with the plain one (mlp == NULL), same sweeps as sbp_finetune.
+ * Metropolis-Hastings (and the hybrid's high-degree pass) keeps the sequential chain exactly: each
+ * visit is proposed, corrected and accepted against the state left by every earlier visit.
+ * Early stop: Metropolis-Hastings its own rule (each sweep's summed accepted delta-MDL); the
+ * others per lopt->stop_rule.  Optional per-sweep MDL trace. */
 SbpStatus sbp_finetune_learned(SbpBlockmodel *bm, const SbpGraph *g, int32_t algorithm, const SbpFinetuneOptions *opt,
                                const SbpMlp *mlp, const SbpLearnedOptions *lopt, SbpTrace *trace, SbpStats *stats);
-/* sbp_partition with the learned proposal in every asynchronous-Gibbs / hybrid finetune
+/* sbp_partition with the learned proposal in every finetune, Metropolis-Hastings included
  * (mlp == NULL: the plain proposal, with lopt->stop_rule). */
 SbpStatus sbp_partition_learned(const SbpGraph *g, const SbpOptions *opt, const SbpMlp *mlp,
                                 const SbpLearnedOptions *lopt, int32_t *out_assignment, SbpStats *stats);

@@ -200,11 +200,107 @@ def test_learned_finetune_keeps_the_blockmodel_consistent(S, O, mlp):
     odo, odi, _ = ob.degrees()
     assert np.array_equal(do, odo) and np.array_equal(di, odi)
     assert st["mdl"] == pytest.approx(ob.mdl(), rel=1e-6)
-    # hybrid: high-degree vertices keep plain Metropolis-Hastings
+    # hybrid: the high-degree vertices go through the learned Metropolis-Hastings pass
     st2 = S.learned.finetune(bm, mlp, algorithm="hybrid_mcmc", batches=5, seed=4, max_sweeps=3, stop_rule=1)
-    assert 1 <= st2["sweeps"] <= 3
+    assert 1 <= st2["sweeps"] <= 3 and st2["learned_sweeps"] == st2["sweeps"]
+    ob = O.Blockmodel(O.Graph(V, s, d), B, bm.block_assignment())
+    assert np.array_equal(bm.blockmatrix(), ob.matrix())
     with pytest.raises(S.SbpError):
-        S.learned.finetune(bm, mlp, algorithm="metropolis_hastings")
+        S.learned.finetune(bm, mlp, algorithm=7)
+
+
+def sequential_learned_mh(S, O, bm, mlp, verts, seed, call, sweep, eps):
+    """The sequential Metropolis-Hastings chain with the learned proposal, one visit at a time
+    through the per-vertex entry points (finetune::metropolis_hastings, src/finetune.cpp:412-444):
+    evaluate v against the current state with the Philox record of its visit, move it when
+    accepted.  Returns the number of accepted moves."""
+    key = [seed & 0xFFFFFFFF, seed >> 32]
+    accepted = 0
+    for v in verts:
+        rec = O.philox([int(v), sweep, call, 0], key)[None, :]
+        prop, _, _, _, acc = S.learned.evaluate(bm, mlp, np.array([v], np.int32), rec, epsilon=eps)
+        if acc[0]:
+            bm.move_vertex(int(v), int(prop[0]))
+            accepted += 1
+    return accepted
+
+
+@pytest.mark.parametrize("storage", ["dense", "hashed"])
+def test_learned_mh_sweep_is_the_sequential_chain(S, O, mlp, storage):
+    """One learned Metropolis-Hastings sweep, run as rounds of up to 16 speculative visits with
+    the network on the tensor cores, equals the sequential chain bit for bit: assignment, block
+    matrix and all three degree vectors (the drifting d included)."""
+    S.set_option("dense_max_blocks", 131072 if storage == "dense" else 1)
+    try:
+        V, s, d, _ = random_graph(700, 10, 131, kmin=4, kmax=40, w=0.8)
+        g = S.Graph(V, s, d)
+        B = 24
+        a = random_assignment(V, B, 131)
+        bm, ref = S.Blockmodel(g, B, a), S.Blockmodel(g, B, a)
+        st = S.learned.finetune(bm, mlp, algorithm="metropolis_hastings", seed=9, call=4, max_sweeps=1)
+        acc = sequential_learned_mh(S, O, ref, mlp, range(V), 9, 4, 0, 0.05)
+        assert st["visits"] == V and st["sweeps"] == 1 and st["learned_sweeps"] == 1
+        assert st["accepted"] == acc > V // 20
+        assert np.array_equal(bm.block_assignment(), ref.block_assignment())
+        assert np.array_equal(bm.blockmatrix(), ref.blockmatrix())
+        for x, y in zip(bm.degrees_all(), ref.degrees_all()):
+            assert np.array_equal(x, y)
+    finally:
+        S.set_option("dense_max_blocks", 131072)
+
+
+def test_learned_mh_high_degree_pass_of_hybrid_is_the_sequential_chain(S, O, mlp):
+    """The hybrid's high-degree pass with the learned proposal visits the high-degree list in its
+    order, exactly as the sequential chain over that list would."""
+    V, s, d, _ = random_graph(900, 10, 141, kmin=4, kmax=60, w=0.8)
+    g = S.Graph(V, s, d)
+    high, low = g.split()
+    # every vertex in the high-degree list (the high ones first, then the rest) and none left for
+    # the batches: one hybrid sweep is then the learned pass over that list alone
+    order = np.concatenate([high, low]).astype(np.int32)
+    g.set_split(order, np.zeros(0, np.int32))
+    B = 20
+    a = random_assignment(V, B, 141)
+    bm, ref = S.Blockmodel(g, B, a), S.Blockmodel(g, B, a)
+    st = S.learned.finetune(bm, mlp, algorithm="hybrid_mcmc", batches=2, seed=3, call=1, max_sweeps=1)
+    acc = sequential_learned_mh(S, O, ref, mlp, order, 3, 1, 0, 0.05)
+    assert st["visits"] == V
+    assert st["accepted"] == acc > 0
+    assert np.array_equal(bm.block_assignment(), ref.block_assignment())
+    assert np.array_equal(bm.blockmatrix(), ref.blockmatrix())
+    for x, y in zip(bm.degrees_all(), ref.degrees_all()):
+        assert np.array_equal(x, y)
+
+
+def test_plain_mode_of_the_learned_mh_is_the_plain_mh(S):
+    """mlp = None: the same Metropolis-Hastings chain, early stop included, as sbp_finetune."""
+    V, s, d, _ = random_graph(1200, 8, 83)
+    g = S.Graph(V, s, d)
+    a = random_assignment(V, 30, 83)
+    bm1, bm2 = S.Blockmodel(g, 30, a), S.Blockmodel(g, 30, a)
+    st1 = S.finetune.metropolis_hastings(bm1, seed=7, call=2)
+    st2 = S.learned.finetune(bm2, None, algorithm="metropolis_hastings", seed=7, call=2)
+    assert np.array_equal(bm1.block_assignment(), bm2.block_assignment())
+    assert st1["sweeps"] == st2["sweeps"] and st1["accepted"] == st2["accepted"]
+    assert st2["learned_sweeps"] == 0
+
+
+def test_learned_mh_fallback_and_partition(S, O):
+    """The plain proposal takes over when the learned sweeps' acceptance falls below the
+    threshold; a learned Metropolis-Hastings partition of a config-1-sized graph recovers the
+    planted blocks and its MDL is the oracle's MDL of its assignment."""
+    V, s, d, truth = random_graph(1000, 11, 151, kmin=10, kmax=100, w=0.8, alpha=10.0)
+    g = S.Graph(V, s, d)
+    m = S.Mlp(seed=3)
+    bm = S.Blockmodel(g, 40, random_assignment(V, 40, 151))
+    st = S.learned.finetune(bm, m, algorithm="metropolis_hastings", seed=1, max_sweeps=5, fallback_acceptance=1.01)
+    assert st["learned_sweeps"] == 1 and st["sweeps"] >= 2
+    out, st = S.learned.stochastic_block_partition(g, m, algorithm="metropolis_hastings", seed=2,
+                                                   fallback_acceptance=0.05)
+    assert st["learned_sweeps"] > 0 and st["num_blocks"] >= 2
+    assert O.nmi(out, truth) > 0.9
+    ob = O.Blockmodel(O.Graph(V, s, d), int(out.max()) + 1, out)
+    assert st["mdl"] == pytest.approx(ob.mdl(), rel=1e-5)
 
 
 def test_fallback_to_the_plain_proposal(S, mlp):
