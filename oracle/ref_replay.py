@@ -10,7 +10,6 @@ proposal i of a block).
 """
 import json
 import os
-import struct
 import subprocess
 import tempfile
 

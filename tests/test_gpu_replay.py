@@ -20,8 +20,6 @@ The reference runs here on the host cores (its build travels with the repository
 import numpy as np
 import pytest
 
-from conftest import ROOT
-
 pytestmark = pytest.mark.gpu
 RTOL_MDL = 1e-9
 
