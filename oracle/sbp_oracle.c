@@ -25,7 +25,10 @@
  *   D1  random numbers come from Philox4x32-10 keyed by (seed) with counter
  *       (vertex, sweep, call, 0) for a finetune visit and (block, proposal, call, 1) for a
  *       merge proposal, or from a host-supplied replay buffer of the same 4-word records,
- *       instead of per-translation-unit std::default_random_engine objects;
+ *       instead of per-translation-unit std::default_random_engine objects.  A replay buffer
+ *       may instead hold a recorded proposal stream (moves mode): records (s, 0, u_hi, u_lo)
+ *       with the proposed block of every visit or merge proposal and the bits of its accept
+ *       uniform, as the patched reference logs them;
  *   D2  the multinomial over M[t,:]+M[:,t] (src/common.cpp:159-180) walks row t ascending
  *       and then column t ascending (a canonical order; the reference walks robin_map
  *       buckets), and the dead `std::rand() <= B/(d_t+B)` branch (src/common.cpp:154, true
@@ -69,6 +72,7 @@ typedef struct {
     uint64_t seed;
     const uint32_t *replay;   /* optional: 4 words per record */
     int64_t replay_records;
+    int moves;                /* 1: replay records are recorded proposals (s, 0, u_hi, u_lo) */
 } SbpoRng;
 
 /* Draw the 4-word record for (a, b, call, tag). Replay records are indexed by `slot`. */
@@ -91,6 +95,14 @@ double sbpo_u53(uint32_t hi, uint32_t lo) {
 }
 
 static inline int64_t sbpo_scale(uint32_t x, int64_t n) { return (int64_t)(((uint64_t)x * (uint64_t)n) >> 32); }
+
+/* The accept uniform of a recorded proposal: the double whose bits are (u_hi, u_lo). */
+static double record_uniform(const uint32_t x[4]) {
+    uint64_t bits = ((uint64_t)x[2] << 32) | (uint64_t)x[3];
+    double u;
+    memcpy(&u, &bits, sizeof u);
+    return u;
+}
 
 /* ------------------------------------------------------------------------------------- */
 /* Graph (include/graph.hpp:15-113, src/graph.cpp:165-228, src/utils.cpp:52-60)            */
@@ -554,10 +566,28 @@ static Proposal propose_vertex(const SbpoBM *bm, const SbpoGraph *g, int v, cons
  * (finetune::propose_move/move_vertex/accept, src/finetune.cpp:19-29,446-501). */
 typedef struct { int s; int moved_proposal; int accepted; double dS, H; } Eval;
 
-static Eval eval_vertex(const SbpoBM *bm, const SbpoGraph *g, int v, const uint32_t x[4]) {
+/* The proposal of a visit: drawn from the record x, or (moves) the recorded block x[0].
+ * Returns 0 when a recorded block is out of range. */
+static int visit_proposal(const SbpoBM *bm, const SbpoGraph *g, int v, const uint32_t x[4], int moves,
+                          Proposal *p) {
+    if (!moves) { *p = propose_vertex(bm, g, v, x); return 1; }
+    p->k_out = g->out_ptr[v + 1] - g->out_ptr[v];
+    p->k_in = (g->in_ptr[v + 1] - g->in_ptr[v]) - g->self[v];
+    p->k = p->k_out + p->k_in;
+    p->s = (int)x[0];
+    if (p->s < 0 || p->s >= bm->B) { p->s = bm->b[v]; return 0; }
+    return 1;
+}
+
+static double visit_uniform(const uint32_t x[4], int moves) {
+    return moves ? record_uniform(x) : sbpo_u53(x[2], x[3]);
+}
+
+static Eval eval_vertex(const SbpoBM *bm, const SbpoGraph *g, int v, const uint32_t x[4], int moves, int *bad) {
     Eval ev = {0};
     int r = bm->b[v];
-    Proposal p = propose_vertex(bm, g, v, x);
+    Proposal p;
+    if (!visit_proposal(bm, g, v, x, moves, &p)) *bad = 1;
     ev.s = p.s;
     if (p.s == r) return ev;   /* no move, no uniform consumed */
     ev.moved_proposal = 1;
@@ -566,7 +596,7 @@ static Eval eval_vertex(const SbpoBM *bm, const SbpoGraph *g, int v, const uint3
     ev.H = hastings_move(bm, g, &dl, v, &p);
     ev.dS = delta_mdl_move(bm, &dl, &p, g->E);
     delta_free(&dl);
-    double u = sbpo_u53(x[2], x[3]);
+    double u = visit_uniform(x, moves);
     double ap = exp(-3.0 * ev.dS) * ev.H;
     ap = (ap >= 1.0) ? 1.0 : ap;
     ev.accepted = (u <= ap);
@@ -576,7 +606,8 @@ static Eval eval_vertex(const SbpoBM *bm, const SbpoGraph *g, int v, const uint3
 /* Public single-step helpers for unit tests. */
 int sbpo_eval_vertex(const SbpoBM *bm, const SbpoGraph *g, int v, const uint32_t x[4],
                      int *s, double *dS, double *H, int *accepted) {
-    Eval ev = eval_vertex(bm, g, v, x);
+    int bad = 0;
+    Eval ev = eval_vertex(bm, g, v, x, 0, &bad);
     *s = ev.s; *dS = ev.dS; *H = ev.H; *accepted = ev.accepted;
     return ev.moved_proposal;
 }
@@ -638,14 +669,15 @@ static int mh_visit(SbpoBM *bm, const SbpoGraph *g, const SbpoRng *rng, int v, i
     if (sbpo_draw(rng, (uint32_t)v, (uint32_t)sweep, call, 0, visit_slot(sweep, g->V, v), x)) { st->rng_error = 1; return 0; }
     st->visits++;
     int r = bm->b[v];
-    Proposal p = propose_vertex(bm, g, v, x);
+    Proposal p;
+    if (!visit_proposal(bm, g, v, x, rng->moves, &p)) { st->rng_error = 1; return 0; }
     if (p.s == r) return 0;
     st->proposals_moved++;
     Delta dl;
     vertex_delta(&dl, bm, g, v, r, p.s);
     double H = hastings_move(bm, g, &dl, v, &p);
     double dS = delta_mdl_move(bm, &dl, &p, g->E);
-    double u = sbpo_u53(x[2], x[3]);
+    double u = visit_uniform(x, rng->moves);
     double ap = exp(-3.0 * dS) * H;
     ap = (ap >= 1.0) ? 1.0 : ap;
     int acc = (u <= ap);
@@ -663,7 +695,9 @@ static void gibbs_batch(SbpoBM *bm, const SbpoGraph *g, const SbpoRng *rng, cons
         uint32_t x[4];
         if (sbpo_draw(rng, (uint32_t)v, (uint32_t)sweep, call, 0, visit_slot(sweep, g->V, v), x)) { st->rng_error = 1; return; }
         st->visits++;
-        Eval ev = eval_vertex(bm, g, v, x);
+        int bad = 0;
+        Eval ev = eval_vertex(bm, g, v, x, rng->moves, &bad);
+        if (bad) { st->rng_error = 1; return; }
         if (ev.moved_proposal) st->proposals_moved++;
         if (ev.accepted) { moved[v] = 1; prop_of[v] = ev.s; }
     }
@@ -688,11 +722,9 @@ static void gibbs_batch(SbpoBM *bm, const SbpoGraph *g, const SbpoRng *rng, cons
 enum { SBPO_MH = 0, SBPO_GIBBS = 1, SBPO_HYBRID = 2 };
 
 /* finetune::{metropolis_hastings, asynchronous_gibbs, hybrid_mcmc}. */
-int sbpo_finetune(SbpoBM *bm, const SbpoGraph *g, int algo, int batches, int bracket_established,
-                  uint64_t seed, uint32_t call, const uint32_t *replay, int64_t replay_records,
-                  int max_sweeps, SbpoStats *st) {
+static int finetune_run(SbpoBM *bm, const SbpoGraph *g, int algo, int batches, int bracket_established,
+                        SbpoRng rng, uint32_t call, int max_sweeps, SbpoStats *st) {
     memset(st, 0, sizeof(*st));
-    SbpoRng rng = {seed, replay, replay_records};
     if (max_sweeps <= 0 || max_sweeps > SBPO_MAX_ITERATIONS) max_sweeps = SBPO_MAX_ITERATIONS;
     if (bm->B == 1) { st->mdl = bm->overall_entropy; return 0; }
     int V = g->V, E = g->E;
@@ -739,6 +771,21 @@ int sbpo_finetune(SbpoBM *bm, const SbpoGraph *g, int algo, int batches, int bra
     bm->overall_entropy = (float)sbpo_mdl(bm, V, E);
     st->mdl = bm->overall_entropy;
     return st->rng_error ? -1 : 0;
+}
+
+int sbpo_finetune(SbpoBM *bm, const SbpoGraph *g, int algo, int batches, int bracket_established,
+                  uint64_t seed, uint32_t call, const uint32_t *replay, int64_t replay_records,
+                  int max_sweeps, SbpoStats *st) {
+    SbpoRng rng = {seed, replay, replay_records, 0};
+    return finetune_run(bm, g, algo, batches, bracket_established, rng, call, max_sweeps, st);
+}
+
+/* The finetune driven by a recorded proposal stream: record t*V + v holds the proposed block
+ * of vertex v's visit in sweep t and the bits of its accept uniform. */
+int sbpo_finetune_moves(SbpoBM *bm, const SbpoGraph *g, int algo, int batches, int bracket_established,
+                        const uint32_t *records, int64_t num_records, int max_sweeps, SbpoStats *st) {
+    SbpoRng rng = {0, records, num_records, 1};
+    return finetune_run(bm, g, algo, batches, bracket_established, rng, 0, max_sweeps, st);
 }
 
 /* ------------------------------------------------------------------------------------- */
@@ -813,8 +860,12 @@ double sbpo_merge_delta_mdl(const SbpoBM *bm, int r, int s) {
 static double merge_score(double dS) { return nearbyint(dS * 1048576.0) / 1048576.0; }
 
 /* common::propose_new_block(block_merge = true) for block r with record x (D2 order). */
-static int propose_merge(const SbpoBM *bm, int r, const uint32_t x[4]) {
+static int propose_merge(const SbpoBM *bm, int r, const uint32_t x[4], int moves) {
     int B = bm->B;
+    if (moves) {   /* a recorded proposal: any block but r */
+        int s = (int)x[0];
+        return (s < 0 || s >= B || s == r) ? -1 : s;
+    }
     int64_t k_out = row_sum(bm, r, -1), k_in = col_sum(bm, r, -1), k = k_out + k_in;
     if (k == 0) return random_block(r, B, x[1]);
     int64_t target = sbpo_scale(x[0], k);
@@ -942,10 +993,8 @@ static int carry_out_advanced(SbpoBM *bm, const double *dS, const int *best) {
 typedef struct { int64_t proposals, avoided; } SbpoMergeStats;
 
 /* block_merge::merge_blocks (src/block_merge.cpp:278-311). best/dS may be NULL. */
-int sbpo_merge_blocks(SbpoBM *bm, const SbpoGraph *g, int approximate, uint64_t seed, uint32_t call,
-                      const uint32_t *replay, int64_t replay_records, int *best_out, double *dS_out,
-                      SbpoMergeStats *ms) {
-    SbpoRng rng = {seed, replay, replay_records};
+static int merge_run(SbpoBM *bm, const SbpoGraph *g, int approximate, SbpoRng rng, uint32_t call, int *best_out,
+                     double *dS_out, SbpoMergeStats *ms) {
     int B = bm->B;
     int *best = (int *)malloc(sizeof(int) * (size_t)(B + 1));
     double *dS = (double *)malloc(sizeof(double) * (size_t)(B + 1));
@@ -960,7 +1009,8 @@ int sbpo_merge_blocks(SbpoBM *bm, const SbpoGraph *g, int approximate, uint64_t 
             if (sbpo_draw(&rng, (uint32_t)r, (uint32_t)i, call, 1, (int64_t)r * SBPO_PROPOSALS_PER_BLOCK + i, x)) {
                 free(best); free(dS); free(past); free(pl); return -1;
             }
-            int s = propose_merge(bm, r, x);
+            int s = propose_merge(bm, r, x, rng.moves);
+            if (s < 0) { free(best); free(dS); free(past); free(pl); return -1; }
             if (ms) ms->proposals++;
             if (past[s]) { if (ms) ms->avoided++; continue; }
             double d = merge_score(sbpo_merge_delta_mdl(bm, r, s));
@@ -976,6 +1026,21 @@ int sbpo_merge_blocks(SbpoBM *bm, const SbpoGraph *g, int approximate, uint64_t 
     if (rc) return rc;
     sbpo_bm_rebuild(bm, g);
     return 0;
+}
+
+int sbpo_merge_blocks(SbpoBM *bm, const SbpoGraph *g, int approximate, uint64_t seed, uint32_t call,
+                      const uint32_t *replay, int64_t replay_records, int *best_out, double *dS_out,
+                      SbpoMergeStats *ms) {
+    SbpoRng rng = {seed, replay, replay_records, 0};
+    return merge_run(bm, g, approximate, rng, call, best_out, dS_out, ms);
+}
+
+/* The merge step driven by a recorded proposal stream: record r*10 + i holds proposal i of
+ * block r. */
+int sbpo_merge_blocks_moves(SbpoBM *bm, const SbpoGraph *g, int approximate, const uint32_t *records,
+                            int64_t num_records, int *best_out, double *dS_out, SbpoMergeStats *ms) {
+    SbpoRng rng = {0, records, num_records, 1};
+    return merge_run(bm, g, approximate, rng, 0, best_out, dS_out, ms);
 }
 
 void sbpo_bm_set_num_blocks_to_merge(SbpoBM *bm, int n) { bm->num_blocks_to_merge = n; }

@@ -104,6 +104,12 @@ def lib():
         L.sbpo_merge_blocks.restype = ctypes.c_int
         L.sbpo_merge_blocks.argtypes = [vp, vp, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint32, _u32p,
                                         ctypes.c_int64, _i32p, _f64p, ctypes.POINTER(_MergeStats)]
+        L.sbpo_finetune_moves.restype = ctypes.c_int
+        L.sbpo_finetune_moves.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _u32p, ctypes.c_int64,
+                                          ctypes.c_int, ctypes.POINTER(_Stats)]
+        L.sbpo_merge_blocks_moves.restype = ctypes.c_int
+        L.sbpo_merge_blocks_moves.argtypes = [vp, vp, ctypes.c_int, _u32p, ctypes.c_int64, _i32p, _f64p,
+                                              ctypes.POINTER(_MergeStats)]
         L.sbpo_sbp.restype = ctypes.c_int
         L.sbpo_sbp.argtypes = [vp, ctypes.POINTER(_Options), _i32p, ctypes.POINTER(_RunStats)]
         L.sbpo_nmi.restype = ctypes.c_double
@@ -252,10 +258,51 @@ class Blockmodel:
             raise RuntimeError("oracle merge failed")
         return dict(best=best, dS=dS, proposals=ms.proposals, avoided=ms.avoided)
 
+    def finetune_replayed(self, algo, proposal, uniform, batches=10, bracket=False, max_sweeps=0):
+        """The finetune driven by a recorded proposal stream: proposal[t*V + v] and uniform[t*V + v]
+        are the proposed block and the accept uniform of vertex v's visit in sweep t (2.0 where
+        the stream has none: never accepts)."""
+        rp = move_records(proposal, uniform)
+        st = _Stats()
+        rc = lib().sbpo_finetune_moves(self.h, self.graph.h, algo, batches, int(bracket), _p(rp, _u32p),
+                                       len(rp) // 4, max_sweeps, ctypes.byref(st))
+        if rc != 0:
+            raise RuntimeError("oracle finetune failed (a visit with no recorded proposal, or one out of range)")
+        return dict(visits=st.visits, proposals_moved=st.proposals_moved, accepted=st.accepted,
+                    sweeps=st.sweeps, mdl=st.mdl)
+
+    def merge_blocks_replayed(self, proposal, approximate=True):
+        """The merge step with proposal[r*10 + i] as proposal i of block r."""
+        B = self.B
+        best = np.zeros(B, np.int32)
+        dS = np.zeros(B, np.float64)
+        ms = _MergeStats()
+        rp = move_records(proposal, None)
+        rc = lib().sbpo_merge_blocks_moves(self.h, self.graph.h, int(approximate), _p(rp, _u32p), len(rp) // 4,
+                                           _p(best), _p(dS, _f64p), ctypes.byref(ms))
+        if rc != 0:
+            raise RuntimeError("oracle merge failed (a proposal missing or out of range)")
+        return dict(best=best, dS=dS, proposals=ms.proposals, avoided=ms.avoided)
+
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:
             _lib.sbpo_bm_destroy(self.h)
             self.h = None
+
+
+def move_records(proposal, uniform):
+    """4-word records (s, 0, u_hi, u_lo) of a recorded proposal stream: the proposed block and
+    the bits of the accept uniform (2.0, which never accepts, where there is none)."""
+    prop = np.ascontiguousarray(proposal, np.int32)
+    uni = np.full(len(prop), 2.0) if uniform is None else np.ascontiguousarray(uniform, np.float64)
+    if uni.shape != prop.shape:
+        raise ValueError("proposal and uniform streams differ in length")
+    bits = uni.view(np.uint64)
+    rec = np.zeros((len(prop), 4), np.uint32)
+    rec[:, 0] = prop.view(np.uint32)
+    rec[:, 2] = (bits >> np.uint64(32)).astype(np.uint32)
+    rec[:, 3] = (bits & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+    return rec.reshape(-1)
 
 
 def null_mdl_v1(E):

@@ -1,0 +1,75 @@
+"""CPU pin of the oracle against the reference itself under seeded replay.
+
+A patched copy of the reference (oracle/_ref/replay/ref_driver, built by oracle/build_reference.py
+from the reference's own sources: seeded engines, a log of every proposal and accept uniform it
+draws, FP64 log terms, one orientation and a stable order for merges of equal delta-MDL) runs
+sbp::stochastic_block_partition on the host and logs the blockmodel at the start and end of every
+merge and finetune call.  The C oracle replays each call from the reference's own start state,
+fed only the reference's recorded proposals and accept uniforms:
+
+  * merge calls: every block's best merge and its delta-MDL, then the state after the carry-out
+    and rebuild;
+  * finetune calls (all three algorithms, the reference's own order of equal degrees in the
+    hybrid split): the sweep count and the end state, the drifting block degree d included.
+
+Integer state bit for bit, delta-MDL within 1e-9 relative.  This checks the oracle's trajectory
+rules (quirks Q1-Q5, the batch apply order, the early stops, the carry-out) against the reference
+directly, without the GPU engine in between.
+"""
+import numpy as np
+import pytest
+
+RTOL_MDL = 1e-9
+
+
+@pytest.fixture(scope="module")
+def RR():
+    import build_reference as R
+    if not R.replay_built():
+        if not R.reference_available():
+            pytest.fail("oracle/_ref/replay/ref_driver is not built and the reference sources are absent")
+        R.build_replay()
+    import ref_replay
+    return ref_replay
+
+
+def assert_state(RR, bm, state, what):
+    assert bm.B == state["B"], what
+    assert np.array_equal(bm.assignment(), state["assignment"]), what + ": assignment"
+    assert np.array_equal(bm.matrix(), RR.matrix(state)), what + ": block matrix"
+    do, di, d = bm.degrees()
+    assert np.array_equal(do, state["d_out"]), what + ": d_out"
+    assert np.array_equal(di, state["d_in"]), what + ": d_in"
+    assert np.array_equal(d, state["d"]), what + ": d"
+
+
+@pytest.mark.parametrize("algo", ["metropolis_hastings", "async_gibbs", "hybrid_mcmc"])
+def test_oracle_replays_the_reference_call_by_call(O, RR, algo):
+    import dcsbm
+    V, src, dst, _ = dcsbm.config_graph(1)
+    res, calls = RR.run("sbp", V, src, dst, algo=algo, seed=11)
+    og = O.Graph(V, src, dst)
+    og.set_split(*res["split"])
+    code = {"metropolis_hastings": O.MH, "async_gibbs": O.GIBBS, "hybrid_mcmc": O.HYBRID}
+    checked = {"merge": 0, "finetune": 0}
+    for c in calls:
+        st0, st1 = c["begin"], c["end"]
+        bm = O.Blockmodel(og, st0["B"], st0["assignment"])
+        if c["kind"] == "merge":
+            bm.set_num_blocks_to_merge(st0["num_blocks_to_merge"])
+            out = bm.merge_blocks_replayed(RR.merge_stream(c))
+            best, delta = c["scores"]
+            assert np.array_equal(out["best"], best), f"call {c['id']}: best merge per block"
+            np.testing.assert_allclose(out["dS"], delta, rtol=RTOL_MDL, atol=RTOL_MDL * np.abs(delta).max())
+            assert_state(RR, bm, st1, f"merge call {c['id']} (B {st0['B']} -> {st1['B']})")
+            checked["merge"] += 1
+        else:
+            # a finetune starts from a fresh rebuild (it follows a merge), d included
+            assert_state(RR, bm, st0, f"finetune call {c['id']} start")
+            prop, uni = RR.finetune_stream(c, V)
+            st = bm.finetune_replayed(code[c["kind"]], prop, uni, batches=10, bracket=c["bracket"] == 1)
+            assert st["sweeps"] == c["sweeps"], f"finetune call {c['id']}: sweeps"
+            assert_state(RR, bm, st1, f"{c['kind']} call {c['id']} at B {st0['B']}")
+            assert np.float32(bm.mdl()) == pytest.approx(st1["overall_entropy"], rel=1e-6)
+            checked["finetune"] += 1
+    assert checked["merge"] >= 5 and checked["finetune"] >= 5, checked
