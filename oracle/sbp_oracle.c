@@ -1104,8 +1104,38 @@ typedef struct {
     int64_t visits, accepted;
 } SbpoRunStats;
 
+/* Recorded streams of a partition's calls, in call order (merges and finetunes alternate as
+ * the loop makes them); block_counts receives the block count after every call. */
+typedef struct {
+    int num_calls;
+    const uint32_t *const *records;
+    const int64_t *num_records;
+    int max_sweeps;
+    int calls_made;
+    int *block_counts;
+} SbpoPartitionReplay;
+
+static int sbp_run(const SbpoGraph *g, const SbpoOptions *opt, int *assignment_out, SbpoRunStats *rs,
+                   SbpoPartitionReplay *rp);
+
 /* sbp::stochastic_block_partition (src/sbp.cpp:61-98). */
 int sbpo_sbp(const SbpoGraph *g, const SbpoOptions *opt, int *assignment_out, SbpoRunStats *rs) {
+    return sbp_run(g, opt, assignment_out, rs, NULL);
+}
+
+/* The same loop driven by recorded streams: call k reads records[k] (num_records[k] records),
+ * every finetune capped at max_sweeps sweeps (0: no cap, as the reference's patched
+ * MAX_NUM_ITERATIONS).  Returns the number of calls made, or -1 when a stream runs out. */
+int sbpo_sbp_moves(const SbpoGraph *g, const SbpoOptions *opt, int num_calls, const uint32_t *const *records,
+                   const int64_t *num_records, int max_sweeps, int *assignment_out, int *block_counts,
+                   SbpoRunStats *rs) {
+    SbpoPartitionReplay rp = {num_calls, records, num_records, max_sweeps, 0, block_counts};
+    int rc = sbp_run(g, opt, assignment_out, rs, &rp);
+    return rc ? -1 : rp.calls_made;
+}
+
+static int sbp_run(const SbpoGraph *g, const SbpoOptions *opt, int *assignment_out, SbpoRunStats *rs,
+                   SbpoPartitionReplay *rp) {
     memset(rs, 0, sizeof(*rs));
     int V = g->V;
     int *ident = (int *)malloc(sizeof(int) * (size_t)(V + 1));
@@ -1117,11 +1147,24 @@ int sbpo_sbp(const SbpoGraph *g, const SbpoOptions *opt, int *assignment_out, Sb
     uint32_t call = 0;
     int rc = 0;
     while (!t.optimal_found) {
-        if (sbpo_merge_blocks(bm, g, opt->approximate, opt->seed, call, NULL, 0, NULL, NULL, NULL)) { rc = -1; break; }
+        SbpoRng rng = {opt->seed, NULL, 0, 0};
+        if (rp) {
+            if (rp->calls_made >= rp->num_calls) { rc = -1; break; }
+            rng = (SbpoRng){0, rp->records[rp->calls_made], rp->num_records[rp->calls_made], 1};
+        }
+        if (merge_run(bm, g, opt->approximate, rng, call, NULL, NULL, NULL)) { rc = -1; break; }
+        if (rp) rp->block_counts[rp->calls_made++] = bm->B;
         int algo = opt->algo;
         if (algo == SBPO_GIBBS && !(iteration < (float)opt->asynciterations)) algo = SBPO_MH;
         SbpoStats st;
-        sbpo_finetune(bm, g, algo, opt->batches, t.bm[2] != NULL, opt->seed, call, NULL, 0, 0, &st);
+        rng = (SbpoRng){opt->seed, NULL, 0, 0};
+        if (rp) {
+            if (rp->calls_made >= rp->num_calls) { rc = -1; break; }
+            rng = (SbpoRng){0, rp->records[rp->calls_made], rp->num_records[rp->calls_made], 1};
+        }
+        if (finetune_run(bm, g, algo, opt->batches, t.bm[2] != NULL, rng, call, rp ? rp->max_sweeps : 0, &st) &&
+            rp) { rc = -1; break; }
+        if (rp) rp->block_counts[rp->calls_made++] = bm->B;
         rs->mcmc_sweeps += st.sweeps; rs->visits += st.visits; rs->accepted += st.accepted;
         ++iteration; ++call;
         SbpoBM *next = tri_next(&t, bm);

@@ -18,6 +18,7 @@ MH, GIBBS, HYBRID = 0, 1, 2
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _f64p = ctypes.POINTER(ctypes.c_double)
+_i64p = ctypes.POINTER(ctypes.c_int64)
 
 
 def build(force=False):
@@ -110,6 +111,10 @@ def lib():
         L.sbpo_merge_blocks_moves.restype = ctypes.c_int
         L.sbpo_merge_blocks_moves.argtypes = [vp, vp, ctypes.c_int, _u32p, ctypes.c_int64, _i32p, _f64p,
                                               ctypes.POINTER(_MergeStats)]
+        L.sbpo_sbp_moves.restype = ctypes.c_int
+        L.sbpo_sbp_moves.argtypes = [vp, ctypes.POINTER(_Options), ctypes.c_int,
+                                     ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32)), _i64p, ctypes.c_int, _i32p,
+                                     _i32p, ctypes.POINTER(_RunStats)]
         L.sbpo_sbp.restype = ctypes.c_int
         L.sbpo_sbp.argtypes = [vp, ctypes.POINTER(_Options), _i32p, ctypes.POINTER(_RunStats)]
         L.sbpo_nmi.restype = ctypes.c_double
@@ -327,6 +332,26 @@ def sbp(graph, algo=GIBBS, batches=10, approximate=True, asynciterations=2**31 -
         raise RuntimeError("oracle sbp failed")
     return out, dict(mdl=rs.mdl, num_blocks=rs.num_blocks, outer_iterations=rs.outer_iterations,
                      mcmc_sweeps=rs.mcmc_sweeps, visits=rs.visits, accepted=rs.accepted)
+
+
+def sbp_replayed(graph, streams, algo=GIBBS, batches=10, approximate=True, max_sweeps=0):
+    """sbp with every merge and finetune call driven by a recorded stream, in call order:
+    streams[k] = (proposal, uniform) of call k (uniform None for a merge call).  Returns
+    (assignment, stats, block count after every call)."""
+    recs = [move_records(p, u) for p, u in streams]
+    ptrs = (ctypes.POINTER(ctypes.c_uint32) * max(1, len(recs)))(*[_p(r, _u32p) for r in recs])
+    counts = np.array([len(r) // 4 for r in recs] or [0], np.int64)
+    blocks = np.zeros(max(1, len(recs)), np.int32)
+    opt = _Options(algo, batches, int(approximate), 2**31 - 1, 0)
+    rs = _RunStats()
+    out = np.zeros(graph.V, np.int32)
+    made = lib().sbpo_sbp_moves(graph.h, ctypes.byref(opt), len(recs), ptrs, counts.ctypes.data_as(_i64p),
+                                int(max_sweeps), _p(out), _p(blocks), ctypes.byref(rs))
+    if made < 0:
+        raise RuntimeError("oracle sbp replay failed (the partition needed more calls than were recorded, or a "
+                           "stream lacked a proposal)")
+    return out, dict(mdl=rs.mdl, num_blocks=rs.num_blocks, outer_iterations=rs.outer_iterations,
+                     mcmc_sweeps=rs.mcmc_sweeps, visits=rs.visits, accepted=rs.accepted), blocks[:made].copy()
 
 
 # ------------------------------------------------------------------------------------------

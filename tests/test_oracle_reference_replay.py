@@ -10,7 +10,9 @@ fed only the reference's recorded proposals and accept uniforms:
   * merge calls: every block's best merge and its delta-MDL, then the state after the carry-out
     and rebuild;
   * finetune calls (all three algorithms, the reference's own order of equal degrees in the
-    hybrid split): the sweep count and the end state, the drifting block degree d included.
+    hybrid split): the sweep count and the end state, the drifting block degree d included;
+  * whole partitions: the oracle's own merge, finetune and golden-section loop fed only the
+    recorded streams, the block count after every call and the final assignment.
 
 Integer state bit for bit, delta-MDL within 1e-9 relative.  This checks the oracle's trajectory
 rules (quirks Q1-Q5, the batch apply order, the early stops, the carry-out) against the reference
@@ -73,3 +75,22 @@ def test_oracle_replays_the_reference_call_by_call(O, RR, algo):
             assert np.float32(bm.mdl()) == pytest.approx(st1["overall_entropy"], rel=1e-6)
             checked["finetune"] += 1
     assert checked["merge"] >= 5 and checked["finetune"] >= 5, checked
+
+
+@pytest.mark.parametrize("algo", ["metropolis_hastings", "async_gibbs", "hybrid_mcmc"])
+def test_oracle_replays_the_reference_partition(O, RR, algo):
+    """The oracle's own merge, finetune and golden-section loop, fed only the reference's
+    recorded proposals and uniforms: the block count after every call, the final blockmodel's
+    assignment and its MDL equal the reference's."""
+    import dcsbm
+    V, src, dst, _ = dcsbm.config_graph(1)
+    res, calls = RR.run("sbp", V, src, dst, algo=algo, seed=12)
+    og = O.Graph(V, src, dst)
+    og.set_split(*res["split"])
+    streams = [(RR.merge_stream(c), None) if c["kind"] == "merge" else RR.finetune_stream(c, V) for c in calls]
+    code = {"metropolis_hastings": O.MH, "async_gibbs": O.GIBBS, "hybrid_mcmc": O.HYBRID}
+    out, st, counts = O.sbp_replayed(og, streams, algo=code[algo], batches=10)
+    assert list(counts) == [c["end"]["B"] for c in calls], "block count after every call"
+    assert st["num_blocks"] == res["num_blocks"]
+    assert st["mdl"] == pytest.approx(res["mdl"], rel=1e-6)
+    assert np.array_equal(out, res["assignment"])
