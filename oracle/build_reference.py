@@ -170,6 +170,21 @@ REPLAY_PATCHES = [
      "        proposal.num_out_neighbor_edges, proposal.num_in_neighbor_edges, blockmodel);", 1),
     ("src/blockmodel/blockmodel.cpp", "lit", "std::vector<int> best_merges = utils::sort_indices(delta_entropy_for_each_block);",
      "std::vector<int> best_merges = sbp_replay::stable_sort_indices(delta_entropy_for_each_block);", 1),
+    # P3, advanced carry-out (src/block_merge.cpp:123-217): the priority queue breaks equal
+    # delta-MDLs by block id (std::priority_queue leaves their order to its heap), and a queued
+    # merge is re-evaluated as the canonical rounded score, as merges are ranked everywhere
+    # (both anchors start at a line break: the file keeps a commented-out copy of the function)
+    ("src/block_merge.cpp", "after", ("\nvoid carry_out_best_merges_advanced(",
+                                      "\n    auto cmp_fxn = [](merge_t left, merge_t right) { return std::get<2>(left) > "
+                                      "std::get<2>(right); };"),
+     "\n    auto cmp_fxn = [](merge_t left, merge_t right) {\n"
+     "        return std::get<2>(left) != std::get<2>(right) ? std::get<2>(left) > std::get<2>(right)\n"
+     "                                                       : std::get<0>(left) > std::get<0>(right);\n"
+     "    };", 1),
+    ("src/block_merge.cpp", "lit",
+     "double delta_entropy_actual = entropy::block_merge_delta_mdl(merge_from, proposal, blockmodel, delta);",
+     "double delta_entropy_actual = sbp_replay::merge_delta_canonical(merge_from, merge_to, k_out, k_in, blockmodel);",
+     1),
 ]
 
 

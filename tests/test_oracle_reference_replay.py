@@ -8,7 +8,7 @@ merge and finetune call.  The C oracle replays each call from the reference's ow
 fed only the reference's recorded proposals and accept uniforms:
 
   * merge calls: every block's best merge and its delta-MDL, then the state after the carry-out
-    and rebuild;
+    (simple, and the advanced priority-queue one) and rebuild;
   * finetune calls (all three algorithms, the reference's own order of equal degrees in the
     hybrid split): the sweep count and the end state, the drifting block degree d included;
   * whole partitions: the oracle's own merge, finetune and golden-section loop fed only the
@@ -45,11 +45,14 @@ def assert_state(RR, bm, state, what):
     assert np.array_equal(d, state["d"]), what + ": d"
 
 
-@pytest.mark.parametrize("algo", ["metropolis_hastings", "async_gibbs", "hybrid_mcmc"])
-def test_oracle_replays_the_reference_call_by_call(O, RR, algo):
+@pytest.mark.parametrize("algo,approximate", [("metropolis_hastings", True), ("async_gibbs", True),
+                                              ("hybrid_mcmc", True), ("async_gibbs", False)])
+def test_oracle_replays_the_reference_call_by_call(O, RR, algo, approximate):
+    """approximate False: the advanced carry-out (block_merge::carry_out_best_merges_advanced,
+    a priority queue with lazily re-evaluated merges)."""
     import dcsbm
     V, src, dst, _ = dcsbm.config_graph(1)
-    res, calls = RR.run("sbp", V, src, dst, algo=algo, seed=11)
+    res, calls = RR.run("sbp", V, src, dst, algo=algo, seed=11, approximate=approximate)
     og = O.Graph(V, src, dst)
     og.set_split(*res["split"])
     code = {"metropolis_hastings": O.MH, "async_gibbs": O.GIBBS, "hybrid_mcmc": O.HYBRID}
@@ -59,7 +62,7 @@ def test_oracle_replays_the_reference_call_by_call(O, RR, algo):
         bm = O.Blockmodel(og, st0["B"], st0["assignment"])
         if c["kind"] == "merge":
             bm.set_num_blocks_to_merge(st0["num_blocks_to_merge"])
-            out = bm.merge_blocks_replayed(RR.merge_stream(c))
+            out = bm.merge_blocks_replayed(RR.merge_stream(c), approximate=approximate)
             best, delta = c["scores"]
             assert np.array_equal(out["best"], best), f"call {c['id']}: best merge per block"
             np.testing.assert_allclose(out["dS"], delta, rtol=RTOL_MDL, atol=RTOL_MDL * np.abs(delta).max())
@@ -77,19 +80,20 @@ def test_oracle_replays_the_reference_call_by_call(O, RR, algo):
     assert checked["merge"] >= 5 and checked["finetune"] >= 5, checked
 
 
-@pytest.mark.parametrize("algo", ["metropolis_hastings", "async_gibbs", "hybrid_mcmc"])
-def test_oracle_replays_the_reference_partition(O, RR, algo):
+@pytest.mark.parametrize("algo,approximate", [("metropolis_hastings", True), ("async_gibbs", True),
+                                              ("hybrid_mcmc", True), ("metropolis_hastings", False)])
+def test_oracle_replays_the_reference_partition(O, RR, algo, approximate):
     """The oracle's own merge, finetune and golden-section loop, fed only the reference's
     recorded proposals and uniforms: the block count after every call, the final blockmodel's
     assignment and its MDL equal the reference's."""
     import dcsbm
     V, src, dst, _ = dcsbm.config_graph(1)
-    res, calls = RR.run("sbp", V, src, dst, algo=algo, seed=12)
+    res, calls = RR.run("sbp", V, src, dst, algo=algo, seed=12, approximate=approximate)
     og = O.Graph(V, src, dst)
     og.set_split(*res["split"])
     streams = [(RR.merge_stream(c), None) if c["kind"] == "merge" else RR.finetune_stream(c, V) for c in calls]
     code = {"metropolis_hastings": O.MH, "async_gibbs": O.GIBBS, "hybrid_mcmc": O.HYBRID}
-    out, st, counts = O.sbp_replayed(og, streams, algo=code[algo], batches=10)
+    out, st, counts = O.sbp_replayed(og, streams, algo=code[algo], batches=10, approximate=approximate)
     assert list(counts) == [c["end"]["B"] for c in calls], "block count after every call"
     assert st["num_blocks"] == res["num_blocks"]
     assert st["mdl"] == pytest.approx(res["mdl"], rel=1e-6)
