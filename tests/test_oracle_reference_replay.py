@@ -12,7 +12,9 @@ fed only the reference's recorded proposals and accept uniforms:
   * finetune calls (all three algorithms, the reference's own order of equal degrees in the
     hybrid split): the sweep count and the end state, the drifting block degree d included;
   * whole partitions: the oracle's own merge, finetune and golden-section loop fed only the
-    recorded streams, the block count after every call and the final assignment.
+    recorded streams, the block count after every call and the final assignment;
+  * on the 20,000-vertex benchmark graph: finetunes of all three algorithms from a perturbed
+    planted partition, and a 640 -> 320 block merge with both carry-outs.
 
 Integer state bit for bit, delta-MDL within 1e-9 relative.  This checks the oracle's trajectory
 rules (quirks Q1-Q5, the batch apply order, the early stops, the carry-out) against the reference
@@ -124,3 +126,54 @@ def test_oracle_meets_the_unseeded_criterion_against_the_unmodified_reference(O,
     out, st = O.sbp(og, algo=code[run["algorithm"]], batches=run["batches"], approximate=run["approximate"], seed=17)
     assert abs(st["mdl"] - run["mdl"]) <= 0.005 * run["mdl"]
     assert abs(O.nmi(out, truth) - run["nmi"]) <= 0.01
+
+
+def _perturbed_planted(truth, frac, seed):
+    rng = np.random.default_rng(seed)
+    a = truth.astype(np.int32).copy()
+    moved = rng.random(len(a)) < frac
+    a[moved] = rng.integers(0, int(a.max()) + 1, moved.sum())
+    return a
+
+
+@pytest.mark.parametrize("algo", ["metropolis_hastings", "async_gibbs", "hybrid_mcmc"])
+def test_oracle_replays_reference_finetunes_on_the_20k_graph(O, RR, algo):
+    """The 20,000-vertex, 32-block benchmark graph from its planted partition with 30 % of the
+    vertices moved: one reference finetune capped at 5 sweeps, replayed by the oracle bit for
+    bit (thousands of accepted moves per call)."""
+    import dcsbm
+    V, src, dst, truth = dcsbm.config_graph(2)
+    a = _perturbed_planted(truth, 0.3, 5)
+    res, calls = RR.run("finetune", V, src, dst, algo=algo, assignment=a, seed=7, max_sweeps=5)
+    og = O.Graph(V, src, dst)
+    og.set_split(*res["split"])
+    (c,) = [c for c in calls if c["kind"] != "merge"]
+    code = {"metropolis_hastings": O.MH, "async_gibbs": O.GIBBS, "hybrid_mcmc": O.HYBRID}
+    bm = O.Blockmodel(og, c["begin"]["B"], c["begin"]["assignment"])
+    prop, uni = RR.finetune_stream(c, V)
+    st = bm.finetune_replayed(code[algo], prop, uni, batches=10, bracket=c["bracket"] == 1, max_sweeps=5)
+    assert st["sweeps"] == c["sweeps"]
+    assert st["accepted"] > 1000
+    assert_state(RR, bm, c["end"], f"{algo} on the 20k graph")
+
+
+@pytest.mark.parametrize("approximate", [True, False])
+def test_oracle_replays_a_reference_merge_on_the_20k_graph(O, RR, approximate):
+    """A merge of the 20,000-vertex graph from 640 blocks (each planted block split 20 ways) to
+    320, both carry-outs: every block's best merge and delta-MDL and the state after it."""
+    import dcsbm
+    V, src, dst, truth = dcsbm.config_graph(2)
+    rng = np.random.default_rng(6)
+    _, a = np.unique(truth.astype(np.int64) * 20 + rng.integers(0, 20, V), return_inverse=True)
+    a = a.astype(np.int32)
+    B = int(a.max()) + 1
+    res, calls = RR.run("merge", V, src, dst, assignment=a, num_blocks_to_merge=B // 2, seed=8,
+                        approximate=approximate)
+    (c,) = [c for c in calls if c["kind"] == "merge"]
+    bm = O.Blockmodel(O.Graph(V, src, dst), c["begin"]["B"], c["begin"]["assignment"])
+    bm.set_num_blocks_to_merge(c["begin"]["num_blocks_to_merge"])
+    out = bm.merge_blocks_replayed(RR.merge_stream(c), approximate=approximate)
+    best, delta = c["scores"]
+    assert np.array_equal(out["best"], best)
+    np.testing.assert_allclose(out["dS"], delta, rtol=RTOL_MDL, atol=RTOL_MDL * np.abs(delta).max())
+    assert_state(RR, bm, c["end"], "merge on the 20k graph")
