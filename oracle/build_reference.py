@@ -214,8 +214,44 @@ def _apply(text, kind, anchor, repl, count, name):
     raise ValueError(kind)
 
 
+def _fingerprint(patches, files):
+    """Hash of a patched build's inputs that live in this repository (its patch list, hooks,
+    driver and shims), so that a build made from older inputs counts as not built."""
+    import hashlib
+    h = hashlib.sha256(repr(patches).encode())
+    for path in sorted(files):
+        with open(path, "rb") as f:
+            h.update(os.path.relpath(path, HERE).encode() + f.read())
+    return h.hexdigest()
+
+
+def _built_from(driver, out_dir, fingerprint):
+    stamp = os.path.join(out_dir, "inputs.sha256")
+    if not (os.path.exists(driver) and os.path.exists(stamp)):
+        return False
+    with open(stamp) as f:
+        return f.read().strip() == fingerprint
+
+
+def _stamp(out_dir, fingerprint):
+    with open(os.path.join(out_dir, "inputs.sha256"), "w") as f:
+        f.write(fingerprint + "\n")
+
+
+def _files_under(d):
+    return [os.path.join(r, n) for r, _, names in os.walk(d) for n in names if not n.endswith(".pyc")]
+
+
+def _shim_files():
+    return _files_under(os.path.join(HERE, "ref_shims")) + [os.path.join(HERE, "ref_driver.cpp")]
+
+
+def _replay_fingerprint():
+    return _fingerprint(REPLAY_PATCHES, _shim_files() + _files_under(HOOKS))
+
+
 def replay_built():
-    return os.path.exists(REPLAY_DRIVER)
+    return _built_from(REPLAY_DRIVER, REPLAY_OUT, _replay_fingerprint())
 
 
 def _patched_tree(out_dir, patches):
@@ -244,8 +280,10 @@ def build_replay(force=False, jobs=8):
     if not reference_available():
         raise RuntimeError("reference sources not found")
     root = _patched_tree(REPLAY_OUT, REPLAY_PATCHES)
-    return _compile(root, REPLAY_OUT, REPLAY_DRIVER, extra_sources=[os.path.join(HOOKS, "sbp_replay.cpp")],
-                    extra_flags=["-I" + HOOKS, "-include", os.path.join(HOOKS, "sbp_replay.h")], jobs=jobs)
+    out = _compile(root, REPLAY_OUT, REPLAY_DRIVER, extra_sources=[os.path.join(HOOKS, "sbp_replay.cpp")],
+                   extra_flags=["-I" + HOOKS, "-include", os.path.join(HOOKS, "sbp_replay.h")], jobs=jobs)
+    _stamp(REPLAY_OUT, _replay_fingerprint())
+    return out
 
 
 # ---- the capped timing build: the reference unchanged except for a sweep cap -------------------
@@ -261,7 +299,7 @@ CAPPED_PATCHES = [
 
 
 def capped_built():
-    return os.path.exists(CAPPED_DRIVER)
+    return _built_from(CAPPED_DRIVER, CAPPED_OUT, _fingerprint(CAPPED_PATCHES, _shim_files()))
 
 
 def build_capped(force=False, jobs=8):
@@ -270,8 +308,10 @@ def build_capped(force=False, jobs=8):
     if not reference_available():
         raise RuntimeError("reference sources not found")
     root = _patched_tree(CAPPED_OUT, CAPPED_PATCHES)
-    return _compile(root, CAPPED_OUT, CAPPED_DRIVER,
-                    extra_flags=["-include", os.path.join(HERE, "ref_shims", "sweep_cap.h")], jobs=jobs)
+    out = _compile(root, CAPPED_OUT, CAPPED_DRIVER,
+                   extra_flags=["-include", os.path.join(HERE, "ref_shims", "sweep_cap.h")], jobs=jobs)
+    _stamp(CAPPED_OUT, _fingerprint(CAPPED_PATCHES, _shim_files()))
+    return out
 
 
 def _write_edges(path, V, src, dst):
