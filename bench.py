@@ -67,6 +67,9 @@ def args_parse():
     ap.add_argument("--eval-case", type=int, default=0, metavar="PARTS",
                     help="a small case for kernel profilers instead of the bench: three host-driven asynchronous-"
                          "Gibbs sweeps from the planted partition split PARTS ways")
+    ap.add_argument("--eval-load-model", type=int, default=0, metavar="PARTS",
+                    help="host only, no GPU: the loads one visit of the evaluation kernel makes on the --eval-case "
+                         "state, counted from the graph and the assignment (bytes and DRAM sectors per visit)")
     return ap.parse_args()
 
 
@@ -78,13 +81,72 @@ def eval_case(a, V, src, dst, truth):
     import sbp_b200 as S
     S.load()
     g = S.Graph(V, src, dst)
-    rng = np.random.default_rng(0)
-    b = truth.astype(np.int64) * a.eval_case + rng.integers(0, a.eval_case, V)
-    b = np.unique(b, return_inverse=True)[1].astype(np.int32)
+    b = split_planted(truth, a.eval_case)
     S.set_option("graph_sweeps", 0)
     bm = S.Blockmodel(g, int(b.max()) + 1, b)
     st = S.finetune.asynchronous_gibbs(bm, batches=a.batches, seed=3, max_sweeps=3)
     print(json.dumps({"eval_case": a.eval_case, "B": bm.B, "visits": st["visits"], "accepted": st["accepted"]}))
+
+
+def split_planted(truth, parts):
+    """The planted partition with each block split into `parts` random parts (seed 0), relabelled
+    0..B-1: the state of the kernel-profiler case."""
+    import numpy as np
+    rng = np.random.default_rng(0)
+    b = truth.astype(np.int64) * parts + rng.integers(0, parts, len(truth))
+    return np.unique(b, return_inverse=True)[1].astype(np.int32)
+
+
+def eval_load_model(V, src, dst, truth, parts):
+    """Loads of one visit of the evaluation kernel on dense storage (evaluate_vertex), counted on
+    the host from the de-duplicated graph and the profiler case's assignment, averaged over all
+    vertices.  Per visit of v (block r, k = k_out + k_in neighbours, nb distinct neighbour
+    blocks u, proposed block s, walk block t):
+      graph    CSR offsets (16 B), self flag, b[v], the neighbour ids (4 k B) and blocks (4 k B);
+      cells    M[r,u], M[u,r], M[s,u], M[u,s] and d[u] for every u, the corners and degrees of r, s;
+      walk     d_out[t], d_in[t], chunk sums of t (nch ints, nch = ld / 128; both directions when
+               nch <= 32), and one 128-cell chunk (512 B).
+    `formula` is the roofline's algorithmic bytes (12 + 8 k); `with_blockmodel` adds the cells and
+    the walk.  The DRAM estimates count whole 32-byte (and 64-byte) segments of the neighbour
+    lists, of the matrix rows r and s of M and MT that hold the cells (u's sharing a segment share
+    it), and of the walk; b[], the degree arrays and the log table are taken to stay in L2
+    (under 20 MB together here), the matrices (1 GB here) not."""
+    import numpy as np
+    b = split_planted(truth, parts)
+    B = int(b.max()) + 1
+    key = src.astype(np.int64) * V + dst
+    keep = np.sort(np.unique(key, return_index=True)[1])
+    s_, d_ = src[keep].astype(np.int64), dst[keep].astype(np.int64)
+    loop = s_ == d_
+    # every vertex's neighbours: out-neighbours, then in-neighbours without the self loop
+    v_all = np.concatenate([s_, d_[~loop]])
+    u_all = np.concatenate([d_, s_[~loop]])
+    k = np.bincount(v_all, minlength=V)
+    kout = np.bincount(s_, minlength=V)
+    ld = (B + 127) // 128 * 128
+    nch = ld // 128
+    order = np.argsort(v_all, kind="stable")
+    u_sorted = u_all[order]
+    starts = np.concatenate([[0], np.cumsum(k)])
+    nb = np.zeros(V)
+    cells = {32: np.zeros(V), 64: np.zeros(V)}
+    for v in range(V):
+        us = u_sorted[starts[v]:starts[v + 1]]
+        blocks = np.unique(b[us[us != v]])
+        nb[v] = len(blocks)
+        for g in cells:
+            cells[g][v] = 4 * len(np.unique(blocks // (g // 4))) * g   # rows r, s of M and MT
+    seg = lambda n, g: -(-n // g) * g                                   # noqa: E731
+    sums = 2 if nch <= 32 else 1
+    walk_useful = 8 + sums * nch * 4 + 512
+    formula = 12 + 8 * k
+    with_bm = 16 + 1 + 4 + 8 * k + 20 * nb + 12 + 20 + walk_useful
+    dram = {f"{g}B_segments": float((seg(4 * kout, g) + seg(4 * (k - kout), g) + cells[g] +
+                                     sums * seg(nch * 4, g) + 512).mean()) for g in (32, 64)}
+    return {"workload": f"directed DC-SBM {V} V, planted partition split {parts} ways", "B": B, "ld": ld,
+            "chunks_per_row": nch, "mean_k": float(k.mean()), "mean_distinct_neighbour_blocks": float(nb.mean()),
+            "bytes_per_visit": {"formula": float(formula.mean()), "with_blockmodel": float(with_bm.mean())},
+            "dram_bytes_per_visit_estimate": dram}
 
 
 def peaks():
@@ -373,6 +435,9 @@ def main():
               "sweep_driver": "host loop" if a.host_sweeps else "one CUDA graph per finetune call"}
     if a.eval_case:
         eval_case(a, V, src, dst, truth)
+        return
+    if a.eval_load_model:
+        print(json.dumps(eval_load_model(V, src, dst, truth, a.eval_load_model)))
         return
 
     if a.impl == "reference":
