@@ -19,7 +19,11 @@ import os
 
 import numpy as np
 
-# Configurations of the benchmark suite (sizes and laws as specified; seeds fixed).
+# The suite's graphs by suite number (seeds fixed; the batched suite is batched_config):
+#   1  1,000 vertices, 11 blocks, low size variation: the small plain-SBP case the reference runs in seconds
+#   2  20,000 vertices, 32 blocks, high variation and overlap: asynchronous Gibbs, hybrid, replay at scale
+#   4  200,000 vertices, 71 blocks: the bench graph (vertex moves/s, learned vs plain proposal)
+#   5  2,000,000 vertices, 150 blocks, degree exponent 2.1 on [10, 200]: the large hybrid case
 CONFIGS = {
     1: dict(V=1_000, K=11, alpha=10.0, gamma=2.5, kmin=10, kmax=100, w=0.8, seed=1),
     2: dict(V=20_000, K=32, alpha=1.0, gamma=2.5, kmin=10, kmax=100, w=0.6, seed=2),
